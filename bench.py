@@ -1,0 +1,311 @@
+"""Headline benchmark: Helmholtz solves/s, C192 x 70, to 1e-8, mixed vs FP64.
+
+One step = one complete solve of the seeded C192 x 70 W3 Helmholtz system
+(GCR(10) preconditioned by a 4-level multigrid V-cycle, C192/96/48/24,
+block-Jacobi column smoother 2+2 sweeps) from a zero initial guess to a
+relative FP64 residual of 1e-8, in the mixed-precision form (FP32 inner
+GCR + multigrid, FP64 residual and refinement).  The plain FP64 solve is
+timed beside it.  Inputs (operators, right-hand side) are resident in HBM;
+the e2e figure adds, every step, the host->device copy of the right-hand
+side from pinned host memory and the device->host copy of the solution,
+through the C ABI.
+
+--impl reference times the CPU restatement of the same solver (the oracle;
+the Fortran reference cannot be compiled here) on the host cores.
+
+Multi-GPU: the path does not shard (the whole mesh is resident on one GPU);
+--gpus N runs N independent replicas and reports their total throughput.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "Helmholtz solves/s C192x70L to 1e-8: mixed vs FP64 on 1 B200; HBM GB/s"
+N_FINE, NLAYERS, MG_LEVELS, SEED = 192, 70, 4, 3
+FALLBACK_HBM_GBS = 6650.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="lfg", choices=["lfg", "reference"])
+    ap.add_argument("--n", type=int, default=N_FINE, help=argparse.SUPPRESS)
+    return ap.parse_args()
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.idx, self.rows, self.proc = gpu_index, [], None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except (FileNotFoundError, OSError):
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 8:
+                self.rows.append(parts)
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(r[0]) for r in self.rows if r[0].replace(".", "").isdigit()]
+        mx = [float(r[1]) for r in self.rows if r[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows for i in range(4)
+                          if r[4 + i].lower().startswith("active")})
+        return {"sm_mhz": float(np.median(sm)) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.rows)}
+
+
+def measured_hbm_peak():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        try:
+            return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+        except Exception:
+            pass
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+def cpu_sample(n_sample: int):
+    """The oracle's mixed solve on C_{n_sample} x 70 (one host thread)."""
+    from lfric_core_b200.problems import helmholtz_problem
+    from oracle.oracle import Helmholtz as OraHelm
+    p = helmholtz_problem(n_sample, NLAYERS, seed=SEED, mg_levels=MG_LEVELS)
+    ora = OraHelm(p)
+    t0 = time.perf_counter()
+    _, st, info = ora.mixed_solve(p.rhs)
+    dt = time.perf_counter() - t0
+    return dt, st, info
+
+
+def run_reference(args, rank, world):
+    """CPU reference arm: rank 0 alone times the oracle on the host cores."""
+    if rank != 0:
+        return
+    n_sample = max(24, args.n // 2)
+    scale = (n_sample / args.n) ** 2          # solve cost scales with the dof count
+    for _ in range(args.warmup):
+        cpu_sample(n_sample)
+    times = []
+    for _ in range(args.steps):
+        dt, st, info = cpu_sample(n_sample)
+        times.append(dt)
+    t = float(np.sum(times))
+    value = args.steps * scale / t
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1e3 * t / args.steps / scale, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
+        "config": {"workload": f"helmholtz_c{args.n}x{NLAYERS}_gcr10_mg{MG_LEVELS}_mixed_to_1e-8",
+                   "sample": f"C{n_sample}x{NLAYERS}"},
+        "cpu_baseline": {"value": value, "unit": "solves/s", "cores": 1, "kind": "port",
+                         "sample": f"one full mixed solve per step on C{n_sample}x{NLAYERS} "
+                                   f"(the C oracle, one thread), throughput scaled to "
+                                   f"C{args.n} by the dof ratio {scale:.4f}"},
+        "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse()
+    rank, world, local = dist_env()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import torch
+    if world > 1:
+        import torch.distributed as dist
+        from datetime import timedelta
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+    else:
+        torch.cuda.set_device(0)
+    dev = torch.cuda.current_device()
+
+    from lfric_core_b200 import api
+    from lfric_core_b200.problems import helmholtz_problem
+
+    prob = helmholtz_problem(args.n, NLAYERS, seed=SEED + rank, mg_levels=MG_LEVELS)
+    ctx = api.Context(dev)
+    stream = torch.cuda.current_stream()
+    ctx.set_stream(stream.cuda_stream)
+    system = api.HelmholtzSystem(ctx, prob)
+    system.b64.import_(prob.rhs)
+    N = prob.ndof
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            torch.distributed.barrier()
+            torch.cuda.synchronize()
+
+    def timed(fn, steps):
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        n0 = ctx.kernel_launches()
+        e0.record(stream)
+        last = None
+        for _ in range(steps):
+            last = fn()
+        e1.record(stream)
+        barrier()
+        ms = e0.elapsed_time(e1)
+        if world > 1:
+            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            ms = float(t.item())
+        return ms, ctx.kernel_launches() - n0, last
+
+    # ---- warm-up (both forms)
+    for _ in range(args.warmup):
+        system.solve_mixed()
+        system.solve_fp64()
+
+    # ---- mixed (headline, device-resident inputs)
+    with ClockSampler(dev) as clk:
+        ms_mixed, launches, res_m = timed(system.solve_mixed, args.steps)
+    # ---- plain FP64 drop-in
+    ms_fp64, launches64, res_64 = timed(system.solve_fp64, args.steps)
+
+    # ---- e2e through the ABI with host buffers (pinned)
+    b_host = torch.from_numpy(prob.rhs.astype(np.float64)).pin_memory()
+    x_host = torch.empty(N, dtype=torch.float64).pin_memory()
+    b_np, x_np = b_host.numpy(), x_host.numpy()
+
+    def e2e_step():
+        system.b64.import_(b_np)
+        r = system.mixed.apply(system.x64, system.b64)
+        system.x64.export_into(x_np)
+        return r
+
+    for _ in range(1):
+        e2e_step()
+    ms_e2e, _, _ = timed(e2e_step, args.steps)
+
+    # true residual of the last mixed solve, in FP64 on the device
+    system.solve_mixed()
+    R = system.op64.field()
+    system.op64.apply(R, system.x64)
+    R.aypx(-1.0, system.b64)
+    true_rel = R.norm() / system.b64.norm()
+
+    # ---- roofline of the dominant kernel: the fused FP32 column smoother
+    op32 = system.levels32[0]
+    xs, bs, ys = op32.field(), op32.field(), op32.field()
+    xs.copy(system.x64)
+    bs.copy(system.b64)
+    nrep = 20
+    for _ in range(3):
+        op32.smooth(0.8, xs, bs, ys)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for i in range(nrep):
+        op32.smooth(0.8, xs if i % 2 == 0 else ys, bs, ys if i % 2 == 0 else xs)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    smooth_ms = e0.elapsed_time(e1) / nrep
+    smooth_bytes = 10 * N * 4          # x, b, 3 bands, 4 couplings read; x_out written
+    peak, peak_kind = measured_hbm_peak()
+    achieved = smooth_bytes / (smooth_ms * 1e-3) / 1e9
+
+    # ---- CPU baseline (rank 0, N=1 only): the oracle on a bounded sample
+    cpu = None
+    if rank == 0 and world == 1:
+        n_sample = max(24, args.n // 2)
+        scale = (n_sample / args.n) ** 2
+        dt, st, info = cpu_sample(n_sample)
+        cpu = {"value": scale / dt, "unit": "solves/s", "cores": 1, "kind": "port",
+               "sample": f"one mixed solve on C{n_sample}x{NLAYERS} with the C oracle on one "
+                         f"host thread ({dt:.2f} s), scaled to C{args.n} by the dof ratio "
+                         f"{scale:.4f}"}
+
+    value = world * args.steps / (ms_mixed * 1e-3)
+    fp64_value = world * args.steps / (ms_fp64 * 1e-3)
+    e2e_value = world * args.steps / (ms_e2e * 1e-3)
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "solves/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_mixed / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32+f64", "data": "synthetic",
+            "config": {"workload": f"helmholtz_c{args.n}x{NLAYERS}_gcr10_mg{MG_LEVELS}_mixed_to_1e-8",
+                       "ndof": N, "mg": "C192/96/48/24 block-Jacobi column smoother 2+2, 8 coarse",
+                       "parallelism": f"replicas x{world}",
+                       "l2": "inputs larger than L2 (FP64 operator 0.87 GB, FP32 0.43 GB)"},
+            "fp64": {"value": fp64_value, "unit": "solves/s", "ms_per_step": ms_fp64 / args.steps,
+                     "iterations": res_64.iterations, "final_err": res_64.final_err,
+                     "gpu_launches": launches64},
+            "mixed_over_fp64": value / fp64_value,
+            "mixed": {"outer": res_m.outer_iterations, "inner": res_m.inner_iterations,
+                      "rel_residual": res_m.rel_residual, "true_rel_residual": true_rel},
+            "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": N * 8,
+                    "d2h_bytes_per_step": N * 8},
+            "gpu_launches": launches,
+            "roofline": {"bound": "hbm", "kernel": "k_helm_smooth<float> (C192x70 fine level)",
+                         "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "peak_source": peak_kind,
+                         "traffic": None, "algorithmic_bytes": smooth_bytes,
+                         "ms_per_launch": smooth_ms},
+            "cpu_baseline": cpu,
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

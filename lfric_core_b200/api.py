@@ -1,0 +1,521 @@
+"""Python front end of the C ABI (include/lfg.h).
+
+Each class owns one ABI handle and mirrors a reference type:
+
+  Field              field_type data + abstract_vector_type algebra
+                     (infrastructure/source/field/vector_mod.F90:17-189)
+  ColumnwiseOperator columnwise_operator_type (operator/columnwise_operator_mod.f90)
+  LocalOperator      operator_type LMA (operator/operator_mod.t90)
+  Helmholtz          the project-defined W3 Helmholtz operator
+  LinearOperator     abstract_linear_operator_type (solver/sci_linear_operator_mod.f90)
+  Preconditioner     abstract_preconditioner_type (solver/sci_preconditioner_mod.f90)
+  IterativeSolver    abstract_iterative_solver_type and its solvers
+                     (solver/sci_iterative_solver_mod.f90)
+
+Errors come back as LfgError carrying the ABI status; the solver's
+NOT_CONVERGED / NAN statuses are returned, not raised, as the reference's
+fail_on_non_converged decides what is fatal.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import _lib
+from ._lib import lfg_solver_cfg
+
+R_SINGLE, R_DOUBLE = 4, 8
+OK, NOT_CONVERGED, NAN_STATUS = 0, 1, 2
+LMA_INC, LMA_WRITE, LMA_TRANSPOSE = 0, 1, 2
+RESTRICT_UNWEIGHTED, RESTRICT_WEIGHTED, RESTRICT_MASS_W3 = 0, 1, 2
+SOLVERS = {"cg": 0, "gcr": 1, "jacobi": 2, "chebyshev": 3, "precondition_only": 4,
+           "bicgstab": 5, "gmres": 6, "fgmres": 7}
+
+
+class LfgError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"[status {status}] {message}")
+        self.status = status
+
+
+def _kind_of(dtype) -> int:
+    dt = np.dtype(dtype)
+    if dt == np.float64:
+        return R_DOUBLE
+    if dt == np.float32:
+        return R_SINGLE
+    raise TypeError(f"unsupported dtype {dt}")
+
+
+def _dtype_of(kind: int):
+    return np.float64 if kind == R_DOUBLE else np.float32
+
+
+def _iptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_int))
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(C.POINTER(C.c_double))
+
+
+class Context:
+    """One CUDA device and stream; owns every device buffer made through it."""
+
+    def __init__(self, device: int = 0):
+        self.lib = _lib.load()
+        h = C.c_void_p()
+        st = self.lib.lfg_ctx_create(device, C.byref(h))
+        if st != OK:
+            raise LfgError(st, "lfg_ctx_create failed (is a CUDA device present?)")
+        self.h = h
+
+    def check(self, status: int, what: str = "") -> int:
+        if status not in (OK,):
+            msg = self.lib.lfg_last_error(self.h).decode()
+            raise LfgError(status, f"{what}: {msg}" if what else msg)
+        return status
+
+    def synchronize(self):
+        self.check(self.lib.lfg_ctx_synchronize(self.h), "synchronize")
+
+    def set_stream(self, stream_ptr: int | None):
+        self.check(self.lib.lfg_ctx_set_stream(self.h, C.c_void_p(stream_ptr or 0)), "set_stream")
+
+    def kernel_launches(self) -> int:
+        n = C.c_uint64()
+        self.check(self.lib.lfg_ctx_kernel_launches(self.h, C.byref(n)))
+        return n.value
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.lfg_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class _Handle:
+    _destroy = None
+
+    def __init__(self, ctx: Context, h, keep=()):
+        self.ctx, self.h, self._keep = ctx, h, list(keep)
+
+    def close(self):
+        if getattr(self, "h", None) and self._destroy:
+            getattr(self.ctx.lib, self._destroy)(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class Field(_Handle):
+    """A column field: ncol entities x nlev levels, level-major on the device."""
+
+    _destroy = "lfg_field_destroy"
+
+    def __init__(self, ctx: Context, kind: int, ncol: int, nlev: int, device_ptr: int | None = None,
+                 keep=()):
+        h = C.c_void_p()
+        if device_ptr is None:
+            ctx.check(ctx.lib.lfg_field_create(ctx.h, kind, ncol, nlev, C.byref(h)), "field_create")
+        else:
+            ctx.check(ctx.lib.lfg_field_wrap(ctx.h, kind, ncol, nlev, C.c_void_p(device_ptr),
+                                             C.byref(h)), "field_wrap")
+        super().__init__(ctx, h, keep)
+        self.kind, self.ncol, self.nlev = kind, ncol, nlev
+
+    @property
+    def size(self) -> int:
+        return self.ncol * self.nlev
+
+    def device_ptr(self) -> int:
+        p = C.c_void_p()
+        self.ctx.check(self.ctx.lib.lfg_field_device_ptr(self.h, C.byref(p)))
+        return p.value
+
+    def import_(self, data: np.ndarray) -> "Field":
+        """Copy a host array in the reference's column-contiguous order in."""
+        a = np.ascontiguousarray(data)
+        if a.size != self.size:
+            raise ValueError(f"import: {a.size} values for a field of {self.size}")
+        self.ctx.check(self.ctx.lib.lfg_field_import(self.h, a.ctypes.data_as(C.c_void_p),
+                                                     _kind_of(a.dtype)), "field_import")
+        return self
+
+    def export(self, dtype=None) -> np.ndarray:
+        dt = np.dtype(dtype or _dtype_of(self.kind))
+        out = np.empty(self.size, dtype=dt)
+        self.ctx.check(self.ctx.lib.lfg_field_export(self.h, out.ctypes.data_as(C.c_void_p),
+                                                     _kind_of(dt)), "field_export")
+        return out
+
+    def export_into(self, out: np.ndarray) -> np.ndarray:
+        self.ctx.check(self.ctx.lib.lfg_field_export(self.h, out.ctypes.data_as(C.c_void_p),
+                                                     _kind_of(out.dtype)), "field_export")
+        return out
+
+    # abstract_vector_type bindings (vector_mod.F90:17-59)
+    def set_scalar(self, a: float):
+        self.ctx.check(self.ctx.lib.lfg_setval_c(self.h, a), "setval_c")
+
+    def copy(self, src: "Field"):
+        self.ctx.check(self.ctx.lib.lfg_setval_X(self.h, src.h), "setval_X")
+
+    def axpy(self, alpha: float, x: "Field"):      # self = self + alpha x
+        self.ctx.check(self.ctx.lib.lfg_inc_X_plus_bY(self.h, alpha, x.h), "inc_X_plus_bY")
+
+    def aypx(self, alpha: float, x: "Field"):      # self = alpha self + x
+        self.ctx.check(self.ctx.lib.lfg_inc_aX_plus_Y(alpha, self.h, x.h), "inc_aX_plus_Y")
+
+    def axpby(self, a: float, x: "Field", b: float, y: "Field"):  # self = a x + b y
+        self.ctx.check(self.ctx.lib.lfg_aX_plus_bY(self.h, a, x.h, b, y.h), "aX_plus_bY")
+
+    def scale(self, a: float):
+        self.ctx.check(self.ctx.lib.lfg_inc_a_times_X(a, self.h), "inc_a_times_X")
+
+    def divide(self, x: "Field", y: "Field"):      # self = x / y
+        self.ctx.check(self.ctx.lib.lfg_X_divideby_Y(self.h, x.h, y.h), "X_divideby_Y")
+
+    def dot(self, x: "Field") -> float:
+        r = C.c_double()
+        self.ctx.check(self.ctx.lib.lfg_X_innerproduct_Y(self.h, x.h, C.byref(r)), "innerproduct")
+        return r.value
+
+    def norm(self) -> float:
+        r = C.c_double()
+        self.ctx.check(self.ctx.lib.lfg_X_innerproduct_X(self.h, C.byref(r)), "innerproduct")
+        return float(np.sqrt(r.value))
+
+    def duplicate(self) -> "Field":
+        return Field(self.ctx, self.kind, self.ncol, self.nlev)
+
+
+def field_from(ctx: Context, data: np.ndarray, ncol: int, nlev: int, kind: int | None = None) -> Field:
+    kind = kind or _kind_of(np.asarray(data).dtype)
+    return Field(ctx, kind, ncol, nlev).import_(data)
+
+
+class Mesh(_Handle):
+    _destroy = "lfg_mesh_destroy"
+
+    def __init__(self, ctx: Context, links: np.ndarray):
+        links = np.ascontiguousarray(links, dtype=np.int32)
+        h = C.c_void_p()
+        ctx.check(ctx.lib.lfg_mesh_create(ctx.h, links.shape[0], _iptr(links), C.byref(h)),
+                  "mesh_create")
+        super().__init__(ctx, h)
+        self.ncol = links.shape[0]
+
+
+class Intergrid(_Handle):
+    """cell_map: (ncoarse, ny, nx) fine cells of each coarse cell (0-based)."""
+
+    _destroy = "lfg_intergrid_destroy"
+
+    def __init__(self, ctx: Context, cell_map: np.ndarray, nfine: int,
+                 coarse_corners: np.ndarray | None = None, fine_corners: np.ndarray | None = None):
+        cm = np.ascontiguousarray(cell_map, dtype=np.int32)
+        ncoarse, ny, nx = cm.shape
+        cc = None if coarse_corners is None else np.ascontiguousarray(coarse_corners, dtype=np.int32)
+        fc = None if fine_corners is None else np.ascontiguousarray(fine_corners, dtype=np.int32)
+        h = C.c_void_p()
+        ctx.check(ctx.lib.lfg_intergrid_create(
+            ctx.h, ncoarse, nfine, nx, ny, _iptr(cm), None if cc is None else _iptr(cc),
+            None if fc is None else _iptr(fc), C.byref(h)), "intergrid_create")
+        super().__init__(ctx, h)
+        self.ncoarse, self.nfine, self.nx, self.ny = ncoarse, nfine, nx, ny
+
+    def restrict(self, mode: int, coarse: Field, fine: Field, weights: Field | None = None):
+        self.ctx.check(self.ctx.lib.lfg_restrict_scalar(self.h, mode, coarse.h, fine.h,
+                                                        None if weights is None else weights.h),
+                       "restrict_scalar")
+
+    def prolong(self, fine: Field, coarse: Field, weights: Field | None = None):
+        self.ctx.check(self.ctx.lib.lfg_prolong_scalar(self.h, fine.h, coarse.h,
+                                                       None if weights is None else weights.h),
+                       "prolong_scalar")
+
+    def restrict_w0(self, coarse: Field, fine: Field):
+        self.ctx.check(self.ctx.lib.lfg_restrict_w0(self.h, coarse.h, fine.h), "restrict_w0")
+
+    def prolong_w0(self, fine: Field, coarse: Field):
+        self.ctx.check(self.ctx.lib.lfg_prolong_w0(self.h, fine.h, coarse.h), "prolong_w0")
+
+
+class ColumnwiseOperator(_Handle):
+    """columnwise_operator_type: columnwise_matrix(bw, nrow, ncol) Fortran order."""
+
+    _destroy = "lfg_cma_destroy"
+
+    def __init__(self, ctx: Context, kind: int, ncol: int, nrow: int, ncolumn: int, bandwidth: int,
+                 alpha: int, beta: int, gamma_m: int, gamma_p: int, ind_to, ind_from,
+                 columnwise_matrix: np.ndarray):
+        it = np.ascontiguousarray(ind_to, dtype=np.int32)
+        iff = np.ascontiguousarray(ind_from, dtype=np.int32)
+        cm = np.ascontiguousarray(columnwise_matrix, dtype=np.float64).ravel()
+        h = C.c_void_p()
+        ctx.check(ctx.lib.lfg_cma_create(ctx.h, kind, ncol, nrow, ncolumn, bandwidth, alpha,
+                                         beta, gamma_m, gamma_p, _iptr(it), _iptr(iff),
+                                         _dptr(cm), C.byref(h)), "cma_create")
+        super().__init__(ctx, h)
+        self.kind, self.ncol, self.nrow, self.ncolumn = kind, ncol, nrow, ncolumn
+
+    def apply(self, lhs: Field, x: Field):           # lhs += A x
+        self.ctx.check(self.ctx.lib.lfg_cma_apply(self.h, lhs.h, x.h), "cma_apply")
+
+    def apply_inverse(self, lhs: Field, x: Field):   # lhs = A^{-1} x
+        self.ctx.check(self.ctx.lib.lfg_cma_apply_inverse(self.h, lhs.h, x.h), "cma_apply_inverse")
+
+
+def tri_solve(y: Field, x: Field, tri_0: Field, tri_plus: Field, tri_minus: Field):
+    y.ctx.check(y.ctx.lib.lfg_tri_solve(y.h, x.h, tri_0.h, tri_plus.h, tri_minus.h), "tri_solve")
+
+
+class LocalOperator(_Handle):
+    """operator_type LMA: local_stencil(ncell*nlayers, ndf_to, ndf_from), Fortran order."""
+
+    _destroy = "lfg_lma_destroy"
+
+    def __init__(self, ctx: Context, kind: int, ncell: int, nlayers: int, local_stencil: np.ndarray,
+                 map_to: np.ndarray, nent_to: int, nlev_to: int,
+                 map_from: np.ndarray | None = None, nent_from: int | None = None,
+                 nlev_from: int | None = None):
+        mt = np.ascontiguousarray(map_to, dtype=np.int32)
+        mf = mt if map_from is None else np.ascontiguousarray(map_from, dtype=np.int32)
+        nent_from = nent_to if nent_from is None else nent_from
+        nlev_from = nlev_to if nlev_from is None else nlev_from
+        ndf_to, ndf_from = mt.shape[1], mf.shape[1]
+        ls = np.ascontiguousarray(local_stencil, dtype=np.float64).ravel()
+        h = C.c_void_p()
+        ctx.check(ctx.lib.lfg_lma_create(ctx.h, kind, ncell, nlayers, ndf_to, ndf_from, _dptr(ls),
+                                         _iptr(mt), nent_to, nlev_to, _iptr(mf), nent_from,
+                                         nlev_from, C.byref(h)), "lma_create")
+        super().__init__(ctx, h)
+        self.kind, self.ncell, self.nlayers = kind, ncell, nlayers
+        self.ndf_to, self.ndf_from = ndf_to, ndf_from
+        self.nent_to, self.nlev_to, self.nent_from, self.nlev_from = nent_to, nlev_to, nent_from, nlev_from
+
+    def set_values(self, local_stencil: np.ndarray):
+        ls = np.ascontiguousarray(local_stencil, dtype=np.float64).ravel()
+        self.ctx.check(self.ctx.lib.lfg_lma_set_values(self.h, _dptr(ls)), "lma_set_values")
+
+    def apply(self, mode: int, lhs: Field, x: Field):
+        self.ctx.check(self.ctx.lib.lfg_lma_apply(self.h, mode, lhs.h, x.h), "lma_apply")
+
+    def diagonal(self, diag: Field):
+        self.ctx.check(self.ctx.lib.lfg_lma_diagonal(self.h, diag.h), "lma_diagonal")
+
+    def operator_tri_solve(self, y: Field, x: Field):
+        self.ctx.check(self.ctx.lib.lfg_operator_tri_solve(self.h, y.h, x.h), "operator_tri_solve")
+
+    def combine(self, m: "LocalOperator", k: "LocalOperator", kappa: Field):
+        self.ctx.check(self.ctx.lib.lfg_lma_combine(self.h, m.h, k.h, kappa.h), "lma_combine")
+
+    def bilinear(self, u: Field, v: Field, scale: float, g: Field):
+        self.ctx.check(self.ctx.lib.lfg_lma_bilinear(self.h, u.h, v.h, scale, g.h), "lma_bilinear")
+
+
+class Helmholtz(_Handle):
+    _destroy = "lfg_helm_destroy"
+
+    def __init__(self, ctx: Context, kind: int, mesh: Mesh, nlayers: int, cm=None, hf=None,
+                 handle=None, keep=()):
+        if handle is None:
+            cm = np.ascontiguousarray(cm, dtype=np.float64).ravel()
+            hf = np.ascontiguousarray(hf, dtype=np.float64).ravel()
+            handle = C.c_void_p()
+            ctx.check(ctx.lib.lfg_helm_create(ctx.h, kind, mesh.h, nlayers, _dptr(cm), _dptr(hf),
+                                              C.byref(handle)), "helm_create")
+        super().__init__(ctx, handle, [mesh, *keep])
+        self.kind, self.mesh, self.nlayers, self.ncol = kind, mesh, nlayers, mesh.ncol
+
+    def apply(self, y: Field, x: Field):
+        self.ctx.check(self.ctx.lib.lfg_helm_apply(self.h, y.h, x.h), "helm_apply")
+
+    def smooth(self, omega: float, x_in: Field | None, b: Field, x_out: Field):
+        self.ctx.check(self.ctx.lib.lfg_helm_smooth(self.h, omega, None if x_in is None else x_in.h,
+                                                    b.h, x_out.h), "helm_smooth")
+
+    def coarsen(self, ig: Intergrid, coarse_mesh: Mesh, kind: int) -> "Helmholtz":
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.lfg_helm_coarsen(self.h, ig.h, coarse_mesh.h, kind, C.byref(h)),
+                       "helm_coarsen")
+        return Helmholtz(self.ctx, kind, coarse_mesh, self.nlayers, handle=h)
+
+    def copy_kind(self, kind: int) -> "Helmholtz":
+        h = C.c_void_p()
+        self.ctx.check(self.ctx.lib.lfg_helm_copy_kind(self.h, kind, C.byref(h)), "helm_copy_kind")
+        return Helmholtz(self.ctx, kind, self.mesh, self.nlayers, handle=h)
+
+    def field(self, data=None) -> Field:
+        f = Field(self.ctx, self.kind, self.ncol, self.nlayers)
+        if data is not None:
+            f.import_(data)
+        return f
+
+
+class LinearOperator(_Handle):
+    _destroy = "lfg_linop_destroy"
+
+    @classmethod
+    def from_helmholtz(cls, op: Helmholtz) -> "LinearOperator":
+        h = C.c_void_p()
+        op.ctx.check(op.ctx.lib.lfg_linop_from_helm(op.h, C.byref(h)), "linop_from_helm")
+        return cls(op.ctx, h, [op])
+
+    @classmethod
+    def from_lma(cls, op: LocalOperator) -> "LinearOperator":
+        h = C.c_void_p()
+        op.ctx.check(op.ctx.lib.lfg_linop_from_lma(op.h, C.byref(h)), "linop_from_lma")
+        return cls(op.ctx, h, [op])
+
+    def apply(self, x: Field, y: Field):
+        self.ctx.check(self.ctx.lib.lfg_linop_apply(self.h, x.h, y.h), "linop_apply")
+
+
+class Preconditioner(_Handle):
+    _destroy = "lfg_prec_destroy"
+
+    @classmethod
+    def null(cls, ctx: Context) -> "Preconditioner":
+        h = C.c_void_p()
+        ctx.check(ctx.lib.lfg_prec_null(ctx.h, C.byref(h)), "prec_null")
+        return cls(ctx, h)
+
+    @classmethod
+    def diagonal(cls, diag: Field) -> "Preconditioner":
+        h = C.c_void_p()
+        diag.ctx.check(diag.ctx.lib.lfg_prec_diagonal(diag.h, C.byref(h)), "prec_diagonal")
+        return cls(diag.ctx, h, [diag])
+
+    @classmethod
+    def multigrid(cls, levels: list, maps: list, n_pre=2, n_post=2, n_coarse=8,
+                  omega=0.8) -> "Preconditioner":
+        ctx = levels[0].ctx
+        lv = (C.c_void_p * len(levels))(*[l.h.value for l in levels])
+        mp = (C.c_void_p * max(1, len(maps)))(*[m.h.value for m in maps])
+        h = C.c_void_p()
+        ctx.check(ctx.lib.lfg_prec_multigrid(len(levels), C.cast(lv, C.POINTER(C.c_void_p)),
+                                             C.cast(mp, C.POINTER(C.c_void_p)), n_pre, n_post,
+                                             n_coarse, omega, C.byref(h)), "prec_multigrid")
+        return cls(ctx, h, [*levels, *maps])
+
+    def apply(self, x: Field, y: Field):
+        self.ctx.check(self.ctx.lib.lfg_prec_apply(self.h, x.h, y.h), "prec_apply")
+
+
+@dataclass
+class SolveResult:
+    status: int
+    iterations: int
+    final_err: float
+
+
+class IterativeSolver(_Handle):
+    """abstract_iterative_solver_type; method one of SOLVERS."""
+
+    _destroy = "lfg_solver_destroy"
+
+    def __init__(self, lin_op: LinearOperator, prec: Preconditioner, like: Field, method: str,
+                 r_tol=1e-8, a_tol=0.0, max_iter=100, monitor_convergence=True,
+                 fail_on_non_converged=True, gcrk=10, rho_relax=1.0, lmin=0.0, lmax=1.0):
+        cfg = lfg_solver_cfg(SOLVERS[method], gcrk, r_tol, a_tol, max_iter,
+                             int(monitor_convergence), int(fail_on_non_converged), rho_relax,
+                             lmin, lmax)
+        h = C.c_void_p()
+        ctx = lin_op.ctx
+        ctx.check(ctx.lib.lfg_solver_create(lin_op.h, prec.h, C.byref(cfg), like.h, C.byref(h)),
+                  "solver_create")
+        super().__init__(ctx, h, [lin_op, prec])
+        self.method, self.kind = method, like.kind
+
+    def apply(self, x: Field, b: Field) -> SolveResult:
+        it, err = C.c_int(), C.c_double()
+        st = self.ctx.lib.lfg_solver_apply(self.h, x.h, b.h, C.byref(it), C.byref(err))
+        if st not in (OK, NOT_CONVERGED, NAN_STATUS):
+            self.ctx.check(st, "solver_apply")
+        return SolveResult(st, it.value, err.value)
+
+
+@dataclass
+class MixedResult:
+    status: int
+    outer_iterations: int
+    inner_iterations: int
+    rel_residual: float
+
+
+class MixedSolver(_Handle):
+    _destroy = "lfg_mixed_destroy"
+
+    def __init__(self, op64: Helmholtz, inner: IterativeSolver, tol=1e-8, max_outer=10):
+        h = C.c_void_p()
+        op64.ctx.check(op64.ctx.lib.lfg_mixed_create(op64.h, inner.h, tol, max_outer, C.byref(h)),
+                       "mixed_create")
+        super().__init__(op64.ctx, h, [op64, inner])
+
+    def apply(self, x: Field, b: Field) -> MixedResult:
+        o, i, r = C.c_int(), C.c_int(), C.c_double()
+        st = self.ctx.lib.lfg_mixed_apply(self.h, x.h, b.h, C.byref(o), C.byref(i), C.byref(r))
+        if st not in (OK, NOT_CONVERGED, NAN_STATUS):
+            self.ctx.check(st, "mixed_apply")
+        return MixedResult(st, o.value, i.value, r.value)
+
+
+class HelmholtzSystem:
+    """Device-resident Helmholtz problem: operators of every multigrid level
+    (Galerkin, built on the device), FP64 and FP32 V-cycles, the FP64
+    GCR(k) solver and the mixed-precision refinement solver."""
+
+    def __init__(self, ctx: Context, prob, gcrk=10, tol=1e-8, max_iter=20, n_pre=2, n_post=2,
+                 n_coarse=8, omega=0.8, inner_tol=1e-4, inner_max_iter=2, max_outer=10,
+                 mixed=True, fp64=True):
+        self.ctx, self.prob = ctx, prob
+        nl = prob.nlayers
+        self.meshes = [Mesh(ctx, prob.links)] + [Mesh(ctx, l) for l in prob.mg_links]
+        self.maps = [Intergrid(ctx, ch, self.meshes[i].ncol) for i, ch in enumerate(prob.mg_child)]
+        op64 = Helmholtz(ctx, R_DOUBLE, self.meshes[0], nl, prob.cm, prob.hf)
+        self.levels64 = [op64]
+        for i, ig in enumerate(self.maps):
+            self.levels64.append(self.levels64[-1].coarsen(ig, self.meshes[i + 1], R_DOUBLE))
+        self.op64 = op64
+        mgkw = dict(n_pre=n_pre, n_post=n_post, n_coarse=n_coarse, omega=omega)
+        self.b64 = Field(ctx, R_DOUBLE, op64.ncol, nl)
+        self.x64 = Field(ctx, R_DOUBLE, op64.ncol, nl)
+        if fp64:
+            self.mg64 = Preconditioner.multigrid(self.levels64, self.maps, **mgkw)
+            self.gcr64 = IterativeSolver(LinearOperator.from_helmholtz(op64), self.mg64, self.x64,
+                                         "gcr", r_tol=tol, max_iter=max_iter, gcrk=gcrk)
+        if mixed:
+            self.levels32 = [l.copy_kind(R_SINGLE) for l in self.levels64]
+            self.mg32 = Preconditioner.multigrid(self.levels32, self.maps, **mgkw)
+            like32 = Field(ctx, R_SINGLE, op64.ncol, nl)
+            self.gcr32 = IterativeSolver(LinearOperator.from_helmholtz(self.levels32[0]), self.mg32,
+                                         like32, "gcr", r_tol=inner_tol, max_iter=inner_max_iter,
+                                         gcrk=gcrk, fail_on_non_converged=False)
+            self.mixed = MixedSolver(op64, self.gcr32, tol=tol, max_outer=max_outer)
+
+    def solve_fp64(self, b: np.ndarray | None = None) -> SolveResult:
+        if b is not None:
+            self.b64.import_(b)
+        self.x64.set_scalar(0.0)
+        return self.gcr64.apply(self.x64, self.b64)
+
+    def solve_mixed(self, b: np.ndarray | None = None) -> MixedResult:
+        if b is not None:
+            self.b64.import_(b)
+        return self.mixed.apply(self.x64, self.b64)
+
+    def solution(self) -> np.ndarray:
+        return self.x64.export(np.float64)

@@ -1,0 +1,643 @@
+// Columnwise-assembled (CMA) operators, the Thomas column solves and the
+// intergrid transfers.
+//
+// Drop-ins for the reference kernels (components/science/source/kernel/):
+//   columnwise_operators/sci_columnwise_op_app_kernel_mod.F90:73-124     (lfg_cma_apply)
+//   columnwise_operators/sci_columnwise_op_appinv_kernel_mod.F90:77-145  (lfg_cma_apply_inverse)
+//   solver/sci_tri_solve_kernel_mod.f90:116-156                          (lfg_tri_solve)
+//   solver/sci_operator_tri_solve_kernel_mod.f90:69-120                  (lfg_operator_tri_solve)
+//   inter_mesh/sci_restrict_scalar_{unweighted,weighted}_kernel_mod.F90,
+//   inter_mesh/sci_restrict_mass_w3_kernel_mod.F90,
+//   inter_mesh/sci_prolong_scalar_{unweighted,weighted}_kernel_mod.F90,
+//   inter_mesh/sci_restrict_w0_kernel_mod.F90, sci_prolong_w0_kernel_mod.F90.
+// The reference calls each once per column from the PSy layer; here one
+// launch covers the mesh and one thread owns a column (or a coarse column).
+#include "lfg_internal.cuh"
+
+#include <algorithm>
+
+using namespace lfg;
+
+namespace {
+
+// ------------------------------------------------------------- Thomas
+// Source of the tridiagonal rows and of the right-hand side of one column.
+enum { SRC_CMA = 0, SRC_FIELDS = 1, SRC_LMA2 = 2 };
+
+template <class T>
+struct TriSrc {
+  int ncol, nrow;
+  const T* __restrict__ bands;  // CMA [3][nrow][ncol]; LMA2 [2][2][nl][ncol]
+  const T* __restrict__ t0;     // fields: tri_0, tri_plus, tri_minus [nrow][ncol]
+  const T* __restrict__ tp;
+  const T* __restrict__ tm;
+  const int* __restrict__ ind;  // CMA: 0-based dof offset of each row
+  int nl;                       // LMA2: number of layers (nrow = nl + 1)
+};
+
+template <class T, int SRC>
+__device__ __forceinline__ void tri_row(const TriSrc<T>& s, int k, int c, T& a1, T& a2, T& a3) {
+  const size_t N = s.ncol;
+  if (SRC == SRC_CMA) {
+    const size_t plane = (size_t)s.nrow * N;
+    a1 = s.bands[(size_t)k * N + c];
+    a2 = s.bands[plane + (size_t)k * N + c];
+    a3 = s.bands[2 * plane + (size_t)k * N + c];
+  } else if (SRC == SRC_FIELDS) {
+    a1 = s.tm[(size_t)k * N + c];
+    a2 = s.t0[(size_t)k * N + c];
+    a3 = s.tp[(size_t)k * N + c];
+  } else {
+    // 2x2 LMA M(layer, i, j) at bands[((i*2+j)*nl + layer)*N + c]
+    const size_t lay = (size_t)s.nl * N;
+    const T m11 = k < s.nl ? s.bands[0 * lay + (size_t)k * N + c] : (T)0;
+    const T m22 = k > 0 ? s.bands[3 * lay + (size_t)(k - 1) * N + c] : (T)0;
+    a2 = m11 + m22;
+    a3 = k < s.nl ? s.bands[1 * lay + (size_t)k * N + c] : (T)0;
+    a1 = k > 0 ? s.bands[2 * lay + (size_t)(k - 1) * N + c] : (T)0;
+  }
+}
+
+template <class T, int SRC>
+__device__ __forceinline__ size_t tri_dof(const TriSrc<T>& s, int k) {
+  return SRC == SRC_CMA ? (size_t)s.ind[k] : (size_t)k;
+}
+
+// lhs = A^{-1} x, one thread per column; c' in shared memory, d' in
+// registers (unrolled level loop).
+template <class T, int SRC, int MAXNL>
+__global__ void k_thomas(TriSrc<T> s, const T* __restrict__ x, T* __restrict__ lhs) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* cps = reinterpret_cast<T*>(smem_raw);
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= s.ncol) return;
+  const size_t N = s.ncol;
+  const int nrow = s.nrow, t = threadIdx.x, bs = blockDim.x;
+  T dp[MAXNL];
+  T cprev = (T)0, dprev = (T)0;
+#pragma unroll
+  for (int k = 0; k < MAXNL; ++k) {
+    if (k < nrow) {
+      T a1, a2, a3;
+      tri_row<T, SRC>(s, k, c, a1, a2, a3);
+      const T xv = x[tri_dof<T, SRC>(s, k) * N + c];
+      T inv, cpk, dpk;
+      if (k == 0) {
+        inv = (T)1 / a2;
+        cpk = inv * a3;
+        dpk = inv * xv;
+      } else {
+        inv = (T)1 / (a2 - a1 * cprev);
+        cpk = (k < nrow - 1) ? inv * a3 : (T)0;
+        dpk = inv * (xv - a1 * dprev);
+      }
+      cps[k * bs + t] = cpk;
+      dp[k] = dpk;
+      cprev = cpk;
+      dprev = dpk;
+    }
+  }
+  T znext = (T)0;
+#pragma unroll
+  for (int k = MAXNL - 1; k >= 0; --k) {
+    if (k < nrow) {
+      T z = dp[k];
+      if (k < nrow - 1) z = z - cps[k * bs + t] * znext;
+      znext = z;
+      lhs[tri_dof<T, SRC>(s, k) * N + c] = z;
+    }
+  }
+}
+
+// Same algorithm for columns taller than the unrolled variants: c' and d'
+// live in a global scratch array of 2*nrow*ncol values.
+template <class T, int SRC>
+__global__ void k_thomas_scratch(TriSrc<T> s, const T* __restrict__ x, T* __restrict__ lhs,
+                                 T* __restrict__ scratch) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= s.ncol) return;
+  const size_t N = s.ncol;
+  const int nrow = s.nrow;
+  T* cp = scratch;
+  T* dp = scratch + (size_t)nrow * N;
+  T cprev = (T)0, dprev = (T)0;
+  for (int k = 0; k < nrow; ++k) {
+    T a1, a2, a3;
+    tri_row<T, SRC>(s, k, c, a1, a2, a3);
+    const T xv = x[tri_dof<T, SRC>(s, k) * N + c];
+    T inv, cpk, dpk;
+    if (k == 0) {
+      inv = (T)1 / a2;
+      cpk = inv * a3;
+      dpk = inv * xv;
+    } else {
+      inv = (T)1 / (a2 - a1 * cprev);
+      cpk = (k < nrow - 1) ? inv * a3 : (T)0;
+      dpk = inv * (xv - a1 * dprev);
+    }
+    cp[(size_t)k * N + c] = cpk;
+    dp[(size_t)k * N + c] = dpk;
+    cprev = cpk;
+    dprev = dpk;
+  }
+  T znext = (T)0;
+  for (int k = nrow - 1; k >= 0; --k) {
+    T z = dp[(size_t)k * N + c];
+    if (k < nrow - 1) z = z - cp[(size_t)k * N + c] * znext;
+    znext = z;
+    lhs[tri_dof<T, SRC>(s, k) * N + c] = z;
+  }
+}
+
+int col_block(int ncol, int nsm) {
+  int per = (ncol + nsm - 1) / nsm;
+  int bs = ((per + 31) / 32) * 32;
+  return std::max(32, std::min(128, bs));
+}
+
+template <class T, int SRC, int MAXNL>
+void launch_thomas_t(lfg_ctx c, const TriSrc<T>& s, const T* x, T* lhs) {
+  const int bs = col_block(s.ncol, c->num_sms);
+  const size_t smem = (size_t)MAXNL * bs * sizeof(T);
+  auto kern = k_thomas<T, SRC, MAXNL>;
+  static bool attr = false;
+  if (!attr) {
+    LFG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)(MAXNL * 128 * sizeof(T))));
+    attr = true;
+  }
+  kern<<<(s.ncol + bs - 1) / bs, bs, smem, c->stream>>>(s, x, lhs);
+  after_launch(c, "thomas");
+}
+
+template <class T, int SRC>
+void launch_thomas(lfg_ctx c, const TriSrc<T>& s, const T* x, T* lhs) {
+  if (s.nrow <= 16) launch_thomas_t<T, SRC, 16>(c, s, x, lhs);
+  else if (s.nrow <= 32) launch_thomas_t<T, SRC, 32>(c, s, x, lhs);
+  else if (s.nrow <= 72) launch_thomas_t<T, SRC, 72>(c, s, x, lhs);
+  else {
+    T* scratch = (T*)c->scratch(2 * (size_t)s.nrow * s.ncol * sizeof(T));
+    const int bs = 128;
+    k_thomas_scratch<T, SRC><<<(s.ncol + bs - 1) / bs, bs, 0, c->stream>>>(s, x, lhs, scratch);
+    after_launch(c, "thomas_scratch");
+  }
+}
+
+// ------------------------------------------------------------- CMA apply
+// lhs(ind_to(i)) += sum_j band(j - j_minus(i), i) x(ind_from(j)), one thread
+// per (row, column); rows of one column are distinct dofs.
+template <class T>
+__global__ void k_cma_app(const T* __restrict__ bands, const int* __restrict__ ind_to,
+                          const int* __restrict__ ind_from, const int* __restrict__ jminus,
+                          const int* __restrict__ jplus, int ncol, int nrow, int ncolumn,
+                          const T* __restrict__ x, T* __restrict__ lhs) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y;
+  if (c >= ncol) return;
+  const size_t N = ncol, plane = (size_t)nrow * N;
+  const int jm = jminus[i];
+  const int jlo = max(0, jm), jhi = min(ncolumn - 1, jplus[i]);
+  const size_t o = (size_t)ind_to[i] * N + c;
+  T acc = lhs[o];
+  for (int j = jlo; j <= jhi; ++j)
+    acc = acc + bands[(size_t)(j - jm) * plane + (size_t)i * N + c] * x[(size_t)ind_from[j] * N + c];
+  lhs[o] = acc;
+}
+
+// ------------------------------------------------------------- intergrid
+// coarse(C,k) from the fine children, y outer and x inner (slot q = y*nx+x).
+template <class T, int MODE>
+__global__ void k_restrict(T* __restrict__ coarse, const T* __restrict__ fine,
+                           const T* __restrict__ w, const int* __restrict__ child, int ncoarse,
+                           int nfine, int nq, int nlev) {
+  const int C = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y;
+  if (C >= ncoarse || k >= nlev) return;
+  const T denom = (T)1 / (T)nq;
+  T acc = (T)0;
+  for (int q = 0; q < nq; ++q) {
+    const size_t i = (size_t)k * nfine + child[(size_t)q * ncoarse + C];
+    if (MODE == LFG_RESTRICT_UNWEIGHTED) acc = acc + fine[i] * denom;
+    else if (MODE == LFG_RESTRICT_WEIGHTED) acc = acc + fine[i] * denom / w[i];
+    else acc = acc + fine[i];
+  }
+  coarse[(size_t)k * ncoarse + C] = acc;
+}
+
+template <class T, bool WEIGHTED>
+__global__ void k_prolong(T* __restrict__ fine, const T* __restrict__ coarse,
+                          const T* __restrict__ w, const int* __restrict__ parent, int nfine,
+                          int ncoarse, int nlev) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y;
+  if (c >= nfine || k >= nlev) return;
+  const size_t i = (size_t)k * nfine + c;
+  const T cv = coarse[(size_t)k * ncoarse + parent[c]];
+  fine[i] = WEIGHTED ? fine[i] + w[i] * cv : fine[i] + cv;
+}
+
+// W0 injection: coarse vertex v takes the value of the coinciding fine vertex.
+template <class T>
+__global__ void k_restrict_w0(T* __restrict__ coarse, const T* __restrict__ fine,
+                              const int* __restrict__ inj, int nvc, int nvf, int nlev) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y;
+  if (v >= nvc || k >= nlev) return;
+  coarse[(size_t)k * nvc + v] = fine[(size_t)k * nvf + inj[v]];
+}
+
+// W0 bilinear prolongation: every fine vertex takes the value of the last
+// write the reference loop would make to it (coarse cell, four weights).
+template <class T>
+__global__ void k_prolong_w0(T* __restrict__ fine, const T* __restrict__ coarse,
+                             const int* __restrict__ src_cell, const double* __restrict__ wts,
+                             const int* __restrict__ ccorner, int nvf, int nvc, int ncoarse,
+                             int nlev) {
+  const int v = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y;
+  if (v >= nvf || k >= nlev) return;
+  const int C = src_cell[v];
+  if (C < 0) return;
+  const size_t ko = (size_t)k * nvc;
+  // weights stored NE, SE, SW, NW with a term count; corners SW,SE,NE,NW
+  const double* w = wts + (size_t)v * 5;
+  const int nterm = (int)w[4];
+  const T cne = coarse[ko + ccorner[2 * ncoarse + C]];
+  const T cse = coarse[ko + ccorner[1 * ncoarse + C]];
+  const T csw = coarse[ko + ccorner[0 * ncoarse + C]];
+  const T cnw = coarse[ko + ccorner[3 * ncoarse + C]];
+  T val;
+  if (nterm == 4) val = (T)w[0] * cne + (T)w[1] * cse + (T)w[2] * csw + (T)w[3] * cnw;
+  else if (nterm == 2) val = (T)w[0] * cne + (T)w[1] * cse;          // SE dof, last column
+  else if (nterm == 3) val = (T)w[0] * cne + (T)w[3] * cnw;          // NW dof, first row
+  else val = cne;                                                    // NE dof
+  fine[(size_t)k * nvf + v] = val;
+}
+
+template <class F>
+void dispatch(int kind, F&& f) {
+  if (kind == LFG_R_DOUBLE) f(double{});
+  else f(float{});
+}
+
+}  // namespace
+
+extern "C" {
+
+// ------------------------------------------------------------- CMA objects
+int lfg_cma_create(lfg_ctx c, int kind, int ncol, int nrow, int ncolumn, int bw, int alpha,
+                   int beta, int gamma_m, int gamma_p, const int* ind_to, const int* ind_from,
+                   const double* cm, lfg_cma* out) {
+  if (!c || !out) return LFG_ERR_ARG;
+  return guard(c, [&] {
+    LFG_REQUIRE(kind == LFG_R_DOUBLE || kind == LFG_R_SINGLE, "cma_create: bad kind");
+    LFG_REQUIRE(ncol > 0 && nrow > 0 && ncolumn > 0 && bw > 0 && beta > 0 && ind_to &&
+                    ind_from && cm,
+                "cma_create: bad arguments");
+    std::vector<int> it(nrow), iff(ncolumn), jm(nrow), jp(nrow);
+    for (int i = 0; i < nrow; ++i) {
+      LFG_REQUIRE(ind_to[i] >= 1, "cma_create: indirection maps are 1-based");
+      it[i] = ind_to[i] - 1;
+      // j_minus = ceiling((alpha*i - gamma_p)/beta) for the 1-based row i
+      const int row = i + 1;
+      const double q = (double)(alpha * row - gamma_p) / (double)beta;
+      jm[i] = (int)std::ceil(q) - 1;  // 0-based first column of the band
+      // j_plus = floor((alpha*i + gamma_m)/beta)
+      jp[i] = (int)std::floor((double)(alpha * row + gamma_m) / (double)beta) - 1;
+      LFG_REQUIRE(jp[i] - jm[i] + 1 <= bw, "cma_create: bandwidth too small for alpha/beta/gamma");
+    }
+    for (int j = 0; j < ncolumn; ++j) {
+      LFG_REQUIRE(ind_from[j] >= 1, "cma_create: indirection maps are 1-based");
+      iff[j] = ind_from[j] - 1;
+    }
+    int max_to = 0, max_from = 0;
+    for (int i = 0; i < nrow; ++i) max_to = std::max(max_to, ind_to[i]);
+    for (int j = 0; j < ncolumn; ++j) max_from = std::max(max_from, ind_from[j]);
+    lfg_cma m = new lfg_cma_s;
+    m->ctx = c;
+    m->kind = kind;
+    m->ncol = ncol;
+    m->nrow = nrow;
+    m->ncolumn = ncolumn;
+    m->bw = bw;
+    m->alpha = alpha;
+    m->beta = beta;
+    m->gm = gamma_m;
+    m->gp = gamma_p;
+    m->max_ind_to = max_to;
+    m->max_ind_from = max_from;
+    const size_t n = (size_t)bw * nrow * ncol;
+    std::vector<double> dev(n);
+    for (int col = 0; col < ncol; ++col)
+      for (int i = 0; i < nrow; ++i)
+        for (int b = 0; b < bw; ++b)
+          dev[((size_t)b * nrow + i) * ncol + col] = cm[((size_t)col * nrow + i) * bw + b];
+    try {
+      m->bands = dmalloc(n * kind);
+      if (kind == LFG_R_DOUBLE) upload(m->bands, dev.data(), n * sizeof(double));
+      else {
+        std::vector<float> f(dev.begin(), dev.end());
+        upload(m->bands, f.data(), n * sizeof(float));
+      }
+      m->ind_to = (int*)dmalloc(nrow * sizeof(int));
+      m->ind_from = (int*)dmalloc(ncolumn * sizeof(int));
+      m->jminus = (int*)dmalloc(nrow * sizeof(int));
+      m->jplus = (int*)dmalloc(nrow * sizeof(int));
+      upload(m->jplus, jp.data(), nrow * sizeof(int));
+      upload(m->ind_to, it.data(), nrow * sizeof(int));
+      upload(m->ind_from, iff.data(), ncolumn * sizeof(int));
+      upload(m->jminus, jm.data(), nrow * sizeof(int));
+    } catch (...) {
+      lfg_cma_destroy(m);
+      throw;
+    }
+    *out = m;
+  });
+}
+
+int lfg_cma_destroy(lfg_cma m) {
+  if (!m) return LFG_OK;
+  dfree(m->bands);
+  dfree(m->ind_to);
+  dfree(m->ind_from);
+  dfree(m->jminus);
+  dfree(m->jplus);
+  delete m;
+  return LFG_OK;
+}
+
+int lfg_cma_apply(lfg_cma m, lfg_field lhs, lfg_field x) {
+  if (!m) return LFG_ERR_ARG;
+  lfg_ctx c = m->ctx;
+  return guard(c, [&] {
+    LFG_REQUIRE(lhs && x && lhs->ncol == m->ncol && x->ncol == m->ncol &&
+                    lhs->nlev >= m->max_ind_to && x->nlev >= m->max_ind_from &&
+                    lhs->kind == m->kind && x->kind == m->kind,
+                "cma_apply: fields do not match the operator");
+    dim3 grid((m->ncol + 127) / 128, m->nrow);
+    dispatch(m->kind, [&](auto tag) {
+      using T = decltype(tag);
+      k_cma_app<T><<<grid, 128, 0, c->stream>>>((const T*)m->bands, m->ind_to, m->ind_from,
+                                                m->jminus, m->jplus, m->ncol, m->nrow,
+                                                m->ncolumn, (const T*)x->d, (T*)lhs->d);
+    });
+    after_launch(c, "cma_app");
+  });
+}
+
+int lfg_cma_apply_inverse(lfg_cma m, lfg_field lhs, lfg_field x) {
+  if (!m) return LFG_ERR_ARG;
+  lfg_ctx c = m->ctx;
+  return guard(c, [&] {
+    LFG_REQUIRE(m->bw == 3 && m->nrow == m->ncolumn,
+                "cma_apply_inverse: needs a square tridiagonal operator (bandwidth 3)");
+    LFG_REQUIRE(lhs && x && lhs->ncol == m->ncol && x->ncol == m->ncol &&
+                    lhs->nlev >= m->max_ind_to && x->nlev >= m->max_ind_to &&
+                    lhs->kind == m->kind && x->kind == m->kind,
+                "cma_apply_inverse: fields do not match the operator");
+    dispatch(m->kind, [&](auto tag) {
+      using T = decltype(tag);
+      TriSrc<T> s{m->ncol, m->nrow, (const T*)m->bands, nullptr, nullptr, nullptr, m->ind_to, 0};
+      launch_thomas<T, SRC_CMA>(c, s, (const T*)x->d, (T*)lhs->d);
+    });
+  });
+}
+
+int lfg_tri_solve(lfg_field y, lfg_field x, lfg_field t0, lfg_field tp, lfg_field tm) {
+  if (!y) return LFG_ERR_ARG;
+  lfg_ctx c = y->ctx;
+  return guard(c, [&] {
+    for (lfg_field f : {x, t0, tp, tm})
+      LFG_REQUIRE(f && f->ncol == y->ncol && f->nlev == y->nlev && f->kind == y->kind,
+                  "tri_solve: fields differ in shape or kind");
+    dispatch(y->kind, [&](auto tag) {
+      using T = decltype(tag);
+      TriSrc<T> s{y->ncol, y->nlev, nullptr, (const T*)t0->d, (const T*)tp->d,
+                  (const T*)tm->d, nullptr, 0};
+      launch_thomas<T, SRC_FIELDS>(c, s, (const T*)x->d, (T*)y->d);
+    });
+  });
+}
+
+int lfg_operator_tri_solve(lfg_lma m, lfg_field y, lfg_field x) {
+  if (!m) return LFG_ERR_ARG;
+  lfg_ctx c = m->ctx;
+  return guard(c, [&] {
+    LFG_REQUIRE(m->ndf_to == 2 && m->ndf_from == 2, "operator_tri_solve: needs a 2x2 LMA");
+    LFG_REQUIRE(y && x && y->ncol == m->ncell && x->ncol == m->ncell &&
+                    y->nlev == m->nl + 1 && x->nlev == m->nl + 1 && y->kind == m->kind &&
+                    x->kind == m->kind,
+                "operator_tri_solve: fields must have nlayers+1 levels per cell");
+    dispatch(m->kind, [&](auto tag) {
+      using T = decltype(tag);
+      TriSrc<T> s{m->ncell, m->nl + 1, (const T*)m->a, nullptr, nullptr, nullptr, nullptr, m->nl};
+      launch_thomas<T, SRC_LMA2>(c, s, (const T*)x->d, (T*)y->d);
+    });
+  });
+}
+
+// ------------------------------------------------------------- intergrid
+int lfg_intergrid_create(lfg_ctx c, int ncoarse, int nfine, int nx, int ny,
+                         const int* cell_map, const int* ccorners, const int* fcorners,
+                         lfg_intergrid* out) {
+  if (!c || !out) return LFG_ERR_ARG;
+  return guard(c, [&] {
+    LFG_REQUIRE(ncoarse > 0 && nfine > 0 && nx > 0 && ny > 0 && cell_map,
+                "intergrid_create: bad arguments");
+    LFG_REQUIRE(nfine == ncoarse * nx * ny, "intergrid_create: nfine != ncoarse*nx*ny");
+    const int nq = nx * ny;
+    std::vector<int> child((size_t)nq * ncoarse), parent(nfine, -1);
+    for (int C = 0; C < ncoarse; ++C)
+      for (int q = 0; q < nq; ++q) {
+        int f = cell_map[(size_t)C * nq + q];
+        LFG_REQUIRE(f >= 0 && f < nfine, "intergrid_create: fine cell id out of range");
+        LFG_REQUIRE(parent[f] < 0, "intergrid_create: fine cell in two coarse cells");
+        child[(size_t)q * ncoarse + C] = f;
+        parent[f] = C;
+      }
+    lfg_intergrid g = new lfg_intergrid_s;
+    g->ctx = c;
+    g->ncoarse = ncoarse;
+    g->nfine = nfine;
+    g->nx = nx;
+    g->ny = ny;
+    g->h_child.assign(cell_map, cell_map + (size_t)nq * ncoarse);
+    try {
+      g->child = (int*)dmalloc(child.size() * sizeof(int));
+      g->parent = (int*)dmalloc(parent.size() * sizeof(int));
+      upload(g->child, child.data(), child.size() * sizeof(int));
+      upload(g->parent, parent.data(), parent.size() * sizeof(int));
+      if (ccorners && fcorners) {
+        int nvc = 0, nvf = 0;
+        for (size_t i = 0; i < (size_t)4 * ncoarse; ++i) nvc = std::max(nvc, ccorners[i] + 1);
+        for (size_t i = 0; i < (size_t)4 * nfine; ++i) nvf = std::max(nvf, fcorners[i] + 1);
+        g->nvert_coarse = nvc;
+        g->nvert_fine = nvf;
+        std::vector<int> cc((size_t)4 * ncoarse);
+        for (int C = 0; C < ncoarse; ++C)
+          for (int s = 0; s < 4; ++s) cc[(size_t)s * ncoarse + C] = ccorners[4 * C + s];
+        // injection table (sci_restrict_w0_kernel_mod.F90:95-150): the NW, SW,
+        // NE, SE coarse corners from the corner fine cells
+        std::vector<int> inj(nvc, -1);
+        const int SWB = 0, SEB = 1, NEB = 2, NWB = 3;
+        for (int C = 0; C < ncoarse; ++C) {
+          auto cm_at = [&](int x, int y) { return cell_map[(size_t)C * nq + y * nx + x]; };
+          inj[ccorners[4 * C + NWB]] = fcorners[4 * cm_at(0, 0) + NWB];
+          inj[ccorners[4 * C + SWB]] = fcorners[4 * cm_at(0, ny - 1) + SWB];
+          inj[ccorners[4 * C + NEB]] = fcorners[4 * cm_at(nx - 1, 0) + NEB];
+          inj[ccorners[4 * C + SEB]] = fcorners[4 * cm_at(nx - 1, ny - 1) + SEB];
+        }
+        for (int v = 0; v < nvc; ++v)
+          LFG_REQUIRE(inj[v] >= 0, "intergrid_create: coarse vertex without fine partner");
+        // last-writer table of the bilinear prolongation (reference loop order)
+        std::vector<int> src(nvf, -1);
+        std::vector<double> wts((size_t)5 * nvf, 0.0);
+        auto put = [&](int v, int C, double a, double b, double cc2, double d, int nterm) {
+          src[v] = C;
+          double* w = &wts[(size_t)5 * v];
+          w[0] = a; w[1] = b; w[2] = cc2; w[3] = d; w[4] = nterm;
+        };
+        for (int C = 0; C < ncoarse; ++C)
+          for (int y = 1; y <= ny; ++y)
+            for (int x = 1; x <= nx; ++x) {
+              const int f = cell_map[(size_t)C * nq + (y - 1) * nx + (x - 1)];
+              const double nxy = (double)(nx * ny);
+              double wsw = (double)y * (double)(nx - x + 1) / nxy;
+              double wnw = (double)(ny - y) * (double)(nx - x + 1) / nxy;
+              double wne = (double)(ny - y) * (double)(x - 1) / nxy;
+              double wse = (double)y * (double)(x - 1) / nxy;
+              put(fcorners[4 * f + SWB], C, wne, wse, wsw, wnw, 4);
+              if (x == nx) {
+                wse = (double)y / (double)ny;
+                wne = 1.0 - wse;
+                put(fcorners[4 * f + SEB], C, wne, wse, 0.0, 0.0, 2);
+              }
+              if (y == 1) {
+                wnw = (double)(nx - x + 1) / (double)nx;
+                wne = 1.0 - wnw;
+                put(fcorners[4 * f + NWB], C, wne, 0.0, 0.0, wnw, 3);
+                if (x == nx) put(fcorners[4 * f + NEB], C, 1.0, 0.0, 0.0, 0.0, 1);
+              }
+            }
+        g->ccorner = (int*)dmalloc(cc.size() * sizeof(int));
+        upload(g->ccorner, cc.data(), cc.size() * sizeof(int));
+        int* d_inj = (int*)dmalloc(inj.size() * sizeof(int));
+        upload(d_inj, inj.data(), inj.size() * sizeof(int));
+        int* d_src = (int*)dmalloc(src.size() * sizeof(int));
+        upload(d_src, src.data(), src.size() * sizeof(int));
+        double* d_w = (double*)dmalloc(wts.size() * sizeof(double));
+        upload(d_w, wts.data(), wts.size() * sizeof(double));
+        g->w0_inj = d_inj;
+        g->w0_src = d_src;
+        g->w0_w = d_w;
+      }
+    } catch (...) {
+      lfg_intergrid_destroy(g);
+      throw;
+    }
+    *out = g;
+  });
+}
+
+int lfg_intergrid_destroy(lfg_intergrid g) {
+  if (!g) return LFG_OK;
+  dfree(g->child);
+  dfree(g->parent);
+  dfree(g->ccorner);
+  dfree(g->w0_inj);
+  dfree(g->w0_src);
+  dfree(g->w0_w);
+  delete g;
+  return LFG_OK;
+}
+
+int lfg_restrict_scalar(lfg_intergrid g, int mode, lfg_field coarse, lfg_field fine,
+                        lfg_field w) {
+  if (!g) return LFG_ERR_ARG;
+  lfg_ctx c = g->ctx;
+  return guard(c, [&] {
+    LFG_REQUIRE(coarse && fine && coarse->ncol == g->ncoarse && fine->ncol == g->nfine &&
+                    coarse->nlev == fine->nlev && coarse->kind == fine->kind,
+                "restrict_scalar: fields do not match the intergrid map");
+    LFG_REQUIRE(mode >= 0 && mode <= 2, "restrict_scalar: bad mode");
+    if (mode == LFG_RESTRICT_WEIGHTED)
+      LFG_REQUIRE(w && w->ncol == fine->ncol && w->nlev == fine->nlev && w->kind == fine->kind,
+                  "restrict_scalar: weighted restriction needs fine weights");
+    dim3 grid((g->ncoarse + 127) / 128, fine->nlev);
+    const int nq = g->nx * g->ny;
+    dispatch(fine->kind, [&](auto tag) {
+      using T = decltype(tag);
+      const T* wp = w ? (const T*)w->d : nullptr;
+      if (mode == LFG_RESTRICT_UNWEIGHTED)
+        k_restrict<T, LFG_RESTRICT_UNWEIGHTED><<<grid, 128, 0, c->stream>>>((T*)coarse->d, (const T*)fine->d, wp, g->child, g->ncoarse, g->nfine, nq, fine->nlev);
+      else if (mode == LFG_RESTRICT_WEIGHTED)
+        k_restrict<T, LFG_RESTRICT_WEIGHTED><<<grid, 128, 0, c->stream>>>((T*)coarse->d, (const T*)fine->d, wp, g->child, g->ncoarse, g->nfine, nq, fine->nlev);
+      else
+        k_restrict<T, LFG_RESTRICT_MASS_W3><<<grid, 128, 0, c->stream>>>((T*)coarse->d, (const T*)fine->d, wp, g->child, g->ncoarse, g->nfine, nq, fine->nlev);
+    });
+    after_launch(c, "restrict_scalar");
+  });
+}
+
+int lfg_prolong_scalar(lfg_intergrid g, lfg_field fine, lfg_field coarse, lfg_field w) {
+  if (!g) return LFG_ERR_ARG;
+  lfg_ctx c = g->ctx;
+  return guard(c, [&] {
+    LFG_REQUIRE(coarse && fine && coarse->ncol == g->ncoarse && fine->ncol == g->nfine &&
+                    coarse->nlev == fine->nlev && coarse->kind == fine->kind,
+                "prolong_scalar: fields do not match the intergrid map");
+    if (w)
+      LFG_REQUIRE(w->ncol == fine->ncol && w->nlev == fine->nlev && w->kind == fine->kind,
+                  "prolong_scalar: weights must be a fine field");
+    dim3 grid((g->nfine + 127) / 128, fine->nlev);
+    dispatch(fine->kind, [&](auto tag) {
+      using T = decltype(tag);
+      if (w)
+        k_prolong<T, true><<<grid, 128, 0, c->stream>>>((T*)fine->d, (const T*)coarse->d, (const T*)w->d, g->parent, g->nfine, g->ncoarse, fine->nlev);
+      else
+        k_prolong<T, false><<<grid, 128, 0, c->stream>>>((T*)fine->d, (const T*)coarse->d, nullptr, g->parent, g->nfine, g->ncoarse, fine->nlev);
+    });
+    after_launch(c, "prolong_scalar");
+  });
+}
+
+int lfg_restrict_w0(lfg_intergrid g, lfg_field coarse, lfg_field fine) {
+  if (!g) return LFG_ERR_ARG;
+  lfg_ctx c = g->ctx;
+  return guard(c, [&] {
+    LFG_REQUIRE(g->ccorner, "restrict_w0: intergrid map was created without W0 corners");
+    LFG_REQUIRE(coarse && fine && coarse->ncol == g->nvert_coarse &&
+                    fine->ncol == g->nvert_fine && coarse->nlev == fine->nlev &&
+                    coarse->kind == fine->kind,
+                "restrict_w0: fields do not match the W0 vertex columns");
+    dim3 grid((g->nvert_coarse + 127) / 128, fine->nlev);
+    dispatch(fine->kind, [&](auto tag) {
+      using T = decltype(tag);
+      k_restrict_w0<T><<<grid, 128, 0, c->stream>>>((T*)coarse->d, (const T*)fine->d, g->w0_inj,
+                                                    g->nvert_coarse, g->nvert_fine, fine->nlev);
+    });
+    after_launch(c, "restrict_w0");
+  });
+}
+
+int lfg_prolong_w0(lfg_intergrid g, lfg_field fine, lfg_field coarse) {
+  if (!g) return LFG_ERR_ARG;
+  lfg_ctx c = g->ctx;
+  return guard(c, [&] {
+    LFG_REQUIRE(g->ccorner, "prolong_w0: intergrid map was created without W0 corners");
+    LFG_REQUIRE(coarse && fine && coarse->ncol == g->nvert_coarse &&
+                    fine->ncol == g->nvert_fine && coarse->nlev == fine->nlev &&
+                    coarse->kind == fine->kind,
+                "prolong_w0: fields do not match the W0 vertex columns");
+    dim3 grid((g->nvert_fine + 127) / 128, fine->nlev);
+    dispatch(fine->kind, [&](auto tag) {
+      using T = decltype(tag);
+      k_prolong_w0<T><<<grid, 128, 0, c->stream>>>((T*)fine->d, (const T*)coarse->d, g->w0_src,
+                                                   g->w0_w, g->ccorner, g->nvert_fine,
+                                                   g->nvert_coarse, g->ncoarse, fine->nlev);
+    });
+    after_launch(c, "prolong_w0");
+  });
+}
+
+}  // extern "C"

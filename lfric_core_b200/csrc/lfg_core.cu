@@ -1,0 +1,648 @@
+// Context, fields, host<->device transfers and the vector-algebra built-ins.
+//
+// The built-ins replace the PSyclone built-ins invoked by the reference's
+// field vectors (components/science/source/algorithm/solver/
+// sci_field_vector_mod.x90:132-286, sci_r_solver_field_vector_mod.x90:119-296)
+// and the FP64-accumulated inner products of the hand-written PSy layer
+// (components/science/source/psy/sci_psykal_light_mod.f90:72-214).  Every
+// inner product is a deterministic two-level reduction: fixed grid-stride
+// partition, fixed-order block tree, and the last block to finish sums the
+// per-block partials in index order -- no floating-point atomics, so repeated
+// runs are bit-identical.
+#include "lfg_internal.cuh"
+
+#include <cstring>
+
+using namespace lfg;
+
+namespace lfg {
+
+void* dmalloc(size_t bytes) {
+  void* p = nullptr;
+  if (bytes == 0) bytes = 16;
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess)
+    throw Error(LFG_ERR_NOMEM, std::string("cudaMalloc(") + std::to_string(bytes) +
+                                   "): " + cudaGetErrorString(e));
+  return p;
+}
+void dfree(void* p) {
+  if (p) cudaFree(p);
+}
+void upload(void* d, const void* h, size_t bytes) {
+  LFG_CUDA(cudaMemcpy(d, h, bytes, cudaMemcpyHostToDevice));
+}
+
+// ------------------------------------------------------------ kernels
+template <class T>
+__global__ void k_set(T* __restrict__ x, size_t n, Sc a) {
+  const T v = (T)sc_eval(a);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    x[i] = v;
+}
+
+template <class TO, class TI>
+__global__ void k_copy(TO* __restrict__ y, const TI* __restrict__ x, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    y[i] = (TO)x[i];
+}
+
+// X = X + b Y   (inc_X_plus_bY); Y may be of another kind (r_def += r_solver,
+// sci_psykal_light_mod.f90:218-265), the product is then formed in X's kind.
+template <class T, class TY>
+__global__ void k_axpy(T* __restrict__ x, const TY* __restrict__ y, size_t n, Sc b) {
+  const T bv = (T)sc_eval(b);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    x[i] = x[i] + bv * (T)y[i];
+}
+
+// X = a X + Y   (inc_aX_plus_Y)
+template <class T>
+__global__ void k_aypx(T* __restrict__ x, const T* __restrict__ y, size_t n, Sc a) {
+  const T av = (T)sc_eval(a);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    x[i] = av * x[i] + y[i];
+}
+
+// Z = a X + b Y   (aX_plus_bY)
+template <class T>
+__global__ void k_axpby(T* __restrict__ z, const T* __restrict__ x, const T* __restrict__ y,
+                        size_t n, Sc a, Sc b) {
+  const T av = (T)sc_eval(a), bv = (T)sc_eval(b);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    z[i] = av * x[i] + bv * y[i];
+}
+
+// X = a X   (inc_a_times_X)
+template <class T>
+__global__ void k_scale(T* __restrict__ x, size_t n, Sc a) {
+  const T av = (T)sc_eval(a);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    x[i] = av * x[i];
+}
+
+// Z = X / Y   (X_divideby_Y)
+template <class T>
+__global__ void k_divide(T* __restrict__ z, const T* __restrict__ x, const T* __restrict__ y,
+                         size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    z[i] = x[i] / y[i];
+}
+
+// <X, Y> accumulated in double
+template <class T>
+__global__ void k_dot(const T* __restrict__ x, const T* __restrict__ y, size_t n, Red r) {
+  double acc = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    acc += (double)x[i] * (double)y[i];
+  red_finish(r, acc);
+}
+
+// Modified Gram-Schmidt step of gcr_solve (sci_iterative_solver_mod.f90:1358-1362)
+// fused with the next inner product: v -= a vj; pv -= a pvj; acc <v, next>
+// (next == null: <v, v>, the norm that follows the loop).
+template <class T>
+__global__ void k_mgs(T* __restrict__ v, T* __restrict__ pv, const T* __restrict__ vj,
+                      const T* __restrict__ pvj, const T* __restrict__ next, size_t n, Sc a,
+                      Red r) {
+  const T av = (T)sc_eval(a);
+  double acc = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const T vn = v[i] + av * vj[i];
+    v[i] = vn;
+    pv[i] = pv[i] + av * pvj[i];
+    const T w = next ? next[i] : vn;
+    acc += (double)vn * (double)w;
+  }
+  red_finish(r, acc);
+}
+
+// v *= b; pv *= b; acc <res, v>   (gcr_solve :1363-1367)
+template <class T>
+__global__ void k_scale2_dot(T* __restrict__ v, T* __restrict__ pv, const T* __restrict__ res,
+                             size_t n, Sc b, Red r) {
+  const T bv = (T)sc_eval(b);
+  double acc = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const T vn = bv * v[i];
+    v[i] = vn;
+    pv[i] = bv * pv[i];
+    acc += (double)res[i] * (double)vn;
+  }
+  red_finish(r, acc);
+}
+
+// dx += a pv; res -= a v; acc <res, res>   (gcr_solve :1368-1374)
+template <class T>
+__global__ void k_update2_norm(T* __restrict__ dx, const T* __restrict__ pv,
+                               T* __restrict__ res, const T* __restrict__ v, size_t n, Sc a,
+                               Red r) {
+  const double ad = sc_eval(a);
+  const T ap = (T)ad, am = (T)(-ad);
+  double acc = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    dx[i] = dx[i] + ap * pv[i];
+    const T rn = res[i] + am * v[i];
+    res[i] = rn;
+    acc += (double)rn * (double)rn;
+  }
+  red_finish(r, acc);
+}
+
+// x += b y; acc <x, x>
+template <class T>
+__global__ void k_axpy_norm(T* __restrict__ x, const T* __restrict__ y, size_t n, Sc b,
+                            Red r) {
+  const T bv = (T)sc_eval(b);
+  double acc = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const T xn = x[i] + bv * y[i];
+    x[i] = xn;
+    acc += (double)xn * (double)xn;
+  }
+  red_finish(r, acc);
+}
+
+// x += b y; acc <x, next> (next null: <x, x>)  (gmres/fgmres Arnoldi)
+template <class T>
+__global__ void k_axpy_dot(T* __restrict__ x, const T* __restrict__ y,
+                           const T* __restrict__ next, size_t n, Sc b, Red r) {
+  const T bv = (T)sc_eval(b);
+  double acc = 0.0;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const T xn = x[i] + bv * y[i];
+    x[i] = xn;
+    acc += (double)xn * (double)(next ? next[i] : xn);
+  }
+  red_finish(r, acc);
+}
+
+// dst = a src   (copy followed by inc_a_times_X)
+template <class T>
+__global__ void k_scale_copy(T* __restrict__ dst, const T* __restrict__ src, size_t n, Sc a) {
+  const T av = (T)sc_eval(a);
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    dst[i] = av * src[i];
+}
+
+// Column-contiguous (e*nlev + k) <-> level-major (k*ncol + e) with kind
+// conversion, through 32x32 shared-memory tiles.
+template <class TO, class TI>
+__global__ void k_to_level_major(TO* __restrict__ out, const TI* __restrict__ in, int ncol,
+                                 int nlev) {
+  __shared__ TI tile[32][33];
+  const int e0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    int e = e0 + j, k = k0 + threadIdx.x;
+    if (e < ncol && k < nlev) tile[j][threadIdx.x] = in[(size_t)e * nlev + k];
+  }
+  __syncthreads();
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    int k = k0 + j, e = e0 + threadIdx.x;
+    if (e < ncol && k < nlev) out[(size_t)k * ncol + e] = (TO)tile[threadIdx.x][j];
+  }
+}
+
+template <class TO, class TI>
+__global__ void k_to_column(TO* __restrict__ out, const TI* __restrict__ in, int ncol,
+                            int nlev) {
+  __shared__ TI tile[32][33];
+  const int e0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    int k = k0 + j, e = e0 + threadIdx.x;
+    if (e < ncol && k < nlev) tile[j][threadIdx.x] = in[(size_t)k * ncol + e];
+  }
+  __syncthreads();
+  for (int j = threadIdx.y; j < 32; j += blockDim.y) {
+    int e = e0 + j, k = k0 + threadIdx.x;
+    if (e < ncol && k < nlev) out[(size_t)e * nlev + k] = (TO)tile[threadIdx.x][j];
+  }
+}
+
+// ------------------------------------------------------------ launchers
+#define DISPATCH_KIND(kind, T, ...)                         \
+  do {                                                      \
+    if ((kind) == LFG_R_DOUBLE) {                           \
+      using T = double;                                     \
+      __VA_ARGS__;                                          \
+    } else {                                                \
+      using T = float;                                      \
+      __VA_ARGS__;                                          \
+    }                                                       \
+  } while (0)
+
+static void same_shape(lfg_field a, lfg_field b, const char* what) {
+  LFG_REQUIRE(a && b, std::string(what) + ": null field");
+  LFG_REQUIRE(a->ncol == b->ncol && a->nlev == b->nlev,
+              std::string(what) + ": fields differ in shape");
+}
+static void same_kind(lfg_field a, lfg_field b, const char* what) {
+  same_shape(a, b, what);
+  LFG_REQUIRE(a->kind == b->kind, std::string(what) + ": fields differ in kind");
+}
+
+void vec_set(lfg_field x, Sc a) {
+  lfg_ctx c = x->ctx;
+  DISPATCH_KIND(x->kind, T,
+                k_set<T><<<c->stream_grid(x->n()), kThreads, 0, c->stream>>>((T*)x->d, x->n(), a));
+  after_launch(c, "set");
+}
+
+void vec_copy(lfg_field dst, lfg_field src) {
+  same_shape(dst, src, "copy");
+  lfg_ctx c = dst->ctx;
+  const int g = c->stream_grid(dst->n());
+  if (dst->kind == LFG_R_DOUBLE && src->kind == LFG_R_DOUBLE)
+    k_copy<double, double><<<g, kThreads, 0, c->stream>>>((double*)dst->d, (const double*)src->d, dst->n());
+  else if (dst->kind == LFG_R_DOUBLE)
+    k_copy<double, float><<<g, kThreads, 0, c->stream>>>((double*)dst->d, (const float*)src->d, dst->n());
+  else if (src->kind == LFG_R_DOUBLE)
+    k_copy<float, double><<<g, kThreads, 0, c->stream>>>((float*)dst->d, (const double*)src->d, dst->n());
+  else
+    k_copy<float, float><<<g, kThreads, 0, c->stream>>>((float*)dst->d, (const float*)src->d, dst->n());
+  after_launch(c, "copy");
+}
+
+void vec_axpy(lfg_field x, Sc b, lfg_field y) {
+  same_shape(x, y, "inc_X_plus_bY");
+  lfg_ctx c = x->ctx;
+  const int g = c->stream_grid(x->n());
+  if (x->kind == y->kind) {
+    DISPATCH_KIND(x->kind, T,
+                  k_axpy<T, T><<<g, kThreads, 0, c->stream>>>((T*)x->d, (const T*)y->d, x->n(), b));
+  } else if (x->kind == LFG_R_DOUBLE) {
+    k_axpy<double, float><<<g, kThreads, 0, c->stream>>>((double*)x->d, (const float*)y->d, x->n(), b);
+  } else {
+    k_axpy<float, double><<<g, kThreads, 0, c->stream>>>((float*)x->d, (const double*)y->d, x->n(), b);
+  }
+  after_launch(c, "axpy");
+}
+
+void vec_aypx(lfg_field x, Sc a, lfg_field y) {
+  same_kind(x, y, "inc_aX_plus_Y");
+  lfg_ctx c = x->ctx;
+  DISPATCH_KIND(x->kind, T,
+                k_aypx<T><<<c->stream_grid(x->n()), kThreads, 0, c->stream>>>((T*)x->d, (const T*)y->d, x->n(), a));
+  after_launch(c, "aypx");
+}
+
+void vec_axpby(lfg_field z, Sc a, lfg_field x, Sc b, lfg_field y) {
+  same_kind(z, x, "aX_plus_bY");
+  same_kind(z, y, "aX_plus_bY");
+  lfg_ctx c = z->ctx;
+  DISPATCH_KIND(z->kind, T,
+                k_axpby<T><<<c->stream_grid(z->n()), kThreads, 0, c->stream>>>(
+                    (T*)z->d, (const T*)x->d, (const T*)y->d, z->n(), a, b));
+  after_launch(c, "axpby");
+}
+
+void vec_scale(lfg_field x, Sc a) {
+  lfg_ctx c = x->ctx;
+  DISPATCH_KIND(x->kind, T,
+                k_scale<T><<<c->stream_grid(x->n()), kThreads, 0, c->stream>>>((T*)x->d, x->n(), a));
+  after_launch(c, "scale");
+}
+
+void vec_divide(lfg_field z, lfg_field x, lfg_field y) {
+  same_kind(z, x, "X_divideby_Y");
+  same_kind(z, y, "X_divideby_Y");
+  lfg_ctx c = z->ctx;
+  DISPATCH_KIND(z->kind, T,
+                k_divide<T><<<c->stream_grid(z->n()), kThreads, 0, c->stream>>>(
+                    (T*)z->d, (const T*)x->d, (const T*)y->d, z->n()));
+  after_launch(c, "divide");
+}
+
+void vec_dot(lfg_field x, lfg_field y, int slot) {
+  same_kind(x, y, "X_innerproduct_Y");
+  lfg_ctx c = x->ctx;
+  DISPATCH_KIND(x->kind, T,
+                k_dot<T><<<c->stream_grid(x->n()), kThreads, 0, c->stream>>>(
+                    (const T*)x->d, (const T*)y->d, x->n(), c->red(slot)));
+  after_launch(c, "dot");
+}
+
+void vec_mgs_step(lfg_field v, lfg_field pv, lfg_field vj, lfg_field pvj, Sc alpha,
+                  lfg_field next, int slot) {
+  same_kind(v, pv, "mgs");
+  same_kind(v, vj, "mgs");
+  same_kind(v, pvj, "mgs");
+  if (next) same_kind(v, next, "mgs");
+  lfg_ctx c = v->ctx;
+  DISPATCH_KIND(v->kind, T,
+                k_mgs<T><<<c->stream_grid(v->n()), kThreads, 0, c->stream>>>(
+                    (T*)v->d, (T*)pv->d, (const T*)vj->d, (const T*)pvj->d,
+                    next ? (const T*)next->d : nullptr, v->n(), alpha, c->red(slot)));
+  after_launch(c, "mgs");
+}
+
+void vec_scale2_dot(lfg_field v, lfg_field pv, Sc beta, lfg_field res, int slot) {
+  same_kind(v, pv, "scale2_dot");
+  same_kind(v, res, "scale2_dot");
+  lfg_ctx c = v->ctx;
+  DISPATCH_KIND(v->kind, T,
+                k_scale2_dot<T><<<c->stream_grid(v->n()), kThreads, 0, c->stream>>>(
+                    (T*)v->d, (T*)pv->d, (const T*)res->d, v->n(), beta, c->red(slot)));
+  after_launch(c, "scale2_dot");
+}
+
+void vec_update2_norm(lfg_field dx, lfg_field pv, lfg_field res, lfg_field v, Sc alpha,
+                      int slot) {
+  same_kind(dx, pv, "update2_norm");
+  same_kind(dx, res, "update2_norm");
+  same_kind(dx, v, "update2_norm");
+  lfg_ctx c = dx->ctx;
+  DISPATCH_KIND(dx->kind, T,
+                k_update2_norm<T><<<c->stream_grid(dx->n()), kThreads, 0, c->stream>>>(
+                    (T*)dx->d, (const T*)pv->d, (T*)res->d, (const T*)v->d, dx->n(), alpha,
+                    c->red(slot)));
+  after_launch(c, "update2_norm");
+}
+
+void vec_axpy_norm(lfg_field x, Sc b, lfg_field y, int slot) {
+  same_kind(x, y, "axpy_norm");
+  lfg_ctx c = x->ctx;
+  DISPATCH_KIND(x->kind, T,
+                k_axpy_norm<T><<<c->stream_grid(x->n()), kThreads, 0, c->stream>>>(
+                    (T*)x->d, (const T*)y->d, x->n(), b, c->red(slot)));
+  after_launch(c, "axpy_norm");
+}
+
+void vec_axpy_dot(lfg_field x, Sc b, lfg_field y, lfg_field next, int slot) {
+  same_kind(x, y, "axpy_dot");
+  if (next) same_kind(x, next, "axpy_dot");
+  lfg_ctx c = x->ctx;
+  DISPATCH_KIND(x->kind, T,
+                k_axpy_dot<T><<<c->stream_grid(x->n()), kThreads, 0, c->stream>>>(
+                    (T*)x->d, (const T*)y->d, next ? (const T*)next->d : nullptr, x->n(), b,
+                    c->red(slot)));
+  after_launch(c, "axpy_dot");
+}
+
+void vec_scale_copy(lfg_field dst, Sc a, lfg_field src) {
+  same_kind(dst, src, "scale_copy");
+  lfg_ctx c = dst->ctx;
+  DISPATCH_KIND(dst->kind, T,
+                k_scale_copy<T><<<c->stream_grid(dst->n()), kThreads, 0, c->stream>>>(
+                    (T*)dst->d, (const T*)src->d, dst->n(), a));
+  after_launch(c, "scale_copy");
+}
+
+}  // namespace lfg
+
+// ------------------------------------------------------------ ctx methods
+void* lfg_ctx_s::staging(size_t bytes) {
+  if (bytes > stage_bytes) {
+    dfree(stage);
+    stage = nullptr;
+    stage_bytes = 0;
+    stage = dmalloc(bytes);
+    stage_bytes = bytes;
+  }
+  return stage;
+}
+
+void* lfg_ctx_s::scratch(size_t bytes) {
+  if (bytes > scratch_bytes) {
+    LFG_CUDA(cudaStreamSynchronize(stream));
+    dfree(scratch_buf);
+    scratch_buf = nullptr;
+    scratch_bytes = 0;
+    scratch_buf = dmalloc(bytes);
+    scratch_bytes = bytes;
+  }
+  return scratch_buf;
+}
+
+double lfg_ctx_s::read_result(int slot) {
+  LFG_CUDA(cudaMemcpyAsync(host_results + slot, red_results + slot, sizeof(double),
+                           cudaMemcpyDeviceToHost, stream));
+  LFG_CUDA(cudaStreamSynchronize(stream));
+  return host_results[slot];
+}
+
+// ================================================================ C ABI
+extern "C" {
+
+const char* lfg_version(void) { return "lfric_core_b200 1.0 (sm_100a)"; }
+
+int lfg_ctx_create(int device, lfg_ctx* out) {
+  if (!out) return LFG_ERR_ARG;
+  *out = nullptr;
+  lfg_ctx c = new (std::nothrow) lfg_ctx_s;
+  if (!c) return LFG_ERR_NOMEM;
+  int st = guard(c, [&] {
+    LFG_CUDA(cudaSetDevice(device));
+    c->device = device;
+    LFG_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
+    LFG_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
+    c->stream = c->own_stream;
+    c->red_partials = (double*)dmalloc(sizeof(double) * kRedSlots * kMaxRedBlocks);
+    c->red_counters = (unsigned*)dmalloc(sizeof(unsigned) * kRedSlots);
+    c->red_results = (double*)dmalloc(sizeof(double) * kRedSlots);
+    LFG_CUDA(cudaMemset(c->red_counters, 0, sizeof(unsigned) * kRedSlots));
+    LFG_CUDA(cudaMemset(c->red_results, 0, sizeof(double) * kRedSlots));
+    LFG_CUDA(cudaMallocHost(&c->host_results, sizeof(double) * kRedSlots));
+  });
+  if (st != LFG_OK) {
+    fprintf(stderr, "lfg_ctx_create: %s\n", c->last_error.c_str());
+    lfg_ctx_destroy(c);
+    return st;
+  }
+  *out = c;
+  return LFG_OK;
+}
+
+int lfg_ctx_destroy(lfg_ctx c) {
+  if (!c) return LFG_OK;
+  if (c->own_stream) cudaStreamSynchronize(c->own_stream);
+  dfree(c->red_partials);
+  dfree(c->red_counters);
+  dfree(c->red_results);
+  dfree(c->stage);
+  dfree(c->scratch_buf);
+  if (c->host_results) cudaFreeHost(c->host_results);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  delete c;
+  return LFG_OK;
+}
+
+int lfg_ctx_set_stream(lfg_ctx c, void* stream) {
+  if (!c) return LFG_ERR_ARG;
+  c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+  return LFG_OK;
+}
+
+int lfg_ctx_synchronize(lfg_ctx c) {
+  if (!c) return LFG_ERR_ARG;
+  return guard(c, [&] { LFG_CUDA(cudaStreamSynchronize(c->stream)); });
+}
+
+int lfg_ctx_kernel_launches(lfg_ctx c, uint64_t* count) {
+  if (!c || !count) return LFG_ERR_ARG;
+  *count = c->launches;
+  return LFG_OK;
+}
+
+const char* lfg_last_error(lfg_ctx c) {
+  if (!c) return "null context";
+  return c->last_error.c_str();
+}
+
+// ------------------------------------------------------------ fields
+int lfg_field_create(lfg_ctx c, int kind, int ncol, int nlev, lfg_field* out) {
+  if (!c || !out) return LFG_ERR_ARG;
+  return guard(c, [&] {
+    LFG_REQUIRE(kind == LFG_R_DOUBLE || kind == LFG_R_SINGLE, "field_create: bad kind");
+    LFG_REQUIRE(ncol > 0 && nlev > 0, "field_create: sizes must be positive");
+    lfg_field f = new lfg_field_s;
+    f->ctx = c;
+    f->kind = kind;
+    f->ncol = ncol;
+    f->nlev = nlev;
+    try {
+      f->d = dmalloc(f->bytes());
+      f->owned = true;
+      LFG_CUDA(cudaMemsetAsync(f->d, 0, f->bytes(), c->stream));
+    } catch (...) {
+      delete f;
+      throw;
+    }
+    *out = f;
+  });
+}
+
+int lfg_field_wrap(lfg_ctx c, int kind, int ncol, int nlev, void* dptr, lfg_field* out) {
+  if (!c || !out) return LFG_ERR_ARG;
+  return guard(c, [&] {
+    LFG_REQUIRE(kind == LFG_R_DOUBLE || kind == LFG_R_SINGLE, "field_wrap: bad kind");
+    LFG_REQUIRE(ncol > 0 && nlev > 0 && dptr, "field_wrap: bad arguments");
+    lfg_field f = new lfg_field_s;
+    f->ctx = c;
+    f->kind = kind;
+    f->ncol = ncol;
+    f->nlev = nlev;
+    f->d = dptr;
+    f->owned = false;
+    *out = f;
+  });
+}
+
+int lfg_field_destroy(lfg_field f) {
+  if (!f) return LFG_OK;
+  if (f->owned) dfree(f->d);
+  delete f;
+  return LFG_OK;
+}
+
+int lfg_field_device_ptr(lfg_field f, void** p) {
+  if (!f || !p) return LFG_ERR_ARG;
+  *p = f->d;
+  return LFG_OK;
+}
+
+int lfg_field_import(lfg_field f, const void* host, int host_kind) {
+  if (!f) return LFG_ERR_ARG;
+  lfg_ctx c = f->ctx;
+  return guard(c, [&] {
+    LFG_REQUIRE(host, "field_import: null host array");
+    LFG_REQUIRE(host_kind == LFG_R_DOUBLE || host_kind == LFG_R_SINGLE,
+                "field_import: bad host kind");
+    const size_t bytes = f->n() * host_kind;
+    void* st = c->staging(bytes);
+    LFG_CUDA(cudaMemcpyAsync(st, host, bytes, cudaMemcpyHostToDevice, c->stream));
+    dim3 grid((f->ncol + 31) / 32, (f->nlev + 31) / 32), block(32, 8);
+    if (f->kind == LFG_R_DOUBLE && host_kind == LFG_R_DOUBLE)
+      k_to_level_major<double, double><<<grid, block, 0, c->stream>>>((double*)f->d, (const double*)st, f->ncol, f->nlev);
+    else if (f->kind == LFG_R_DOUBLE)
+      k_to_level_major<double, float><<<grid, block, 0, c->stream>>>((double*)f->d, (const float*)st, f->ncol, f->nlev);
+    else if (host_kind == LFG_R_DOUBLE)
+      k_to_level_major<float, double><<<grid, block, 0, c->stream>>>((float*)f->d, (const double*)st, f->ncol, f->nlev);
+    else
+      k_to_level_major<float, float><<<grid, block, 0, c->stream>>>((float*)f->d, (const float*)st, f->ncol, f->nlev);
+    after_launch(c, "to_level_major");
+    LFG_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int lfg_field_export(lfg_field f, void* host, int host_kind) {
+  if (!f) return LFG_ERR_ARG;
+  lfg_ctx c = f->ctx;
+  return guard(c, [&] {
+    LFG_REQUIRE(host, "field_export: null host array");
+    LFG_REQUIRE(host_kind == LFG_R_DOUBLE || host_kind == LFG_R_SINGLE,
+                "field_export: bad host kind");
+    const size_t bytes = f->n() * host_kind;
+    void* st = c->staging(bytes);
+    dim3 grid((f->ncol + 31) / 32, (f->nlev + 31) / 32), block(32, 8);
+    if (f->kind == LFG_R_DOUBLE && host_kind == LFG_R_DOUBLE)
+      k_to_column<double, double><<<grid, block, 0, c->stream>>>((double*)st, (const double*)f->d, f->ncol, f->nlev);
+    else if (f->kind == LFG_R_DOUBLE)
+      k_to_column<float, double><<<grid, block, 0, c->stream>>>((float*)st, (const double*)f->d, f->ncol, f->nlev);
+    else if (host_kind == LFG_R_DOUBLE)
+      k_to_column<double, float><<<grid, block, 0, c->stream>>>((double*)st, (const float*)f->d, f->ncol, f->nlev);
+    else
+      k_to_column<float, float><<<grid, block, 0, c->stream>>>((float*)st, (const float*)f->d, f->ncol, f->nlev);
+    after_launch(c, "to_column");
+    LFG_CUDA(cudaMemcpyAsync(host, st, bytes, cudaMemcpyDeviceToHost, c->stream));
+    LFG_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+// ------------------------------------------------------------ built-ins
+#define FIELD_CTX(f) ((f) ? (f)->ctx : nullptr)
+
+int lfg_setval_c(lfg_field x, double v) {
+  if (!x) return LFG_ERR_ARG;
+  return guard(x->ctx, [&] { vec_set(x, sc_const(v)); });
+}
+int lfg_setval_X(lfg_field dst, lfg_field src) {
+  if (!dst || !src) return LFG_ERR_ARG;
+  return guard(dst->ctx, [&] { vec_copy(dst, src); });
+}
+int lfg_inc_X_plus_bY(lfg_field x, double b, lfg_field y) {
+  if (!x || !y) return LFG_ERR_ARG;
+  return guard(x->ctx, [&] { vec_axpy(x, sc_const(b), y); });
+}
+int lfg_inc_aX_plus_Y(double a, lfg_field x, lfg_field y) {
+  if (!x || !y) return LFG_ERR_ARG;
+  return guard(x->ctx, [&] { vec_aypx(x, sc_const(a), y); });
+}
+int lfg_aX_plus_bY(lfg_field z, double a, lfg_field x, double b, lfg_field y) {
+  if (!z || !x || !y) return LFG_ERR_ARG;
+  return guard(z->ctx, [&] { vec_axpby(z, sc_const(a), x, sc_const(b), y); });
+}
+int lfg_inc_a_times_X(double a, lfg_field x) {
+  if (!x) return LFG_ERR_ARG;
+  return guard(x->ctx, [&] { vec_scale(x, sc_const(a)); });
+}
+int lfg_X_divideby_Y(lfg_field z, lfg_field x, lfg_field y) {
+  if (!z || !x || !y) return LFG_ERR_ARG;
+  return guard(z->ctx, [&] { vec_divide(z, x, y); });
+}
+int lfg_X_innerproduct_Y(lfg_field x, lfg_field y, double* result) {
+  if (!x || !y || !result) return LFG_ERR_ARG;
+  return guard(x->ctx, [&] {
+    vec_dot(x, y, 0);
+    *result = x->ctx->read_result(0);
+  });
+}
+int lfg_X_innerproduct_X(lfg_field x, double* result) {
+  return lfg_X_innerproduct_Y(x, x, result);
+}
+
+}  // extern "C"

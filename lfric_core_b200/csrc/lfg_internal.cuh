@@ -1,0 +1,294 @@
+// Internal definitions of the B200 LFRic solver library.
+//
+// Device layout: a field of ncol horizontal entities with nlev dofs each is
+// stored level-major, element (k, c) at k*ncol + c, so that a warp of
+// threads handling consecutive columns reads consecutive addresses at every
+// level.  Operators use the same layout for their coefficient arrays.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include <cmath>
+#include <cstdio>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "../../include/lfg.h"
+
+namespace lfg {
+
+// Blocks per SM used for streaming grids (grid = SMs * this, grid-stride).
+constexpr int kStreamBlocksPerSM = 8;
+constexpr int kThreads = 256;
+// Reduction slots available per context and the partial buffer per slot.
+constexpr int kRedSlots = 512;
+constexpr int kMaxRedBlocks = 4096;
+
+struct Error : std::runtime_error {
+  int code;
+  Error(int c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+#define LFG_CUDA(call)                                                              \
+  do {                                                                              \
+    cudaError_t e_ = (call);                                                        \
+    if (e_ != cudaSuccess)                                                          \
+      throw ::lfg::Error(LFG_ERR_CUDA, std::string(#call) + ": " + cudaGetErrorString(e_)); \
+  } while (0)
+
+#define LFG_REQUIRE(cond, msg)                                             \
+  do {                                                                     \
+    if (!(cond)) throw ::lfg::Error(LFG_ERR_ARG, std::string(msg));        \
+  } while (0)
+
+// A scalar operand evaluated on the device: lets Krylov scalars stay in
+// device memory (no host round trip) while keeping the reference's order of
+// operations.  value = c, c*a, c*a/b or c/sqrt(a).
+enum ScOp : int { SC_CONST = 0, SC_MUL = 1, SC_DIV = 2, SC_RSQRT = 3 };
+struct Sc {
+  int op;
+  double c;
+  const double* a;
+  const double* b;
+};
+inline Sc sc_const(double c) { return Sc{SC_CONST, c, nullptr, nullptr}; }
+inline Sc sc_mul(double c, const double* a) { return Sc{SC_MUL, c, a, nullptr}; }
+inline Sc sc_div(double c, const double* a, const double* b) { return Sc{SC_DIV, c, a, b}; }
+inline Sc sc_rsqrt(double c, const double* a) { return Sc{SC_RSQRT, c, a, nullptr}; }
+
+__device__ __forceinline__ double sc_eval(const Sc& s) {
+  switch (s.op) {
+    case SC_MUL: return s.c * *s.a;
+    case SC_DIV: return s.c * *s.a / *s.b;
+    case SC_RSQRT: return s.c / sqrt(*s.a);
+    default: return s.c;
+  }
+}
+
+// One deterministic reduction: per-block partial sums, then the last block
+// to finish adds the partials in index order and writes the result.
+struct Red {
+  double* partials;   // [kMaxRedBlocks]
+  unsigned* counter;  // zero between reductions
+  double* result;
+};
+
+// ------------------------------------------------------------ reductions
+// Deterministic block sum (fixed shuffle tree) and the last-block finish.
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// Sum over the block; the result is valid in thread 0.  Fixed tree.
+__device__ __forceinline__ double block_sum(double v) {
+  __shared__ double s[32];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  __syncthreads();
+  v = warp_sum(v);
+  if (lane == 0) s[warp] = v;
+  __syncthreads();
+  if (warp == 0) {
+    v = lane < (int)(blockDim.x >> 5) ? s[lane] : 0.0;
+    v = warp_sum(v);
+  }
+  return v;
+}
+
+__device__ __forceinline__ void red_finish(const Red& r, double v) {
+  __shared__ bool is_last;
+  v = block_sum(v);
+  if (threadIdx.x == 0) {
+    r.partials[blockIdx.x] = v;
+    __threadfence();
+    unsigned t = atomicAdd(r.counter, 1u);
+    is_last = (t == gridDim.x - 1);
+  }
+  __syncthreads();
+  if (is_last) {
+    __threadfence();
+    double acc = 0.0;
+    const volatile double* p = r.partials;
+    for (unsigned i = threadIdx.x; i < gridDim.x; i += blockDim.x) acc += p[i];
+    acc = block_sum(acc);
+    if (threadIdx.x == 0) {
+      *r.result = acc;
+      *r.counter = 0u;
+    }
+  }
+}
+
+}  // namespace lfg
+
+// ------------------------------------------------------------------ objects
+struct lfg_ctx_s {
+  int device = 0;
+  int num_sms = 148;
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  std::string last_error;
+  uint64_t launches = 0;
+  // reduction slots
+  double* red_partials = nullptr;  // [kRedSlots][kMaxRedBlocks]
+  unsigned* red_counters = nullptr;
+  double* red_results = nullptr;   // [kRedSlots]
+  double* host_results = nullptr;  // pinned [kRedSlots]
+  // host<->device staging for import/export
+  void* stage = nullptr;
+  size_t stage_bytes = 0;
+  // device scratch of the kernels that need one (grown on demand)
+  void* scratch_buf = nullptr;
+  size_t scratch_bytes = 0;
+
+  lfg::Red red(int slot) {
+    return lfg::Red{red_partials + (size_t)slot * lfg::kMaxRedBlocks, red_counters + slot,
+                    red_results + slot};
+  }
+  int stream_grid(size_t n, int threads = lfg::kThreads) const {
+    size_t need = (n + threads - 1) / threads;
+    size_t cap = (size_t)num_sms * lfg::kStreamBlocksPerSM;
+    if (need < 1) need = 1;
+    return (int)(need < cap ? need : cap);
+  }
+  void* staging(size_t bytes);
+  void* scratch(size_t bytes);
+  double read_result(int slot);   // synchronises the stream
+};
+
+struct lfg_field_s {
+  lfg_ctx ctx = nullptr;
+  int kind = LFG_R_DOUBLE;
+  int ncol = 0, nlev = 0;
+  void* d = nullptr;
+  bool owned = false;
+  size_t n() const { return (size_t)ncol * nlev; }
+  size_t bytes() const { return n() * kind; }
+};
+
+struct lfg_mesh_s {
+  lfg_ctx ctx = nullptr;
+  int ncol = 0;
+  int* links = nullptr;  // device, SoA [4][ncol]
+  std::vector<int> h_links;  // host copy, [ncol][4]
+};
+
+struct lfg_intergrid_s {
+  lfg_ctx ctx = nullptr;
+  int ncoarse = 0, nfine = 0, nx = 0, ny = 0;
+  int* child = nullptr;    // device [nx*ny][ncoarse], slot q = y*nx + x
+  int* parent = nullptr;   // device [nfine]
+  int* ccorner = nullptr;  // device [4][ncoarse] W0 coarse corner vertices (or null)
+  int* w0_inj = nullptr;   // device [nvert_coarse] coinciding fine vertex
+  int* w0_src = nullptr;   // device [nvert_fine] coarse cell of the last write (-1: none)
+  double* w0_w = nullptr;  // device [nvert_fine][5] weights NE,SE,SW,NW and term count
+  int nvert_coarse = 0, nvert_fine = 0;
+  std::vector<int> h_child;  // [ncoarse][ny][nx]
+};
+
+struct lfg_cma_s {
+  lfg_ctx ctx = nullptr;
+  int kind = LFG_R_DOUBLE;
+  int ncol = 0, nrow = 0, ncolumn = 0, bw = 0, alpha = 0, beta = 0, gm = 0, gp = 0;
+  void* bands = nullptr;      // [bw][nrow][ncol]
+  int* ind_to = nullptr;      // device, 0-based column offsets [nrow]
+  int* ind_from = nullptr;    // [ncolumn]
+  int* jminus = nullptr;      // [nrow] first band column of each row (0-based)
+  int* jplus = nullptr;       // [nrow] last band column of each row
+  int max_ind_to = 0, max_ind_from = 0;  // largest 1-based column offsets
+};
+
+struct lfg_lma_s {
+  lfg_ctx ctx = nullptr;
+  int kind = LFG_R_DOUBLE;
+  int ncell = 0, nl = 0, ndf_to = 0, ndf_from = 0;
+  int nent_to = 0, nlev_to = 0, nent_from = 0, nlev_from = 0;
+  void* a = nullptr;        // [ndf_to][ndf_from][nl][ncell]
+  int* ent_to = nullptr;    // [ndf_to][ncell] entity of each cell dof
+  int* off_to = nullptr;    // [ndf_to][ncell] level offset
+  int* ent_from = nullptr;  // [ndf_from][ncell]
+  int* off_from = nullptr;
+  // gather lists: for each output entity its (cell, df) incidences
+  int* inc_to_ptr = nullptr;   // [nent_to+1]
+  int* inc_to = nullptr;       // packed cell*ndf_to + df
+  int* inc_from_ptr = nullptr;
+  int* inc_from = nullptr;
+  int max_inc_to = 0, max_inc_from = 0;
+};
+
+struct lfg_helm_s {
+  lfg_ctx ctx = nullptr;
+  lfg_mesh mesh = nullptr;
+  int kind = LFG_R_DOUBLE;
+  int ncol = 0, nl = 0;
+  void* sub = nullptr;   // [nl][ncol]
+  void* diag = nullptr;
+  void* sup = nullptr;
+  void* h = nullptr;     // [4][nl][ncol]
+};
+
+namespace lfg {
+
+// Launch bookkeeping and error checks shared by all translation units.
+inline void after_launch(lfg_ctx ctx, const char* what) {
+  ctx->launches++;
+  cudaError_t e = cudaGetLastError();
+  if (e != cudaSuccess)
+    throw Error(LFG_ERR_CUDA, std::string("launch of ") + what + ": " + cudaGetErrorString(e));
+}
+
+void* dmalloc(size_t bytes);
+void dfree(void* p);
+void upload(void* d, const void* h, size_t bytes);
+
+// entry-point wrapper: converts exceptions into status codes
+template <class F>
+int guard(lfg_ctx ctx, F&& f) {
+  try {
+    f();
+    return LFG_OK;
+  } catch (const Error& e) {
+    if (ctx) ctx->last_error = e.what();
+    return e.code;
+  } catch (const std::bad_alloc&) {
+    if (ctx) ctx->last_error = "host allocation failed";
+    return LFG_ERR_NOMEM;
+  } catch (const std::exception& e) {
+    if (ctx) ctx->last_error = e.what();
+    return LFG_ERR_ARG;
+  }
+}
+
+// vector algebra launchers (lfg_core.cu)
+void vec_set(lfg_field x, Sc a);
+void vec_copy(lfg_field dst, lfg_field src);
+void vec_axpy(lfg_field x, Sc b, lfg_field y);                 // x = x + b y
+void vec_aypx(lfg_field x, Sc a, lfg_field y);                 // x = a x + y
+void vec_axpby(lfg_field z, Sc a, lfg_field x, Sc b, lfg_field y);
+void vec_scale(lfg_field x, Sc a);
+void vec_divide(lfg_field z, lfg_field x, lfg_field y);
+void vec_dot(lfg_field x, lfg_field y, int slot);               // result in slot
+// fused Krylov steps
+void vec_mgs_step(lfg_field v, lfg_field pv, lfg_field vj, lfg_field pvj, Sc alpha,
+                  lfg_field next, int slot);  // v -= a vj; pv -= a pvj; slot = <v, next or v>
+void vec_scale2_dot(lfg_field v, lfg_field pv, Sc beta, lfg_field res, int slot);
+void vec_update2_norm(lfg_field dx, lfg_field pv, lfg_field res, lfg_field v, Sc alpha,
+                      int slot);             // dx += a pv; res -= a v; slot = <res,res>
+void vec_axpy_norm(lfg_field x, Sc b, lfg_field y, int slot);   // x += b y; slot = <x,x>
+// x += b y; slot = <x, next> (next null: <x, x>)
+void vec_axpy_dot(lfg_field x, Sc b, lfg_field y, lfg_field next, int slot);
+void vec_scale_copy(lfg_field dst, Sc a, lfg_field src);        // dst = a src
+
+// Helmholtz launchers (lfg_helm.cu)
+void helm_apply(lfg_helm op, lfg_field y, lfg_field x, lfg_field dot_with, int slot);
+void helm_residual(lfg_helm op, lfg_field r, lfg_field x, lfg_field b, int norm_slot);
+// x_out = sweep(x_in [+ P xc]); x_in null: zero guess.
+void helm_smooth(lfg_helm op, double omega, lfg_field x_in, lfg_field b, lfg_field x_out,
+                 lfg_intergrid ig, lfg_field xc);
+void helm_residual_restrict(lfg_helm op, lfg_intergrid ig, lfg_field x, lfg_field b,
+                            lfg_field bc);
+void prolong_add(lfg_intergrid ig, lfg_field fine, lfg_field coarse);
+
+}  // namespace lfg

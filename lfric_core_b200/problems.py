@@ -1,0 +1,247 @@
+"""Seeded synthetic problems on the extruded cubed sphere (host-side set-up).
+
+The reference's own Helmholtz operator lives outside lfric_core, so the W3
+Helmholtz problem solved here is defined by this project, from the
+reference's building blocks:
+
+  A = T' - H_off
+    T'    : a columnwise-assembled (CMA) tridiagonal operator per column,
+            stored as columnwise_matrix(3, nlayers, ncol) (bandwidth 3, the
+            W3->W3 layout of infrastructure/source/operator/
+            columnwise_operator_mod.f90:401-413), whose diagonal already holds
+            the sum of the horizontal face couplings;
+    H_off : the symmetric coupling of every cell to its four face neighbours
+            on the same level, stored as hface(4, nlayers, ncol) in the
+            neighbour order W,S,E,N.
+
+so (A x)(c,k) = sum_j T'(j,k,c) x(c,k-2+j) - sum_f hface(f,k,c) x(nbr_f(c),k).
+A is symmetric positive definite: T (the vertical part) is symmetric and
+strictly diagonally dominant and the horizontal part is a weighted graph
+Laplacian.
+
+Vertical coefficients (one value per interface, shared by the two rows so T
+is symmetric): off-diagonal = -u * g_k with u ~ U(0,1) and g_k the mean layer
+spacing over the spacing between the centres of layers k and k+1 (the
+quadratic extrusion of extrusion_mod.f90:341-354 makes the bottom layers
+thin, so their vertical coupling is strong).  T's diagonal is ratio * (|sub|
++ |super|), ratio ~ U(1.5, 3).  Horizontal couplings: h = s * U(0.5, 1.5) *
+dz_k / mean(dz) per unique face and level (thick layers couple strongly in the
+horizontal).  Right-hand sides are N(0,1).  All draws use numpy's PCG64 from
+the given seed.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+from .mesh import EARTH_RADIUS as EARTH_RADIUS_DEFAULT
+from .mesh import CubedSphere, coarsen_map, cubed_sphere, extrusion
+
+DEFAULT_TOP = 80.0e3
+DEFAULT_H_SCALE = 4.0
+
+
+@dataclass
+class HelmholtzProblem:
+    """A W3 Helmholtz operator, right-hand side and multigrid hierarchy.
+
+    Arrays are in the reference layout: column-contiguous fields
+    (index c*nlayers + k), cm = columnwise_matrix(3, nlayers, ncol) flattened
+    in Fortran order (band fastest), hf = hface(4, nlayers, ncol) flattened in
+    Fortran order, links = (ncol, 4) 0-based W,S,E,N neighbours.
+    """
+
+    n: int
+    nlayers: int
+    cm: np.ndarray
+    hf: np.ndarray
+    links: np.ndarray
+    rhs: np.ndarray
+    mg_links: list          # links of levels 1.. (coarser meshes)
+    mg_child: list          # child[l]: (ncol_{l+1}, 2, 2) cells of level l
+
+    @property
+    def ncol(self) -> int:
+        return int(self.links.shape[0])
+
+    @property
+    def ndof(self) -> int:
+        return self.ncol * self.nlayers
+
+    @property
+    def nlevels(self) -> int:
+        return 1 + len(self.mg_child)
+
+
+def _unique_faces(links: np.ndarray):
+    """(cell, side) pairs of every face once, plus the matching far side."""
+    ncol = links.shape[0]
+    cells = np.repeat(np.arange(ncol), 4)
+    sides = np.tile(np.arange(4), ncol)
+    nbrs = links.ravel()
+    # side of the neighbour that points back at the cell
+    back = np.empty_like(sides)
+    lk = links[nbrs]                                  # (4*ncol, 4)
+    back[:] = np.argmax(lk == cells[:, None], axis=1)
+    own = cells < nbrs
+    return cells[own], sides[own], nbrs[own], back[own]
+
+
+def helmholtz_operator(surface: CubedSphere, nlayers: int, seed: int,
+                       top: float = DEFAULT_TOP, stretching: str = "quadratic",
+                       h_scale: float = DEFAULT_H_SCALE):
+    """Bands cm (3*nl*ncol), couplings hf (4*nl*ncol) and links of A."""
+    rng = np.random.default_rng(seed)
+    ncol, nl = surface.ncell, nlayers
+    z = extrusion(nl, top, stretching)
+    dz = np.diff(z)                                    # layer depths (nl,)
+    mean_dz = top / nl
+    zc = 0.5 * (z[1:] + z[:-1])
+    g = mean_dz / np.diff(zc) if nl > 1 else np.zeros(0)   # (nl-1,)
+    # Vertical interfaces: one coefficient per (column, interface k|k+1).
+    off = -rng.uniform(0.0, 1.0, size=(ncol, nl - 1)) * g[None, :]
+    sub = np.zeros((ncol, nl))
+    sup = np.zeros((ncol, nl))
+    sup[:, :-1] = off
+    sub[:, 1:] = off
+    ratio = rng.uniform(1.5, 3.0, size=(ncol, nl))
+    diag = ratio * (np.abs(sub) + np.abs(sup))
+    # A column with a single level has no vertical neighbours.
+    diag = np.where(diag == 0.0, ratio, diag)
+    # Horizontal couplings, symmetric: draw per unique face.
+    links = surface.face_links.astype(np.int32)
+    c, s, nb, bk = _unique_faces(links)
+    hval = h_scale * rng.uniform(0.5, 1.5, size=(c.size, nl)) * (dz / mean_dz)[None, :]
+    hf = np.zeros((ncol, nl, 4))
+    hf[c, :, s] = hval
+    hf[nb, :, bk] = hval
+    diag = diag + hf.sum(axis=2)
+    cm = np.stack([sub, diag, sup], axis=2)            # (ncol, nl, 3)
+    return (np.ascontiguousarray(cm).ravel(), np.ascontiguousarray(hf).ravel(), links)
+
+
+def helmholtz_problem(n: int, nlayers: int, seed: int, mg_levels: int = 4,
+                      top: float = DEFAULT_TOP, stretching: str = "quadratic",
+                      h_scale: float = DEFAULT_H_SCALE, rhs_seed: int | None = None
+                      ) -> HelmholtzProblem:
+    """Helmholtz operator on C_n x nlayers with a mg_levels-deep hierarchy."""
+    surface = cubed_sphere(n)
+    cm, hf, links = helmholtz_operator(surface, nlayers, seed, top, stretching, h_scale)
+    rng = np.random.default_rng(seed + 1000003 if rhs_seed is None else rhs_seed)
+    rhs = rng.standard_normal(surface.ncell * nlayers)
+    mg_links, mg_child = [], []
+    m = n
+    for _ in range(mg_levels - 1):
+        if m % 2:
+            raise ValueError("helmholtz_problem: n must be divisible by 2^(mg_levels-1)")
+        mg_child.append(coarsen_map(m))
+        m //= 2
+        mg_links.append(cubed_sphere(m).face_links.astype(np.int32))
+    return HelmholtzProblem(n=n, nlayers=nlayers, cm=cm, hf=hf, links=links, rhs=rhs,
+                            mg_links=mg_links, mg_child=mg_child)
+
+
+def to_level_major(v: np.ndarray, ncol: int, nlayers: int) -> np.ndarray:
+    """Reference column-contiguous field -> (level, column) layout."""
+    return np.ascontiguousarray(np.asarray(v).reshape(ncol, nlayers).T).ravel()
+
+
+def from_level_major(v: np.ndarray, ncol: int, nlayers: int) -> np.ndarray:
+    return np.ascontiguousarray(np.asarray(v).reshape(nlayers, ncol).T).ravel()
+
+
+# --------------------------------------------------------------------- W0 LMA
+# Reference hexahedron vertex order: bottom SW, SE, NE, NW then top (the
+# W0 dofmap order of ExtrudedMesh.w0_dofmap).
+_HEX = np.array([[0, 0, 0], [1, 0, 0], [1, 1, 0], [0, 1, 0],
+                 [0, 0, 1], [1, 0, 1], [1, 1, 1], [0, 1, 1]], dtype=np.float64)
+
+
+def _q1(xi):
+    """Trilinear basis (8,) and its reference gradient (8, 3) at xi (3,)."""
+    s = _HEX * xi + (1 - _HEX) * (1 - xi)                   # (8, 3) factor per axis
+    sgn = 2 * _HEX - 1
+    phi = s.prod(axis=1)
+    grad = np.stack([sgn[:, 0] * s[:, 1] * s[:, 2], s[:, 0] * sgn[:, 1] * s[:, 2],
+                     s[:, 0] * s[:, 1] * sgn[:, 2]], axis=1)
+    return phi, grad
+
+
+@dataclass
+class W0Problem:
+    """Lowest-order W0 (Q1) mass + kappa * stiffness on an extruded cubed sphere.
+
+    matrix is local_stencil(ncell*nlayers, 8, 8) flattened in Fortran order
+    (operator_mod.t90:113-119, ik = cell*nlayers + layer), map the W0 dofmap
+    (ncell, 8) of first dofs, column-contiguous (vertex*(nlayers+1) + level).
+    mass / stiff are the two parts with unit coefficient, same layout."""
+
+    ncell: int
+    nlayers: int
+    nvert: int
+    map: np.ndarray
+    mass: np.ndarray
+    stiff: np.ndarray
+    kappa: np.ndarray          # (ncell, nlayers) coefficient per 3D cell
+    rhs: np.ndarray
+
+    @property
+    def ndof(self) -> int:
+        return self.nvert * (self.nlayers + 1)
+
+    def matrix(self, kappa=None) -> np.ndarray:
+        kap = self.kappa if kappa is None else kappa
+        n3 = self.ncell * self.nlayers
+        k_ik = np.asarray(kap).reshape(n3)                  # ik = cell*nl + layer
+        m = self.mass.reshape(64, n3)
+        s = self.stiff.reshape(64, n3)
+        return (m + s * k_ik[None, :]).ravel()
+
+
+def w0_element_matrices(mesh) -> tuple[np.ndarray, np.ndarray]:
+    """Q1 mass and unit-coefficient stiffness of every hexahedron, 2x2x2 Gauss,
+    in local_stencil layout (Fortran (ncell*nl, 8, 8) flattened)."""
+    surf, nl = mesh.surface, mesh.nlayers
+    ncell = surf.ncell
+    r = mesh.radius + mesh.heights                           # (nl+1,)
+    base = surf.vertex_xyz[surf.cell_vertices]                # (ncell, 4, 3)
+    # vertices of every hex: (ncell, nl, 8, 3)
+    bot = base[:, None, :, :] * r[None, :-1, None, None]
+    top = base[:, None, :, :] * r[None, 1:, None, None]
+    X = np.concatenate([bot, top], axis=2)
+    n3 = ncell * nl
+    X = X.reshape(n3, 8, 3)
+    g = np.array([0.5 - 0.5 / np.sqrt(3.0), 0.5 + 0.5 / np.sqrt(3.0)])
+    M = np.zeros((n3, 8, 8))
+    K = np.zeros((n3, 8, 8))
+    for a in g:
+        for b in g:
+            for c in g:
+                phi, dphi = _q1(np.array([a, b, c]))
+                J = np.einsum("nia,ib->nab", X, dphi)          # (n3, 3, 3): dx_a/dxi_b
+                detJ = np.linalg.det(J)
+                Jinv = np.linalg.inv(J)                        # dxi/dx
+                gphys = np.einsum("ib,nba->nia", dphi, Jinv)   # (n3, 8, 3)
+                w = 0.125 * np.abs(detJ)
+                M += w[:, None, None] * phi[None, :, None] * phi[None, None, :]
+                K += w[:, None, None] * np.einsum("nia,nja->nij", gphys, gphys)
+    # local_stencil(ik, df, df2): Fortran order, ik fastest
+    to_f = lambda A: np.ascontiguousarray(A.transpose(1, 2, 0)).reshape(8, 8, n3).transpose(1, 0, 2).ravel()
+    return to_f(M), to_f(K)
+
+
+def w0_problem(n: int, nlayers: int, seed: int, top: float, kappa_sigma: float = 0.0,
+               stretching: str = "uniform", radius: float = EARTH_RADIUS_DEFAULT) -> W0Problem:
+    """W0 diffusion problem: A = M + kappa K; kappa = exp(sigma g), g ~ N(0,1)
+    per 3D cell (kappa = 1 when sigma = 0); right-hand side N(0,1)."""
+    from .mesh import extruded_mesh
+    mesh = extruded_mesh(n, nlayers, top, stretching, radius=radius)
+    mass, stiff = w0_element_matrices(mesh)
+    rng = np.random.default_rng(seed)
+    ncell = mesh.ncell
+    kappa = (np.exp(kappa_sigma * rng.standard_normal((ncell, nlayers)))
+             if kappa_sigma > 0 else np.ones((ncell, nlayers)))
+    rhs = rng.standard_normal(mesh.w0_ndof())
+    return W0Problem(ncell=ncell, nlayers=nlayers, nvert=mesh.surface.nvert,
+                     map=mesh.w0_dofmap(), mass=mass, stiff=stiff, kappa=kappa, rhs=rhs)

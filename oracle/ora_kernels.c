@@ -1,0 +1,439 @@
+/*
+ * Oracle: CPU restatement of the reference's per-column kernels.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA path: it
+ * is compiled into oracle/liblfg_oracle.so, which only the tests, the smoke
+ * check and the CPU-baseline leg of the benchmark load.  No product code path
+ * calls it.
+ *
+ * Every routine keeps the reference's calling convention: Fortran 1-based
+ * dofmaps, column-major arrays, one call per horizontal cell (the PSy layer
+ * loops over cells).  Each one cites the reference routine it restates.
+ * Array macros: A2(a,i,j,n1) is a(i,j) of a(n1,*); A3(a,i,j,k,n1,n2) is
+ * a(i,j,k) of a(n1,n2,*); V(a,i) is a(i) -- all 1-based.
+ */
+#include <math.h>
+#include <stddef.h>
+#include "lfg_oracle.h"
+
+#define V(a, i) (a)[(size_t)(i) - 1]
+#define A2(a, i, j, n1) (a)[((size_t)(i) - 1) + (size_t)(n1) * ((size_t)(j) - 1)]
+#define A3(a, i, j, k, n1, n2) \
+  (a)[((size_t)(i) - 1) + (size_t)(n1) * (((size_t)(j) - 1) + (size_t)(n2) * ((size_t)(k) - 1))]
+
+/* ------------------------------------------------------------------------
+ * LMA kernels.
+ * ---------------------------------------------------------------------- */
+
+/* components/science/source/kernel/algebra/matrix_vector_kernel_mod.F90:68-140
+ * lhs(map1(df)+k) += matrix(ik+k, df, df2) * x(map2(df2)+k), df2 outer. */
+#define DEF_MATRIX_VECTOR(T, SFX)                                                     \
+  void ora_matrix_vector_code_##SFX(int cell, int nlayers, T* lhs, const T* x,        \
+                                    int ncell_3d, const T* matrix, int ndf1,          \
+                                    int undf1, const int* map1, int ndf2, int undf2,  \
+                                    const int* map2) {                                \
+    (void)undf1; (void)undf2;                                                         \
+    int ik = (cell - 1) * nlayers + 1;                                                \
+    for (int df2 = 1; df2 <= ndf2; ++df2) {                                           \
+      int i2 = V(map2, df2);                                                          \
+      for (int df = 1; df <= ndf1; ++df) {                                            \
+        int i1 = V(map1, df);                                                         \
+        for (int k = 0; k < nlayers; ++k)                                             \
+          V(lhs, i1 + k) = V(lhs, i1 + k) +                                           \
+                           A3(matrix, ik + k, df, df2, ncell_3d, ndf1) * V(x, i2 + k); \
+      }                                                                               \
+    }                                                                                 \
+  }
+DEF_MATRIX_VECTOR(double, r_double)
+DEF_MATRIX_VECTOR(float, r_single)
+
+/* components/science/source/kernel/algebra/dg_matrix_vector_kernel_mod.F90:68-154
+ * As matrix_vector but lhs is zeroed on the cell's dofs first. */
+#define DEF_DG_MATRIX_VECTOR(T, SFX)                                                  \
+  void ora_dg_matrix_vector_code_##SFX(int cell, int nlayers, T* lhs, const T* x,     \
+                                       int ncell_3d, const T* matrix, int ndf1,       \
+                                       int undf1, const int* map1, int ndf2,          \
+                                       int undf2, const int* map2) {                  \
+    for (int df1 = 1; df1 <= ndf1; ++df1) {                                           \
+      int i1 = V(map1, df1);                                                          \
+      for (int k = 0; k < nlayers; ++k) V(lhs, i1 + k) = (T)0;                        \
+    }                                                                                 \
+    ora_matrix_vector_code_##SFX(cell, nlayers, lhs, x, ncell_3d, matrix, ndf1,       \
+                                 undf1, map1, ndf2, undf2, map2);                     \
+  }
+DEF_DG_MATRIX_VECTOR(double, r_double)
+DEF_DG_MATRIX_VECTOR(float, r_single)
+
+/* components/science/source/kernel/algebra/transpose_matrix_vector_kernel_mod.F90:66-144
+ * matrix is (ncell_3d, ndf2, ndf1); lhs(map1(df)+k) += sum_df2 matrix(ik,df2,df) x_e(df2),
+ * computed per level as lhs_e = matmul(transpose(matrix(ik,:,:)), x_e). */
+#define DEF_TRANSPOSE_MATRIX_VECTOR(T, SFX)                                           \
+  void ora_transpose_matrix_vector_code_##SFX(int cell, int nlayers, T* lhs,          \
+                                              const T* x, int ncell_3d,               \
+                                              const T* matrix, int ndf1, int undf1,   \
+                                              const int* map1, int ndf2, int undf2,   \
+                                              const int* map2) {                      \
+    (void)undf1; (void)undf2;                                                         \
+    for (int k = 0; k < nlayers; ++k) {                                               \
+      int ik = (cell - 1) * nlayers + k + 1;                                          \
+      for (int df = 1; df <= ndf1; ++df) {                                            \
+        T acc = (T)0;                                                                 \
+        for (int df2 = 1; df2 <= ndf2; ++df2)                                         \
+          acc += A3(matrix, ik, df2, df, ncell_3d, ndf2) * V(x, V(map2, df2) + k);    \
+        V(lhs, V(map1, df) + k) = V(lhs, V(map1, df) + k) + acc;                      \
+      }                                                                               \
+    }                                                                                 \
+  }
+DEF_TRANSPOSE_MATRIX_VECTOR(double, r_double)
+DEF_TRANSPOSE_MATRIX_VECTOR(float, r_single)
+
+/* components/science/source/kernel/algebra/sci_mm_diagonal_kernel_mod.F90:68-127 */
+#define DEF_MM_DIAGONAL(T, SFX)                                                       \
+  void ora_mm_diagonal_code_##SFX(int cell, int nlayers, T* mm_diag, int ncell_3d,    \
+                                  const T* mass_matrix, int ndf, int undf,            \
+                                  const int* map) {                                   \
+    (void)undf;                                                                       \
+    for (int k = 0; k < nlayers; ++k) {                                               \
+      int ik = (cell - 1) * nlayers + k + 1;                                          \
+      for (int df = 1; df <= ndf; ++df)                                               \
+        V(mm_diag, V(map, df) + k) =                                                  \
+            V(mm_diag, V(map, df) + k) + A3(mass_matrix, ik, df, df, ncell_3d, ndf);  \
+    }                                                                                 \
+  }
+DEF_MM_DIAGONAL(double, r_double)
+DEF_MM_DIAGONAL(float, r_single)
+
+/* ------------------------------------------------------------------------
+ * CMA kernels (r_solver: both kinds provided).
+ * ---------------------------------------------------------------------- */
+
+/* Fortran ceiling/floor of (num / den) computed in r_solver as the reference
+ * does: ceiling((alpha*i-gamma_p)/(1.0_r_solver*beta), i_def). */
+#define DEF_CMA_APP(T, SFX)                                                           \
+  void ora_columnwise_op_app_code_##SFX(                                              \
+      int cell, int ncell_2d, T* lhs, const T* x, const T* columnwise_matrix,         \
+      int nrow, int ncol, int bandwidth, int alpha, int beta, int gamma_m,            \
+      int gamma_p, int ndf1, int undf1, const int* map1,                              \
+      const int* indirection_dofmap_to, int ndf2, int undf2, const int* map2,         \
+      const int* indirection_dofmap_from) {                                           \
+    (void)ncell_2d; (void)ndf1; (void)undf1; (void)ndf2; (void)undf2;                 \
+    for (int i = 1; i <= nrow; ++i) {                                                 \
+      int mu_i = V(map1, 1) + V(indirection_dofmap_to, i) - 1;                        \
+      int j_minus = (int)ceil((T)(alpha * i - gamma_p) / ((T)1 * (T)beta));           \
+      int j_plus = (int)floor((T)(alpha * i + gamma_m) / ((T)1 * (T)beta));           \
+      int jlo = j_minus > 1 ? j_minus : 1;                                            \
+      int jhi = j_plus < ncol ? j_plus : ncol;                                        \
+      for (int j = jlo; j <= jhi; ++j) {                                              \
+        int mu_j = V(map2, 1) + V(indirection_dofmap_from, j) - 1;                    \
+        V(lhs, mu_i) = V(lhs, mu_i) +                                                 \
+            A3(columnwise_matrix, j - j_minus + 1, i, cell, bandwidth, nrow) * V(x, mu_j); \
+      }                                                                               \
+    }                                                                                 \
+  }
+DEF_CMA_APP(double, r_double)
+DEF_CMA_APP(float, r_single)
+
+/* components/science/source/kernel/columnwise_operators/sci_columnwise_op_appinv_kernel_mod.F90:77-145
+ * Thomas algorithm; lhs is overwritten with the solution. */
+#define DEF_CMA_APPINV(T, SFX)                                                        \
+  void ora_columnwise_op_appinv_code_##SFX(                                           \
+      int cell, int ncell_2d, T* lhs, const T* x, const T* columnwise_matrix,         \
+      int nrow, int bandwidth, int alpha, int beta, int gamma_m, int gamma_p,         \
+      int ndf, int undf, const int* map, const int* indirection_dofmap,               \
+      T* c_prime, T* d_prime) {                                                       \
+    (void)ncell_2d; (void)alpha; (void)beta; (void)gamma_m; (void)gamma_p;            \
+    (void)ndf; (void)undf;                                                            \
+    T inv_denom;                                                                      \
+    for (int i = 1; i <= nrow; ++i) {                                                 \
+      int mu_i = V(map, 1) + V(indirection_dofmap, i) - 1;                            \
+      const T a1 = A3(columnwise_matrix, 1, i, cell, bandwidth, nrow);                \
+      const T a2 = A3(columnwise_matrix, 2, i, cell, bandwidth, nrow);                \
+      const T a3 = A3(columnwise_matrix, 3, i, cell, bandwidth, nrow);                \
+      if (i == 1) {                                                                   \
+        inv_denom = (T)1 / a2;                                                        \
+        V(c_prime, i) = inv_denom * a3;                                               \
+        V(d_prime, i) = inv_denom * V(x, mu_i);                                       \
+      } else {                                                                        \
+        inv_denom = (T)1 / (a2 - a1 * V(c_prime, i - 1));                             \
+        if (i < nrow) V(c_prime, i) = inv_denom * a3;                                 \
+        V(d_prime, i) = inv_denom * (V(x, mu_i) - a1 * V(d_prime, i - 1));            \
+      }                                                                               \
+    }                                                                                 \
+    for (int i = nrow; i >= 1; --i) {                                                 \
+      int mu_i = V(map, 1) + V(indirection_dofmap, i) - 1;                            \
+      if (i < nrow) V(d_prime, i) = V(d_prime, i) - V(c_prime, i) * V(d_prime, i + 1);\
+      V(lhs, mu_i) = V(d_prime, i);                                                   \
+    }                                                                                 \
+  }
+DEF_CMA_APPINV(double, r_double)
+DEF_CMA_APPINV(float, r_single)
+
+/* components/science/source/kernel/solver/sci_tri_solve_kernel_mod.f90:72-156 */
+#define DEF_TRI_SOLVE(T, SFX)                                                         \
+  void ora_tri_solve_code_##SFX(int nlayers, T* y, const T* x, const T* tri_0,        \
+                                const T* tri_plus, const T* tri_minus, int ndf,       \
+                                int undf, const int* map, T* x_new,                   \
+                                T* tri_plus_new) {                                    \
+    (void)ndf; (void)undf;                                                            \
+    int k = 0;                                                                        \
+    int ij = V(map, 1);                                                               \
+    T denom = (T)1 / V(tri_0, ij + k);                                                \
+    V(tri_plus_new, 1) = V(tri_plus, ij + k) * denom;                                 \
+    V(x_new, 1) = V(x, ij + k) * denom;                                               \
+    for (k = 1; k <= nlayers - 1; ++k) {                                              \
+      denom = (T)1 / (V(tri_0, ij + k) - V(tri_minus, ij + k) * V(tri_plus_new, k));  \
+      V(tri_plus_new, k + 1) = V(tri_plus, ij + k) * denom;                           \
+      V(x_new, k + 1) = (V(x, ij + k) - V(tri_minus, ij + k) * V(x_new, k)) * denom;  \
+    }                                                                                 \
+    k = nlayers - 1;                                                                  \
+    V(y, ij + k) = V(x_new, k + 1);                                                   \
+    for (k = nlayers - 2; k >= 0; --k)                                                \
+      V(y, ij + k) = V(x_new, k + 1) - V(tri_plus_new, k + 1) * V(y, ij + k + 1);     \
+  }
+DEF_TRI_SOLVE(double, r_double)
+DEF_TRI_SOLVE(float, r_single)
+
+/* components/science/source/kernel/solver/sci_operator_tri_solve_kernel_mod.f90:69-120
+ * Tridiagonal of nlayers+1 rows assembled from the 2x2 LMA, then Thomas.
+ * Work arrays are indexed 0..nlayers (length nlayers+1 each). */
+void ora_operator_tri_solve_code(int cell, int nlayers, double* y, const double* x,
+                                 int ncell, const double* matrix, int ndf, int undf,
+                                 const int* map, double* work) {
+  (void)undf;
+  double* tri_p = work;
+  double* tri_0 = work + (nlayers + 1);
+  double* tri_m = work + 2 * (nlayers + 1);
+  double* x_new = work + 3 * (nlayers + 1);
+  double* tri_p_new = work + 4 * (nlayers + 1);
+  tri_0[0] = 0.0;
+  tri_m[0] = 0.0;
+  for (int k = 0; k <= nlayers - 1; ++k) {
+    int ik = 1 + k + (cell - 1) * nlayers;
+    tri_0[k] = A3(matrix, ik, 1, 1, ncell, ndf) + tri_0[k];
+    tri_p[k] = A3(matrix, ik, 1, 2, ncell, ndf);
+    tri_m[k + 1] = A3(matrix, ik, 2, 1, ncell, ndf);
+    tri_0[k + 1] = A3(matrix, ik, 2, 2, ncell, ndf);
+  }
+  tri_p[nlayers] = 0.0;
+  int k = 0;
+  int ij = V(map, 1);
+  double denom = 1.0 / tri_0[k];
+  tri_p_new[k] = tri_p[k] * denom;
+  x_new[k] = V(x, ij + k) * denom;
+  for (k = 1; k <= nlayers; ++k) {
+    denom = 1.0 / (tri_0[k] - tri_m[k] * tri_p_new[k - 1]);
+    tri_p_new[k] = tri_p[k] * denom;
+    x_new[k] = (V(x, ij + k) - tri_m[k] * x_new[k - 1]) * denom;
+  }
+  k = nlayers;
+  V(y, ij + k) = x_new[k];
+  for (k = nlayers - 1; k >= 0; --k) V(y, ij + k) = x_new[k] - tri_p_new[k] * V(y, ij + k + 1);
+}
+
+/* ------------------------------------------------------------------------
+ * Intergrid kernels.  cell_map is cell_map(nx, ny), Fortran order, 1-based
+ * fine cell ids; map_fine is map_fine(ndf, ncell_fine).
+ * ---------------------------------------------------------------------- */
+
+/* sci_restrict_scalar_unweighted_kernel_mod.F90:71-183 */
+#define DEF_RESTRICT_UNWEIGHTED(T, SFX)                                               \
+  void ora_restrict_scalar_unweighted_code_##SFX(                                     \
+      int nlayers, const int* cell_map, int nx, int ny, int ncell_fine, T* coarse,    \
+      const T* fine, int undf_coarse, const int* map_coarse, int ndf, int undf_fine,  \
+      const int* map_fine, T* coarse_value) {                                         \
+    (void)ncell_fine; (void)undf_coarse; (void)undf_fine;                             \
+    T denom = (T)1 / (T)(nx * ny);                                                    \
+    int top_df = nlayers - 2 + ndf;                                                   \
+    for (int k = 0; k <= top_df; ++k) coarse_value[k] = (T)0;                         \
+    for (int y = 1; y <= ny; ++y)                                                     \
+      for (int x = 1; x <= nx; ++x) {                                                 \
+        int c = A2(cell_map, x, y, nx);                                               \
+        for (int k = 0; k <= top_df; ++k)                                             \
+          coarse_value[k] = coarse_value[k] + V(fine, A2(map_fine, 1, c, ndf) + k) * denom; \
+      }                                                                               \
+    for (int k = 0; k <= top_df; ++k) V(coarse, V(map_coarse, 1) + k) = coarse_value[k]; \
+  }
+DEF_RESTRICT_UNWEIGHTED(double, r_double)
+DEF_RESTRICT_UNWEIGHTED(float, r_single)
+
+/* sci_restrict_scalar_weighted_kernel_mod.F90:77-196: fine * denom / weights */
+#define DEF_RESTRICT_WEIGHTED(T, SFX)                                                 \
+  void ora_restrict_scalar_weighted_code_##SFX(                                       \
+      int nlayers, const int* cell_map, int nx, int ny, int ncell_fine, T* coarse,    \
+      const T* fine, const T* weights, int undf_coarse, const int* map_coarse,        \
+      int ndf, int undf_fine, const int* map_fine, T* coarse_value) {                 \
+    (void)ncell_fine; (void)undf_coarse; (void)undf_fine;                             \
+    T denom = (T)1 / (T)(nx * ny);                                                    \
+    int top_df = nlayers - 2 + ndf;                                                   \
+    for (int k = 0; k <= top_df; ++k) coarse_value[k] = (T)0;                         \
+    for (int y = 1; y <= ny; ++y)                                                     \
+      for (int x = 1; x <= nx; ++x) {                                                 \
+        int c = A2(cell_map, x, y, nx);                                               \
+        for (int k = 0; k <= top_df; ++k) {                                           \
+          int d = A2(map_fine, 1, c, ndf) + k;                                        \
+          coarse_value[k] = coarse_value[k] + V(fine, d) * denom / V(weights, d);     \
+        }                                                                             \
+      }                                                                               \
+    for (int k = 0; k <= top_df; ++k) V(coarse, V(map_coarse, 1) + k) = coarse_value[k]; \
+  }
+DEF_RESTRICT_WEIGHTED(double, r_double)
+DEF_RESTRICT_WEIGHTED(float, r_single)
+
+/* sci_restrict_mass_w3_kernel_mod.F90:70-179: plain sum of the fine values */
+#define DEF_RESTRICT_MASS_W3(T, SFX)                                                  \
+  void ora_restrict_mass_w3_code_##SFX(                                               \
+      int nlayers, const int* cell_map, int nx, int ny, int ncell_fine, T* coarse,    \
+      const T* fine, int undf_coarse, const int* map_coarse, int ndf, int undf_fine,  \
+      const int* map_fine, T* coarse_value) {                                         \
+    (void)ncell_fine; (void)undf_coarse; (void)undf_fine;                             \
+    int top_df = nlayers - 2 + ndf;                                                   \
+    for (int k = 0; k <= top_df; ++k) coarse_value[k] = (T)0;                         \
+    for (int y = 1; y <= ny; ++y)                                                     \
+      for (int x = 1; x <= nx; ++x) {                                                 \
+        int c = A2(cell_map, x, y, nx);                                               \
+        for (int k = 0; k <= top_df; ++k)                                             \
+          coarse_value[k] = coarse_value[k] + V(fine, A2(map_fine, 1, c, ndf) + k);   \
+      }                                                                               \
+    for (int k = 0; k <= top_df; ++k) V(coarse, V(map_coarse, 1) + k) = coarse_value[k]; \
+  }
+DEF_RESTRICT_MASS_W3(double, r_double)
+DEF_RESTRICT_MASS_W3(float, r_single)
+
+/* sci_prolong_scalar_unweighted_kernel_mod.F90:74-169: fine += coarse */
+#define DEF_PROLONG_UNWEIGHTED(T, SFX)                                                \
+  void ora_prolong_scalar_unweighted_code_##SFX(                                      \
+      int nlayers, const int* cell_map, int nx, int ny, int ncell_fine, T* fine,      \
+      const T* coarse, int ndf, int undf_fine, const int* map_fine, int undf_coarse,  \
+      const int* map_coarse) {                                                        \
+    (void)ncell_fine; (void)undf_coarse; (void)undf_fine;                             \
+    int top_df = nlayers - 2 + ndf;                                                   \
+    for (int y = 1; y <= ny; ++y)                                                     \
+      for (int x = 1; x <= nx; ++x) {                                                 \
+        int c = A2(cell_map, x, y, nx);                                               \
+        for (int k = 0; k <= top_df; ++k) {                                           \
+          int d = A2(map_fine, 1, c, ndf) + k;                                        \
+          V(fine, d) = V(fine, d) + V(coarse, V(map_coarse, 1) + k);                  \
+        }                                                                             \
+      }                                                                               \
+  }
+DEF_PROLONG_UNWEIGHTED(double, r_double)
+DEF_PROLONG_UNWEIGHTED(float, r_single)
+
+/* sci_prolong_scalar_weighted_kernel_mod.F90:77-178: fine += weights * coarse */
+#define DEF_PROLONG_WEIGHTED(T, SFX)                                                  \
+  void ora_prolong_scalar_weighted_code_##SFX(                                        \
+      int nlayers, const int* cell_map, int nx, int ny, int ncell_fine, T* fine,      \
+      const T* coarse, const T* weights, int ndf, int undf_fine, const int* map_fine, \
+      int undf_coarse, const int* map_coarse) {                                       \
+    (void)ncell_fine; (void)undf_coarse; (void)undf_fine;                             \
+    int top_df = nlayers - 2 + ndf;                                                   \
+    for (int y = 1; y <= ny; ++y)                                                     \
+      for (int x = 1; x <= nx; ++x) {                                                 \
+        int c = A2(cell_map, x, y, nx);                                               \
+        for (int k = 0; k <= top_df; ++k) {                                           \
+          int d = A2(map_fine, 1, c, ndf) + k;                                        \
+          V(fine, d) = V(fine, d) + V(weights, d) * V(coarse, V(map_coarse, 1) + k);  \
+        }                                                                             \
+      }                                                                               \
+  }
+DEF_PROLONG_WEIGHTED(double, r_double)
+DEF_PROLONG_WEIGHTED(float, r_single)
+
+enum { SWB = 1, SEB = 2, NEB = 3, NWB = 4 };
+
+/* sci_restrict_w0_kernel_mod.F90:75-154: injection of the four coarse
+ * bottom corners from the corner fine cells, levels 0..nlayers. */
+void ora_restrict_w0_code(int nlayers, const int* cell_map, int nx, int ny, int ncell_fine,
+                          double* coarse, const double* fine, int undf_coarse,
+                          const int* map_coarse, int ndf, int undf_fine,
+                          const int* map_fine) {
+  (void)ncell_fine; (void)undf_coarse; (void)undf_fine;
+  for (int k = 0; k <= nlayers; ++k) {
+    V(coarse, V(map_coarse, NWB) + k) = V(fine, A2(map_fine, NWB, A2(cell_map, 1, 1, nx), ndf) + k);
+    V(coarse, V(map_coarse, SWB) + k) = V(fine, A2(map_fine, SWB, A2(cell_map, 1, ny, nx), ndf) + k);
+    V(coarse, V(map_coarse, NEB) + k) = V(fine, A2(map_fine, NEB, A2(cell_map, nx, 1, nx), ndf) + k);
+    V(coarse, V(map_coarse, SEB) + k) = V(fine, A2(map_fine, SEB, A2(cell_map, nx, ny, nx), ndf) + k);
+  }
+}
+
+/* sci_prolong_w0_kernel_mod.F90:76-194: bilinear weights from the four
+ * coarse corners; SE dofs on the last column, NW dofs on the first row and
+ * the NE dof of the NE fine cell are filled as well. */
+void ora_prolong_w0_code(int nlayers, const int* cell_map, int nx, int ny, int ncell_fine,
+                         double* fine, const double* coarse, int ndf, int undf_fine,
+                         const int* map_fine, int undf_coarse, const int* map_coarse) {
+  (void)ncell_fine; (void)undf_fine; (void)undf_coarse;
+  for (int y = 1; y <= ny; ++y) {
+    for (int x = 1; x <= nx; ++x) {
+      int c = A2(cell_map, x, y, nx);
+      double w_sw = (double)y * (double)(nx - x + 1) / (double)(nx * ny);
+      double w_nw = (double)(ny - y) * (double)(nx - x + 1) / (double)(nx * ny);
+      double w_ne = (double)(ny - y) * (double)(x - 1) / (double)(nx * ny);
+      double w_se = (double)y * (double)(x - 1) / (double)(nx * ny);
+      for (int k = 0; k <= nlayers; ++k)
+        V(fine, A2(map_fine, SWB, c, ndf) + k) =
+            w_ne * V(coarse, V(map_coarse, NEB) + k) + w_se * V(coarse, V(map_coarse, SEB) + k) +
+            w_sw * V(coarse, V(map_coarse, SWB) + k) + w_nw * V(coarse, V(map_coarse, NWB) + k);
+      if (x == nx) {
+        w_se = (double)y / (double)ny;
+        w_ne = 1.0 - w_se;
+        for (int k = 0; k <= nlayers; ++k)
+          V(fine, A2(map_fine, SEB, c, ndf) + k) =
+              w_ne * V(coarse, V(map_coarse, NEB) + k) + w_se * V(coarse, V(map_coarse, SEB) + k);
+      }
+      if (y == 1) {
+        w_nw = (double)(nx - x + 1) / (double)nx;
+        w_ne = 1.0 - w_nw;
+        for (int k = 0; k <= nlayers; ++k)
+          V(fine, A2(map_fine, NWB, c, ndf) + k) =
+              w_ne * V(coarse, V(map_coarse, NEB) + k) + w_nw * V(coarse, V(map_coarse, NWB) + k);
+        if (x == nx)
+          for (int k = 0; k <= nlayers; ++k)
+            V(fine, A2(map_fine, NEB, c, ndf) + k) = V(coarse, V(map_coarse, NEB) + k);
+      }
+    }
+  }
+}
+
+/* ------------------------------------------------------------------------
+ * CMA parameters: infrastructure/source/operator/columnwise_operator_mod.f90
+ * :170-198 (alpha, beta, gamma, gcd division, bandwidth), :350-396
+ * (indirection maps) and :427-470 (nrow, ncol), for horizontally
+ * discontinuous spaces whose cell dofmap is [bottom face..., interior...,
+ * top face...] offsets from the first dof (passed as dof_offsets, 0-based
+ * offsets relative to the first dof, ndof_cell entries each).
+ * out = {alpha, beta, gamma_m, gamma_p, bandwidth, nrow, ncol}.
+ * ---------------------------------------------------------------------- */
+static int gcd_int(int a, int b) {
+  while (b) { int t = a % b; a = b; b = t; }
+  return a;
+}
+
+void ora_cma_params(int nlayers, int nint_to, int nface_to, int nint_from, int nface_from,
+                    const int* offsets_to, const int* offsets_from, int* out,
+                    int* indirection_to, int* indirection_from) {
+  int ncell_to = nint_to + 2 * nface_to, ncell_from = nint_from + 2 * nface_from;
+  int alpha = nint_from + nface_from;
+  int beta = nint_to + nface_to;
+  int gamma_m = (ncell_from - 1) * (nint_to + nface_to);
+  int gamma_p = (ncell_to - 1) * (nint_from + nface_from);
+  int g = gcd_int(alpha, beta);
+  alpha /= g; beta /= g; gamma_m /= g; gamma_p /= g;
+  int bw = 1 + (int)ceil((double)(gamma_m + gamma_p) / (double)beta);
+  int nrow = nlayers * nint_to + (nlayers + 1) * nface_to;
+  int ncol = nlayers * nint_from + (nlayers + 1) * nface_from;
+  out[0] = alpha; out[1] = beta; out[2] = gamma_m; out[3] = gamma_p;
+  out[4] = bw; out[5] = nrow; out[6] = ncol;
+  for (int k = 1; k <= nlayers; ++k) {
+    for (int df = 1; df <= ncell_to; ++df) {
+      int col = offsets_to[df - 1] + 1 + (k - 1);
+      int banded = (k - 1) * (nint_to + nface_to) + df;
+      indirection_to[banded - 1] = col;
+    }
+    for (int df = 1; df <= ncell_from; ++df) {
+      int col = offsets_from[df - 1] + 1 + (k - 1);
+      int banded = (k - 1) * (nint_from + nface_from) + df;
+      indirection_from[banded - 1] = col;
+    }
+  }
+}

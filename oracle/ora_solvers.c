@@ -1,0 +1,144 @@
+/*
+ * Oracle: whole-mesh operators, multigrid and Krylov solvers.
+ * TEST INFRASTRUCTURE ONLY (see lfg_oracle.h).
+ */
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include "lfg_oracle.h"
+
+#define ORA_MAX_NL 4096
+
+#define REAL double
+#define S d
+#define APPINV ora_columnwise_op_appinv_code_r_double
+#include "ora_real.inc"
+#undef REAL
+#undef S
+#undef APPINV
+
+#define REAL float
+#define S f
+#define APPINV ora_columnwise_op_appinv_code_r_single
+#include "ora_real.inc"
+#undef REAL
+#undef S
+#undef APPINV
+
+/* Galerkin coarse operator R A P (project-defined multigrid set-up).
+ * child is (ncoarse, 2(y), 2(x)) with y N->S, x W->E in each coarse cell's
+ * local frame, which the children share.  Coarse bands are sums over the
+ * children (y outer, x inner); the couplings between two children of the
+ * same coarse cell leave the diagonal; a coarse face's coupling is the sum
+ * of the two fine faces that make it up. */
+void ora_galerkin_coarsen(const ora_helm_d* fine, int ncoarse, const int* child,
+                          const int* links_coarse, double* cm_c, double* hf_c) {
+  (void)links_coarse;
+  const int nl = fine->nl;
+  /* children on each side (y, x): W: x=0, S: y=1, E: x=1, N: y=0 */
+  static const int side_q[4][2] = {{0, 2}, {2, 3}, {1, 3}, {0, 1}};
+  for (int C = 0; C < ncoarse; ++C) {
+    const int* ch = child + C * 4;
+    for (int k = 0; k < nl; ++k) {
+      for (int b = 0; b < 3; ++b) {
+        double acc = 0.0;
+        for (int q = 0; q < 4; ++q) acc = acc + fine->cm[((long)ch[q] * nl + k) * 3 + b];
+        cm_c[((long)C * nl + k) * 3 + b] = acc;
+      }
+      double dg = cm_c[((long)C * nl + k) * 3 + 1];
+      for (int q = 0; q < 4; ++q)
+        for (int f = 0; f < 4; ++f) {
+          int nb = fine->links[ch[q] * 4 + f];
+          if (nb == ch[0] || nb == ch[1] || nb == ch[2] || nb == ch[3])
+            dg = dg - fine->hf[((long)ch[q] * nl + k) * 4 + f];
+        }
+      cm_c[((long)C * nl + k) * 3 + 1] = dg;
+      for (int f = 0; f < 4; ++f)
+        hf_c[((long)C * nl + k) * 4 + f] = fine->hf[((long)ch[side_q[f][0]] * nl + k) * 4 + f] +
+                                           fine->hf[((long)ch[side_q[f][1]] * nl + k) * 4 + f];
+    }
+  }
+}
+
+void ora_diag_prec_apply(void* ctx, const double* x, double* y) {
+  const ora_diag_prec* p = (const ora_diag_prec*)ctx;
+  for (long i = 0; i < p->n; ++i) y[i] = x[i] / p->diag[i];
+}
+
+void ora_null_prec_apply(void* ctx, const double* x, double* y) {
+  const ora_null_ctx* p = (const ora_null_ctx*)ctx;
+  memcpy(y, x, sizeof(double) * p->n);
+}
+
+void ora_lma_apply_cb(void* vop, const double* x, double* y) {
+  const ora_lma* op = (const ora_lma*)vop;
+  memset(y, 0, sizeof(double) * op->undf);
+  for (int cell = 1; cell <= op->ncell; ++cell)
+    ora_matrix_vector_code_r_double(cell, op->nlayers, y, x, op->ncell * op->nlayers,
+                                    op->matrix, op->ndf, op->undf,
+                                    op->map + (long)(cell - 1) * op->ndf, op->ndf, op->undf,
+                                    op->map + (long)(cell - 1) * op->ndf);
+}
+
+/* y = A^T x over the mesh with the transpose_matrix_vector kernel, which
+ * reads the matrix as (ncell_3d, ndf2, ndf1); for a square LMA that is the
+ * transpose of the matrix_vector apply. */
+void ora_lma_apply_transpose(const ora_lma* op, const double* x, double* y) {
+  memset(y, 0, sizeof(double) * op->undf);
+  for (int cell = 1; cell <= op->ncell; ++cell)
+    ora_transpose_matrix_vector_code_r_double(cell, op->nlayers, y, x,
+                                              op->ncell * op->nlayers, op->matrix, op->ndf,
+                                              op->undf, op->map + (long)(cell - 1) * op->ndf,
+                                              op->ndf, op->undf,
+                                              op->map + (long)(cell - 1) * op->ndf);
+}
+
+void ora_lma_diagonal(const ora_lma* op, double* diag) {
+  memset(diag, 0, sizeof(double) * op->undf);
+  for (int cell = 1; cell <= op->ncell; ++cell)
+    ora_mm_diagonal_code_r_double(cell, op->nlayers, diag, op->ncell * op->nlayers,
+                                  op->matrix, op->ndf, op->undf,
+                                  op->map + (long)(cell - 1) * op->ndf);
+}
+
+/* Mixed-precision iterative refinement (project-defined).
+ *   x = 0, r = b
+ *   repeat: e = GCR_32(A_32, MG_32; r as float) from zero to inner_tol,
+ *           x += e (FP64), r = b - A_64 x (FP64), stop when ||r||/||b|| <= tol. */
+int ora_mixed_gcr_mg_solve(const ora_helm_d* op64, ora_mg_f* mg32, const double* b,
+                           double* x, double tol, int max_outer, int gcrk, double inner_tol,
+                           int inner_max_iter, ora_mixed_info* info) {
+  const long n = (long)op64->ncol * op64->nl;
+  double* r = (double*)malloc(sizeof(double) * n);
+  float* r32 = (float*)malloc(sizeof(float) * n);
+  float* e32 = (float*)malloc(sizeof(float) * n);
+  float* work = (float*)malloc(sizeof(float) * (2 * gcrk + 3) * n);
+  ora_helm_f* op32 = &mg32->op[0];
+  int status = ORA_NOT_CONVERGED;
+  memset(x, 0, sizeof(double) * n);
+  memcpy(r, b, sizeof(double) * n);
+  const double nb = ora_norm_d(n, b);
+  info->outer_iterations = 0;
+  info->inner_iterations = 0;
+  info->final_rel_residual = nb > 0 ? 1.0 : 0.0;
+  if (nb < DBL_EPSILON) { status = ORA_OK; goto done; }
+  for (int o = 1; o <= max_outer; ++o) {
+    for (long i = 0; i < n; ++i) r32[i] = (float)r[i];
+    memset(e32, 0, sizeof(float) * n);
+    ora_solve_info si;
+    int st = ora_gcr_solve_f(n, ora_helm_apply_cb_f, op32, ora_mg_apply_cb_f, mg32, gcrk,
+                             inner_tol, 0.0, inner_max_iter, 1, e32, r32, work, &si);
+    info->inner_iterations += si.iterations;
+    info->outer_iterations = o;
+    if (st == ORA_NAN) { status = ORA_NAN; goto done; }
+    for (long i = 0; i < n; ++i) x[i] = x[i] + (double)e32[i];
+    ora_helm_residual_d(op64, x, b, r);
+    info->final_rel_residual = ora_norm_d(n, r) / nb;
+    if (isnan(info->final_rel_residual)) { status = ORA_NAN; goto done; }
+    if (info->final_rel_residual <= tol) { status = ORA_OK; goto done; }
+  }
+done:
+  free(r); free(r32); free(e32); free(work);
+  return status;
+}

@@ -1,0 +1,203 @@
+"""ctypes front end of the oracle library (oracle/liblfg_oracle.so).
+
+TEST INFRASTRUCTURE ONLY: imported by tests/, by the smoke check and by the
+CPU-baseline leg of bench.py, never by the product package.  It builds the
+oracle from source on first use if the shared library is missing.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liblfg_oracle.so"
+
+_dp = C.POINTER(C.c_double)
+_fp = C.POINTER(C.c_float)
+_ip = C.POINTER(C.c_int)
+
+
+def build(force: bool = False) -> Path:
+    srcs = [HERE / f for f in ("ora_kernels.c", "ora_solvers.c", "ora_real.inc", "lfg_oracle.h")]
+    if force or not LIB_PATH.exists() or any(
+            s.stat().st_mtime > LIB_PATH.stat().st_mtime for s in srcs):
+        subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib() -> C.CDLL:
+    global _lib
+    if _lib is None:
+        build()
+        _lib = C.CDLL(str(LIB_PATH))
+        _lib.ora_dot_d.restype = C.c_double
+        _lib.ora_norm_d.restype = C.c_double
+        _lib.ora_dot_f.restype = C.c_double
+        _lib.ora_norm_f.restype = C.c_double
+        _lib.ora_mg_work_size_d.restype = C.c_long
+        _lib.ora_mg_work_size_f.restype = C.c_long
+        _setup_signatures(_lib)
+    return _lib
+
+
+def ptr(a: np.ndarray):
+    """ctypes pointer to a contiguous numpy array (int32, float32 or float64)."""
+    if not a.flags["C_CONTIGUOUS"]:
+        raise ValueError("array must be contiguous")
+    if a.dtype == np.float64:
+        return a.ctypes.data_as(_dp)
+    if a.dtype == np.float32:
+        return a.ctypes.data_as(_fp)
+    if a.dtype == np.int32:
+        return a.ctypes.data_as(_ip)
+    raise TypeError(a.dtype)
+
+
+class HelmOp(C.Structure):
+    _fields_ = [("ncol", C.c_int), ("nl", C.c_int), ("cm", C.c_void_p), ("hf", C.c_void_p),
+                ("links", C.c_void_p)]
+
+
+MAX_LEVELS = 8
+
+
+class MGStruct(C.Structure):
+    _fields_ = [("nlevels", C.c_int), ("n_pre", C.c_int), ("n_post", C.c_int),
+                ("n_coarse", C.c_int), ("omega", C.c_double),
+                ("op", HelmOp * MAX_LEVELS), ("child", C.c_void_p * MAX_LEVELS),
+                ("work", C.c_void_p)]
+
+
+class SolveInfo(C.Structure):
+    _fields_ = [("iterations", C.c_int), ("final_err", C.c_double)]
+
+
+class MixedInfo(C.Structure):
+    _fields_ = [("outer_iterations", C.c_int), ("inner_iterations", C.c_int),
+                ("final_rel_residual", C.c_double)]
+
+
+class Helmholtz:
+    """Oracle view of a HelmholtzProblem: operators of every MG level."""
+
+    def __init__(self, prob, dtype=np.float64):
+        L = lib()
+        self.prob = prob
+        self.nl = prob.nlayers
+        self.keep = []
+        # Galerkin coarse operators are built in double, then cast.
+        cms = [np.ascontiguousarray(prob.cm, dtype=np.float64)]
+        hfs = [np.ascontiguousarray(prob.hf, dtype=np.float64)]
+        links = [np.ascontiguousarray(prob.links, dtype=np.int32)]
+        for l, child in enumerate(prob.mg_child):
+            child = np.ascontiguousarray(child, dtype=np.int32)
+            lc = np.ascontiguousarray(prob.mg_links[l], dtype=np.int32)
+            nc = lc.shape[0]
+            fine = HelmOp(links[-1].shape[0], self.nl, cms[-1].ctypes.data, hfs[-1].ctypes.data,
+                          links[-1].ctypes.data)
+            cm_c = np.zeros(3 * self.nl * nc)
+            hf_c = np.zeros(4 * self.nl * nc)
+            L.ora_galerkin_coarsen(C.byref(fine), nc, ptr(child), ptr(lc), ptr(cm_c), ptr(hf_c))
+            cms.append(cm_c)
+            hfs.append(hf_c)
+            links.append(lc)
+        self.cm64, self.hf64, self.links = cms, hfs, links
+        self.child = [np.ascontiguousarray(c, dtype=np.int32) for c in prob.mg_child]
+        self.cm32 = [c.astype(np.float32) for c in cms]
+        self.hf32 = [h.astype(np.float32) for h in hfs]
+
+    def op(self, level: int = 0, dtype=np.float64) -> HelmOp:
+        cm = self.cm64 if dtype == np.float64 else self.cm32
+        hf = self.hf64 if dtype == np.float64 else self.hf32
+        return HelmOp(self.links[level].shape[0], self.nl, cm[level].ctypes.data,
+                      hf[level].ctypes.data, self.links[level].ctypes.data)
+
+    def mg(self, dtype=np.float64, n_pre=2, n_post=2, n_coarse=8, omega=0.8, nlevels=None):
+        nlev = len(self.links) if nlevels is None else nlevels
+        s = MGStruct()
+        s.nlevels, s.n_pre, s.n_post, s.n_coarse, s.omega = nlev, n_pre, n_post, n_coarse, omega
+        for l in range(nlev):
+            s.op[l] = self.op(l, dtype)
+        for l in range(nlev - 1):
+            s.child[l] = self.child[l].ctypes.data
+        L = lib()
+        sfx = "d" if dtype == np.float64 else "f"
+        nwork = getattr(L, f"ora_mg_work_size_{sfx}")(C.byref(s))
+        work = np.zeros(nwork, dtype=dtype)
+        self.keep.append(work)
+        s.work = work.ctypes.data
+        return s
+
+    def apply(self, x: np.ndarray, level: int = 0) -> np.ndarray:
+        dtype = x.dtype
+        y = np.zeros_like(x)
+        op = self.op(level, dtype)
+        fn = lib().ora_helm_apply_d if dtype == np.float64 else lib().ora_helm_apply_f
+        fn(C.byref(op), ptr(x), ptr(y))
+        return y
+
+    def smooth(self, x_in, b, omega=0.8, level: int = 0):
+        dtype = b.dtype
+        op = self.op(level, dtype)
+        out = np.zeros_like(b)
+        work = np.zeros(b.size + 2 * self.nl, dtype=dtype)
+        fn = lib().ora_helm_smooth_d if dtype == np.float64 else lib().ora_helm_smooth_f
+        fn(C.byref(op), C.c_double(omega), None if x_in is None else ptr(x_in), ptr(b),
+           ptr(out), ptr(work))
+        return out
+
+    def mg_apply(self, b: np.ndarray, **kw) -> np.ndarray:
+        s = self.mg(b.dtype, **kw)
+        x = np.zeros_like(b)
+        fn = lib().ora_mg_apply_d if b.dtype == np.float64 else lib().ora_mg_apply_f
+        fn(C.byref(s), ptr(b), ptr(x))
+        return x
+
+    def gcr_mg_solve(self, b, gcrk=10, r_tol=1e-8, max_iter=20, dtype=np.float64, **mgkw):
+        L = lib()
+        sfx = "d" if dtype == np.float64 else "f"
+        b = np.ascontiguousarray(b, dtype=dtype)
+        n = b.size
+        op = self.op(0, dtype)
+        mg = self.mg(dtype, **mgkw)
+        x = np.zeros_like(b)
+        work = np.zeros((2 * gcrk + 3) * n, dtype=dtype)
+        info = SolveInfo()
+        apply_cb = C.cast(getattr(L, f"ora_helm_apply_cb_{sfx}"), C.c_void_p)
+        mg_cb = C.cast(getattr(L, f"ora_mg_apply_cb_{sfx}"), C.c_void_p)
+        st = getattr(L, f"ora_gcr_solve_{sfx}")(
+            C.c_long(n), apply_cb, C.byref(op), mg_cb, C.byref(mg), gcrk, C.c_double(r_tol),
+            C.c_double(0.0), max_iter, 1, ptr(x), ptr(b), ptr(work), C.byref(info))
+        return x, st, info
+
+    def mixed_solve(self, b, tol=1e-8, max_outer=10, gcrk=10, inner_tol=1e-4,
+                    inner_max_iter=2, **mgkw):
+        L = lib()
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        op = self.op(0, np.float64)
+        mg = self.mg(np.float32, **mgkw)
+        x = np.zeros_like(b)
+        info = MixedInfo()
+        st = L.ora_mixed_gcr_mg_solve(C.byref(op), C.byref(mg), ptr(b), ptr(x),
+                                      C.c_double(tol), max_outer, gcrk, C.c_double(inner_tol),
+                                      inner_max_iter, C.byref(info))
+        return x, st, info
+
+
+def _setup_signatures(L):
+    L.ora_gcr_solve_d.argtypes = [C.c_long, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _dp, _dp,
+                                  _dp, C.c_void_p]
+    L.ora_gcr_solve_f.argtypes = [C.c_long, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                  C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _fp, _fp,
+                                  _fp, C.c_void_p]
+    L.ora_cg_solve_d.argtypes = [C.c_long, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                 C.c_double, C.c_double, C.c_int, C.c_int, _dp, _dp, _dp,
+                                 C.c_void_p]
+

@@ -1,0 +1,265 @@
+"""Generate the golden fixtures in this folder from the reference's own tests.
+
+Run in a container that holds the reference source tree (the fixtures it
+writes are committed, so the tests never need the reference at run time):
+
+    python tests/golden/make_golden.py /path/to/lfric_core
+
+The reference is Fortran and cannot be compiled here, so nothing is
+executed: the literal inputs and expected answers are read out of the pFUnit
+test files (``*.pf``) as text, and where a test builds an input or an answer
+with a short loop, that loop is restated below next to its citation.  The
+mesh fixtures are read from the reference's UGRID netCDF test meshes.
+"""
+from __future__ import annotations
+
+import ast
+import json
+import operator
+import re
+import sys
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+UT = "components/science/unit-test/kernel"
+
+_KIND = re.compile(r"_(r_def|r_double|r_single|r_solver|i_def)\b")
+
+
+def _eval_num(expr: str) -> float:
+    """Evaluate one Fortran numeric literal expression (+ - * / only)."""
+    expr = _KIND.sub("", expr.strip())
+    expr = re.sub(r"real\((.*?),\s*\w+\)", r"(\1)", expr)
+    ops = {ast.Add: operator.add, ast.Sub: operator.sub, ast.Mult: operator.mul,
+           ast.Div: operator.truediv, ast.USub: operator.neg, ast.UAdd: operator.pos}
+
+    def ev(node):
+        if isinstance(node, ast.Expression):
+            return ev(node.body)
+        if isinstance(node, ast.Constant):
+            return node.value
+        if isinstance(node, ast.BinOp):
+            return ops[type(node.op)](ev(node.left), ev(node.right))
+        if isinstance(node, ast.UnaryOp):
+            return ops[type(node.op)](ev(node.operand))
+        raise ValueError(f"unsupported literal {expr!r}")
+
+    return ev(ast.parse(expr, mode="eval"))
+
+
+def _source(path: Path) -> str:
+    """The test file with comments removed and continuation lines joined."""
+    lines = []
+    for line in path.read_text().splitlines():
+        if line.lstrip().startswith("!"):
+            continue
+        lines.append(line.split("!")[0] if "!" in line and "'" not in line else line)
+    return re.sub(r"&\s*\n\s*&?", " ", "\n".join(lines))
+
+
+def array_literal(text: str, lhs_regex: str, occurrence: int = 0) -> list[float]:
+    """Values of the array constructor assigned to a left-hand side."""
+    pat = re.compile(lhs_regex + r"\s*=\s*(?:reshape\(\s*|real\(\s*)?\(/(.*?)/\)", re.S)
+    found = pat.findall(text)
+    if len(found) <= occurrence:
+        raise KeyError(f"no array literal for {lhs_regex!r}")
+    return [_eval_num(v) for v in found[occurrence].split(",")]
+
+
+def scalar_literal(text: str, lhs_regex: str) -> float:
+    m = re.search(lhs_regex + r"\s*=\s*([^\n]+)", text)
+    if not m:
+        raise KeyError(lhs_regex)
+    return _eval_num(m.group(1))
+
+
+def tol_literal(text: str, occurrence: int = 0) -> float:
+    found = re.findall(r"tol\s*=\s*([0-9.eE+\-]+_r_\w+)", text)
+    return _eval_num(found[occurrence])
+
+
+def write(name: str, obj: dict) -> None:
+    (HERE / name).write_text(json.dumps(obj, indent=1) + "\n")
+    print("wrote", name)
+
+
+def main(ref: Path) -> None:
+    # ---------------------------------------------------------- tri-solve KAT
+    p = ref / UT / "solver/sci_tri_solve_kernel_mod_test.pf"
+    t = _source(p)
+    x = array_literal(t, r"\bx")
+    ans = array_literal(t, r"answer")
+    write("tri_solve_kat.json", {
+        "source": f"{UT}/solver/sci_tri_solve_kernel_mod_test.pf",
+        "nlayers": len(x), "x": x, "answer": ans,
+        "tri_0": scalar_literal(t, r"\bA0"), "tri_plus": scalar_literal(t, r"\bAP"),
+        "tri_minus": scalar_literal(t, r"\bAM"),
+        "reference_tol": tol_literal(t), "pinned_rel_tol": 1e-12,
+    })
+
+    p = ref / UT / "solver/sci_operator_tri_solve_kernel_mod_test.pf"
+    t = _source(p)
+    nz = 10
+    a0, ap, am = (scalar_literal(t, r"\ba0"), scalar_literal(t, r"\bap"),
+                  scalar_literal(t, r"\bam"))
+    # The test fills tri(2,2,nz-1) with tri(1,1,k)=tri(2,2,k)=a0/2,
+    # tri(1,2,k)=ap, tri(2,1,k)=am (operator_tri_solve_kernel_mod_test.pf:52-57)
+    # and passes it where the kernel expects matrix(ncell=nz-1, 2, 2).
+    tri = np.zeros((2, 2, nz - 1), order="F")
+    tri[0, 0, :] = 0.5 * a0
+    tri[1, 1, :] = 0.5 * a0
+    tri[0, 1, :] = ap
+    tri[1, 0, :] = am
+    write("operator_tri_solve_kat.json", {
+        "source": f"{UT}/solver/sci_operator_tri_solve_kernel_mod_test.pf",
+        "nlayers": nz - 1, "x": array_literal(t, r"\bx"),
+        "answer": array_literal(t, r"answer"),
+        "a0": a0, "ap": ap, "am": am,
+        "tri_as_passed_fortran_order": tri.ravel(order="F").tolist(),
+        "reference_tol": tol_literal(t),
+    })
+
+    # ------------------------------------------------------- LMA kernels
+    def dmat(t: str) -> np.ndarray:
+        d = np.zeros((1, 4, 2))
+        for r in range(4):
+            d[0, r, :] = array_literal(t, rf"d\(1,{r + 1},:\)")
+        return d
+
+    for name, fname in [("matrix_vector", "matrix_vector_mod_test.pf"),
+                        ("dg_matrix_vector", "dg_matrix_vector_mod_test.pf")]:
+        t = _source(ref / UT / "algebra" / fname)
+        d = dmat(t)
+        x = array_literal(t, r"x\(:\)")
+        write(f"{name}_kat.json", {
+            "source": f"{UT}/algebra/{fname}",
+            "matrix_fortran_order": d.ravel(order="F").tolist(),
+            "shape": [1, 4, 2], "x": x, "map1": [1, 2, 3, 4], "map2": [1, 2],
+            "answer": (d[0] @ np.array(x)).tolist(),
+            "tol_r_double": tol_literal(t, 0), "tol_r_single": tol_literal(t, 1),
+        })
+
+    t = _source(ref / UT / "algebra/transpose_matrix_vector_mod_test.pf")
+    d = dmat(t)
+    x = array_literal(t, r"x\(:\)")
+    write("transpose_matrix_vector_kat.json", {
+        "source": f"{UT}/algebra/transpose_matrix_vector_mod_test.pf",
+        "matrix_fortran_order": d.ravel(order="F").tolist(), "shape": [1, 4, 2],
+        "x": x, "map1": [1, 2], "map2": [1, 2, 3, 4],
+        "answer": (d[0].T @ np.array(x)).tolist(),
+        "tol_r_double": tol_literal(t, 0), "tol_r_single": tol_literal(t, 1),
+    })
+
+    t = _source(ref / UT / "algebra/mm_diagonal_kernel_mod_test.pf")
+    mm = np.zeros((2, 3, 3))
+    for cell in range(2):
+        for j in range(3):
+            mm[cell, :, j] = array_literal(t, rf"mm\(cell,:,{j + 1}\)")
+    write("mm_diagonal_kat.json", {
+        "source": f"{UT}/algebra/mm_diagonal_kernel_mod_test.pf",
+        "matrix_fortran_order": mm.ravel(order="F").tolist(), "shape": [2, 3, 3],
+        "nlayers": 1, "map": [array_literal(t, r"map\(:,1\)"),
+                              array_literal(t, r"map\(:,2\)")],
+        "undf": 5, "answer": array_literal(t, r"answer"),
+    })
+
+    # ------------------------------------------------------- CMA (m3x3 data)
+    t = _source(ref / UT / "columnwise_operators/columnwise_op_appinv_kernel_mod_test.pf")
+    asserted = dict(re.findall(r"@assertEqual\((ndf|alpha|g_m|bw),\s*(\d+)\)", t))
+    write("cma_m3x3_kat.json", {
+        "source": [f"{UT}/columnwise_operators/columnwise_op_app_kernel_mod_test.pf",
+                   f"{UT}/columnwise_operators/columnwise_op_appinv_kernel_mod_test.pf",
+                   "components/science/unit-test/support/get_unit_test_m3x3_cma_data_mod.f90"],
+        "space": "Wtheta->Wtheta", "nlayers": 3,
+        "asserted": {k: int(v) for k, v in asserted.items()},
+        "band_first_row": [0.0, 1.0 / 3.0, 1.0 / 6.0],
+        "band_interior": [1.0 / 6.0, 2.0 / 3.0, 1.0 / 6.0],
+        "band_last_row": [1.0 / 6.0, 1.0 / 3.0, 0.0],
+        "tol": tol_literal(t),
+    })
+
+    # ------------------------------------------------------- intergrid KATs
+    im = ref / UT / "inter_mesh"
+    kats = {}
+    t = _source(im / "restrict_scalar_unweighted_kernel_mod_test.pf")
+    kats["restrict_scalar_unweighted"] = {"nlayers": 3, "fine": 1.0, "coarse": [1.0] * 3}
+    t = _source(im / "prolong_scalar_unweighted_kernel_mod_test.pf")
+    kats["prolong_scalar_unweighted"] = {"nlayers": 3, "coarse": 2.5, "fine": [2.5] * 3}
+    t = _source(im / "restrict_mass_w3_kernel_mod_test.pf")
+    kats["restrict_mass_w3"] = {"nlayers": 3, "fine": 1.0, "coarse": [4.0] * 3}
+    t = _source(im / "restrict_scalar_weighted_kernel_mod_test.pf")
+    kats["restrict_scalar_weighted"] = {
+        "nlayers": 1, "fine": array_literal(t, r"fine_field\(:\)"),
+        "weights": array_literal(t, r"weights\(:\)"), "coarse": [0.5]}
+    t = _source(im / "prolong_scalar_weighted_kernel_mod_test.pf")
+    kats["prolong_scalar_weighted"] = {
+        "nlayers": 1, "coarse": 0.5, "weights": array_literal(t, r"weights\(:\)"),
+        "fine": [_eval_num(v) for v in re.findall(
+            r"@assertEqual\(\s*fine_field\(\d\),\s*([0-9.]+_r_def)", t)]}
+    # cell_map(x, y) = x + (y-1)*ny and map_f(1,c) = 1 + (c-1)*nlayers for the
+    # scalar tests (restrict_scalar_unweighted_kernel_mod_test.pf:61-68).
+    kats["scalar_layout"] = {"cell_map_rule": "x + (y-1)*2", "map_fine_rule": "1 + (c-1)*nlayers"}
+
+    t = _source(im / "restrict_w0_kernel_mod_test.pf")
+    map_fine = np.array(array_literal(t, r"map_fine"), dtype=int).reshape(6, 8)  # [cell][df]
+    map_coarse = [int(v) for v in array_literal(t, r"map_coarse")]
+    nl, nx, ny = 3, 3, 2
+    cell_map = np.zeros((nx, ny), dtype=int)             # cell_map(x, y)
+    for y in range(1, ny + 1):
+        for x in range(1, nx + 1):
+            cell_map[x - 1, y - 1] = x + (2 - y) * nx      # restrict_w0_kernel_mod_test.pf
+    SWB, SEB, NEB, NWB = 1, 2, 3, 4
+    fine = 0.5 * np.arange(1, 49, dtype=float)            # fine_field(df) = 0.5*df
+    for k in range(nl + 1):
+        fine[map_fine[0, SWB - 1] + k - 1] = 1.0 + k
+        fine[map_fine[2, SEB - 1] + k - 1] = 0.0 + k
+        fine[map_fine[5, NEB - 1] + k - 1] = 6.0 + k
+        fine[map_fine[3, NWB - 1] + k - 1] = 2.0 + k
+    kats["restrict_w0"] = {
+        "source": f"{UT}/inter_mesh/restrict_w0_kernel_mod_test.pf",
+        "nlayers": nl, "nx": nx, "ny": ny, "cell_map_xy": cell_map.tolist(),
+        "map_fine": map_fine.tolist(), "map_coarse": map_coarse,
+        "fine": fine.tolist(), "coarse": array_literal(t, r"answer\(:\)"),
+        "tol": tol_literal(t)}
+
+    t = _source(im / "prolong_w0_kernel_mod_test.pf")
+    coarse = array_literal(t, r"coarse_field\(:\)")
+    ans = np.zeros(48)
+    # The answer loop of prolong_w0_kernel_mod_test.pf: value + k on the
+    # listed fine dofs, zero elsewhere.
+    rows = re.findall(r"answer\(map_fine\((\w+),(\d)\)\+k\)\s*=\s*(-?[0-9.]+_r_def)", t)
+    named = {"SWB": 1, "SEB": 2, "NEB": 3, "NWB": 4}
+    for corner, cell, val in rows:
+        for k in range(nl + 1):
+            ans[map_fine[int(cell) - 1, named[corner] - 1] + k - 1] = _eval_num(val) + k
+    kats["prolong_w0"] = {
+        "source": f"{UT}/inter_mesh/prolong_w0_kernel_mod_test.pf",
+        "nlayers": nl, "nx": nx, "ny": ny, "cell_map_xy": cell_map.tolist(),
+        "map_fine": map_fine.tolist(), "map_coarse": map_coarse,
+        "coarse": coarse, "fine": ans.tolist(), "tol": tol_literal(t)}
+    write("intergrid_kat.json", kats)
+
+    # ------------------------------------------------------- meshes
+    from scipy.io import netcdf_file
+    f = netcdf_file(str(ref / "infrastructure/unit-test/data/mesh_C32_MG.nc"), "r", mmap=False)
+    mesh = {"source": "infrastructure/unit-test/data/mesh_C32_MG.nc", "meshes": {}, "maps": {}}
+    for m in ("C4", "C8"):
+        fn = f.variables[m + "_face_nodes"][:] - 1
+        nxv = f.variables[m + "_node_x"][:]
+        nyv = f.variables[m + "_node_y"][:]
+        mesh["meshes"][m] = {
+            "face_links_WSEN": (f.variables[m + "_face_links"][:] - 1).tolist(),
+            "corner_lon_SW_SE_NE_NW": np.round(nxv[fn], 12).tolist(),
+            "corner_lat_SW_SE_NE_NW": np.round(nyv[fn], 12).tolist(),
+            "face_lon": np.round(f.variables[m + "_face_x"][:], 12).tolist(),
+            "face_lat": np.round(f.variables[m + "_face_y"][:], 12).tolist(),
+        }
+    for a, b in (("C4", "C8"), ("C8", "C16")):
+        mesh["maps"][f"{a}_{b}"] = (f.variables[f"{a}_{b}_map"][:] - 1).tolist()
+    write("mesh_mg_kat.json", mesh)
+
+
+if __name__ == "__main__":
+    main(Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference"))
