@@ -178,7 +178,9 @@ def main():
 
     prob = helmholtz_problem(args.n, NLAYERS, seed=SEED + rank, mg_levels=MG_LEVELS)
     ctx = api.Context(dev)
-    stream = torch.cuda.current_stream()
+    # one explicit stream for the library's kernels and the timing events
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     ctx.set_stream(stream.cuda_stream)
     system = api.HelmholtzSystem(ctx, prob)
     system.b64.import_(prob.rhs)

@@ -55,162 +55,163 @@ __device__ __forceinline__ T helm_row(const HelmArgs<T>& A, size_t i, int k, T x
 }
 
 // y = A x (RESID: y = b - A x).  DOT: accumulate <y, w> (w null: <y, y>)
-// into a deterministic reduction.
+// into a deterministic reduction.  Grid-stride over all (level, column)
+// elements: no recurrence, so every element is independent and the loads of
+// many elements are in flight at once.
 template <class T, bool RESID, bool DOT>
 __global__ void __launch_bounds__(256) k_helm_apply(HelmArgs<T> A, const T* __restrict__ x,
                                                     const T* __restrict__ b, T* __restrict__ y,
                                                     const T* __restrict__ w, Red r) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const unsigned N = A.ncol;
+  const unsigned total = N * (unsigned)A.nl;
   double acc = 0.0;
-  if (c < A.ncol) {
-    const size_t N = A.ncol;
-    int nb[4];
+  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
+    const unsigned k = i / N, c = i - k * N;
+    T xn[4];
 #pragma unroll
-    for (int f = 0; f < 4; ++f) nb[f] = A.links[f * N + c];
-    T xm = (T)0, x0 = x[c], xp;
-#pragma unroll 4
-    for (int k = 0; k < A.nl; ++k) {
-      const size_t i = (size_t)k * N + c;
-      xp = (k + 1 < A.nl) ? x[i + N] : (T)0;
-      T xn[4];
-#pragma unroll
-      for (int f = 0; f < 4; ++f) xn[f] = x[(size_t)k * N + nb[f]];
-      T v = helm_row(A, i, k, xm, x0, xp, xn);
-      if (RESID) v = b[i] - v;
-      y[i] = v;
-      if (DOT) {
-        const T ww = w ? w[i] : v;
-        acc += (double)v * (double)ww;
-      }
-      xm = x0;
-      x0 = xp;
+    for (int f = 0; f < 4; ++f) xn[f] = x[(size_t)k * N + A.links[f * N + c]];
+    const T xm = k > 0 ? x[i - N] : (T)0;
+    const T xp = k + 1 < (unsigned)A.nl ? x[i + N] : (T)0;
+    T v = helm_row(A, i, (int)k, xm, x[i], xp, xn);
+    if (RESID) v = b[i] - v;
+    y[i] = v;
+    if (DOT) {
+      const T ww = w ? w[i] : v;
+      acc += (double)v * (double)ww;
     }
   }
   if (DOT) red_finish(r, acc);
 }
 
 // One block-Jacobi column sweep of A x = b:
-//   x_out = omega T'^{-1} (b + H_off x_in + kappa T' x_in),  kappa = 1/omega - 1,
+//   x_out = omega T'^{-1} (b + H_off x_in) + (1 - omega) x_in,
 // which equals x_in + omega T'^{-1} (b - A x_in).  XIN false: x_in = 0.
-// PRO: x_in is the prolongation-corrected iterate x_in + P xc (P = add the
-// parent's coarse value), formed on the fly.  c' of the Thomas forward sweep
-// is kept in shared memory and d' in registers (DP_SMEM: also in shared
-// memory); both are indexed by the unrolled level loop.
-template <class T, int MAXNL, bool XIN, bool PRO, bool DP_SMEM>
-__global__ void k_helm_smooth(HelmArgs<T> A, T omega, T kappa, const T* __restrict__ xin,
-                              const T* __restrict__ b, T* __restrict__ xout,
-                              const int* __restrict__ parent, const T* __restrict__ xc,
-                              int ncoarse) {
+// PRO: x_in is the prolongation-corrected iterate x_in + P xc (P adds the
+// parent's coarse value), formed on the fly and never stored.
+//
+// A block owns a tile of tc consecutive columns.  Phase 1: all threads load
+// the tile's x, b and bands for every level into shared memory (coalesced
+// rows of tc columns, many loads in flight) and form the right-hand side
+// with the neighbour couplings.  Phase 2: one thread per column runs the
+// Thomas recurrence of columnwise_op_appinv out of shared memory (c' over
+// the super-diagonal, d' and then the solution over the right-hand side).
+// Phase 3: coalesced write of the relaxed update.  Shared memory holds
+// 5 * nl * tc values.
+template <class T, bool XIN, bool PRO>
+__global__ void __launch_bounds__(256) k_helm_smooth(HelmArgs<T> A, T omega,
+                                                     const T* __restrict__ xin,
+                                                     const T* __restrict__ b,
+                                                     T* __restrict__ xout,
+                                                     const int* __restrict__ parent,
+                                                     const T* __restrict__ xc, int ncoarse,
+                                                     int tc) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  T* cps = reinterpret_cast<T*>(smem_raw);
-  T* dps = cps + MAXNL * blockDim.x;
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= A.ncol) return;
   const int nl = A.nl;
-  const size_t N = A.ncol;
+  const unsigned N = A.ncol;
   const size_t plane = (size_t)nl * N;
-  const int t = threadIdx.x, bs = blockDim.x;
-  int nb[4], pn[4] = {0, 0, 0, 0}, pc = 0;
-  if (XIN) {
-#pragma unroll
-    for (int f = 0; f < 4; ++f) nb[f] = A.links[f * N + c];
-    if (PRO) {
-      pc = parent[c];
-#pragma unroll
-      for (int f = 0; f < 4; ++f) pn[f] = parent[nb[f]];
-    }
-  }
-  auto X = [&](int col, int pcol, int k) -> T {
+  const int tile = nl * tc;
+  T* sx = reinterpret_cast<T*>(smem_raw);
+  T* sr = sx + tile;
+  T* ssub = sr + tile;
+  T* sdg = ssub + tile;
+  T* ssp = sdg + tile;
+  const unsigned c0 = blockIdx.x * tc;
+  auto X = [&](unsigned col, unsigned k) -> T {
     T v = xin[(size_t)k * N + col];
-    if (PRO) v = v + xc[(size_t)k * ncoarse + pcol];
+    if (PRO) v = v + xc[(size_t)k * ncoarse + parent[col]];
     return v;
   };
-  T dp[DP_SMEM ? 1 : MAXNL];
-  T cprev = (T)0, dprev = (T)0;
-  T xm = (T)0, x0 = (T)0, xp = (T)0;
-  if (XIN) x0 = X(c, pc, 0);
+  // phase 1
+#pragma unroll 4
+  for (int e = threadIdx.x; e < tile; e += blockDim.x) {
+    const int k = e / tc, j = e - k * tc;
+    const unsigned c = c0 + j;
+    if (c >= N) continue;
+    const size_t i = (size_t)k * N + c;
+    ssub[e] = A.sub[i];
+    sdg[e] = A.diag[i];
+    ssp[e] = A.sup[i];
+    T rhs = b[i];
+    if (XIN) {
+      sx[e] = X(c, k);
+      T hs = (T)0;
 #pragma unroll
-  for (int k = 0; k < MAXNL; ++k) {
-    if (k < nl) {
-      const size_t i = (size_t)k * N + c;
-      const T sb = A.sub[i], dg = A.diag[i], sp = A.sup[i];
-      T rhs = b[i];
-      if (XIN) {
-        xp = (k + 1 < nl) ? X(c, pc, k + 1) : (T)0;
-        T hs = (T)0;
-#pragma unroll
-        for (int f = 0; f < 4; ++f) hs = hs + A.h[f * plane + i] * X(nb[f], pn[f], k);
-        T tx = (T)0;
-        if (k > 0) tx = tx + sb * xm;
-        tx = tx + dg * x0;
-        if (k < nl - 1) tx = tx + sp * xp;
-        rhs = rhs + hs + kappa * tx;
-      }
+      for (int f = 0; f < 4; ++f) hs = hs + A.h[f * plane + i] * X(A.links[f * N + c], k);
+      rhs = rhs + hs;
+    }
+    sr[e] = rhs;
+  }
+  __syncthreads();
+  // phase 2: Thomas, column j of the tile
+  for (int j = threadIdx.x; j < tc; j += blockDim.x) {
+    if (c0 + j >= N) break;
+    T cprev = (T)0, dprev = (T)0;
+    for (int k = 0; k < nl; ++k) {
+      const int e = k * tc + j;
+      const T a1 = ssub[e], a2 = sdg[e], a3 = ssp[e];
       T inv, cpk, dpk;
       if (k == 0) {
-        inv = (T)1 / dg;
-        cpk = inv * sp;
-        dpk = inv * rhs;
+        inv = (T)1 / a2;
+        cpk = inv * a3;
+        dpk = inv * sr[e];
       } else {
-        inv = (T)1 / (dg - sb * cprev);
-        cpk = (k < nl - 1) ? inv * sp : (T)0;
-        dpk = inv * (rhs - sb * dprev);
+        inv = (T)1 / (a2 - a1 * cprev);
+        cpk = (k < nl - 1) ? inv * a3 : (T)0;
+        dpk = inv * (sr[e] - a1 * dprev);
       }
-      cps[k * bs + t] = cpk;
-      if (DP_SMEM) dps[k * bs + t] = dpk; else dp[DP_SMEM ? 0 : k] = dpk;
+      ssp[e] = cpk;
+      sr[e] = dpk;
       cprev = cpk;
       dprev = dpk;
-      xm = x0;
-      x0 = xp;
+    }
+    T znext = (T)0;
+    for (int k = nl - 1; k >= 0; --k) {
+      const int e = k * tc + j;
+      T z = sr[e];
+      if (k < nl - 1) z = z - ssp[e] * znext;
+      sr[e] = z;
+      znext = z;
     }
   }
-  T znext = (T)0;
-#pragma unroll
-  for (int k = MAXNL - 1; k >= 0; --k) {
-    if (k < nl) {
-      T z = DP_SMEM ? dps[k * bs + t] : dp[DP_SMEM ? 0 : k];
-      if (k < nl - 1) z = z - cps[k * bs + t] * znext;
-      znext = z;
-      xout[(size_t)k * N + c] = omega * z;
-    }
+  __syncthreads();
+  // phase 3
+  const T om1 = (T)1 - omega;
+  for (int e = threadIdx.x; e < tile; e += blockDim.x) {
+    const int k = e / tc, j = e - k * tc;
+    const unsigned c = c0 + j;
+    if (c >= N) continue;
+    T v = omega * sr[e];
+    if (XIN) v = v + om1 * sx[e];
+    xout[(size_t)k * N + c] = v;
   }
 }
 
 // bc(C,k) = sum over the children q (y outer, x inner) of (b - A x)(child,k):
 // residual fused with restrict_mass_w3 (sci_restrict_mass_w3_kernel_mod.F90:126-179).
+// One thread per coarse element (level, coarse column).
 template <class T>
-__global__ void __launch_bounds__(128) k_helm_resid_restrict(HelmArgs<T> A,
+__global__ void __launch_bounds__(256) k_helm_resid_restrict(HelmArgs<T> A,
                                                              const T* __restrict__ x,
                                                              const T* __restrict__ b,
                                                              T* __restrict__ bc,
                                                              const int* __restrict__ child,
                                                              int ncoarse, int nq) {
-  const int C = blockIdx.x * blockDim.x + threadIdx.x;
-  if (C >= ncoarse) return;
-  const size_t N = A.ncol;
-  int ch[4], nb[4][4];
-#pragma unroll
-  for (int q = 0; q < 4; ++q) {
-    ch[q] = q < nq ? child[q * ncoarse + C] : 0;
-#pragma unroll
-    for (int f = 0; f < 4; ++f) nb[q][f] = A.links[f * N + ch[q]];
-  }
-#pragma unroll 2
-  for (int k = 0; k < A.nl; ++k) {
+  const unsigned NC = ncoarse, N = A.ncol;
+  const unsigned total = NC * (unsigned)A.nl;
+  for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
+    const unsigned k = e / NC, C = e - k * NC;
     T acc = (T)0;
+    for (int q = 0; q < nq; ++q) {
+      const unsigned c = child[q * NC + C];
+      const size_t i = (size_t)k * N + c;
+      const T xm = k > 0 ? x[i - N] : (T)0;
+      const T xp = k + 1 < (unsigned)A.nl ? x[i + N] : (T)0;
+      T xn[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) {
-      if (q < nq) {
-        const size_t i = (size_t)k * N + ch[q];
-        const T xm = k > 0 ? x[i - N] : (T)0;
-        const T xp = k + 1 < A.nl ? x[i + N] : (T)0;
-        T xn[4];
-#pragma unroll
-        for (int f = 0; f < 4; ++f) xn[f] = x[(size_t)k * N + nb[q][f]];
-        acc = acc + (b[i] - helm_row(A, i, k, xm, x[i], xp, xn));
-      }
+      for (int f = 0; f < 4; ++f) xn[f] = x[(size_t)k * N + A.links[f * N + c]];
+      acc = acc + (b[i] - helm_row(A, i, (int)k, xm, x[i], xp, xn));
     }
-    bc[(size_t)k * ncoarse + C] = acc;
+    bc[e] = acc;
   }
 }
 
@@ -273,66 +274,50 @@ __global__ void k_convert(TO* __restrict__ y, const TI* __restrict__ x, size_t n
 // dynamic shared memory one block may use (B200: up to 227 KB per block)
 constexpr size_t kSmemCap = 200 * 1024;
 
-int smooth_block(int ncol, int nsm) {
-  // spread small meshes over every SM; 128 threads per block for large ones
-  int per = (ncol + nsm - 1) / nsm;
-  int bs = ((per + 31) / 32) * 32;
-  return std::max(32, std::min(128, bs));
-}
-
-template <class T, int MAXNL, bool XIN, bool PRO, bool DPS>
-void launch_smooth_t(lfg_helm op, T omega, T kappa, const T* xin, const T* b, T* xout,
-                     const int* parent, const T* xc, int ncoarse) {
-  lfg_ctx c = op->ctx;
-  constexpr size_t per_thread = (size_t)MAXNL * sizeof(T) * (DPS ? 2 : 1);
-  constexpr int max_bs = (int)std::min<size_t>(128, (kSmemCap / per_thread) / 32 * 32);
-  static_assert(max_bs >= 32, "smoother column too tall for shared memory");
-  const int bs = std::min(max_bs, smooth_block(op->ncol, c->num_sms));
-  const size_t smem = per_thread * bs;
-  auto kern = k_helm_smooth<T, MAXNL, XIN, PRO, DPS>;
-  static bool attr_set = false;
-  if (!attr_set) {
-    LFG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(per_thread * max_bs)));
-    attr_set = true;
-  }
-  const int grid = (op->ncol + bs - 1) / bs;
-  kern<<<grid, bs, smem, c->stream>>>(args_of<T>(op), omega, kappa, xin, b, xout, parent, xc,
-                                      ncoarse);
-  after_launch(c, "helm_smooth");
+// Columns per smoother tile: as wide as shared memory allows (at most 64),
+// narrowed on small meshes so that every SM receives blocks.
+int smooth_tile(int ncol, int nl, size_t elem, int nsm) {
+  int tc = 64;
+  while (tc > 8 && (size_t)5 * nl * tc * elem > kSmemCap) tc /= 2;
+  while (tc > 8 && (ncol + tc - 1) / tc < 2 * nsm) tc /= 2;
+  return tc;
 }
 
 template <class T, bool XIN, bool PRO>
-void launch_smooth_nl(lfg_helm op, T omega, T kappa, const T* xin, const T* b, T* xout,
-                      const int* parent, const T* xc, int ncoarse) {
-  const int nl = op->nl;
-  if (nl <= 16)
-    launch_smooth_t<T, 16, XIN, PRO, false>(op, omega, kappa, xin, b, xout, parent, xc, ncoarse);
-  else if (nl <= 32)
-    launch_smooth_t<T, 32, XIN, PRO, false>(op, omega, kappa, xin, b, xout, parent, xc, ncoarse);
-  else if (nl <= 72)
-    launch_smooth_t<T, 72, XIN, PRO, false>(op, omega, kappa, xin, b, xout, parent, xc, ncoarse);
-  else if (nl <= 128)
-    launch_smooth_t<T, 128, XIN, PRO, true>(op, omega, kappa, xin, b, xout, parent, xc, ncoarse);
-  else
-    throw Error(LFG_ERR_ARG, "helm_smooth: more than 128 levels is not supported");
+void launch_smooth_t(lfg_helm op, T omega, const T* xin, const T* b, T* xout,
+                     const int* parent, const T* xc, int ncoarse) {
+  lfg_ctx c = op->ctx;
+  const int tc = smooth_tile(op->ncol, op->nl, sizeof(T), c->num_sms);
+  const size_t smem = (size_t)5 * op->nl * tc * sizeof(T);
+  if (smem > kSmemCap)
+    throw Error(LFG_ERR_ARG, "helm_smooth: column too tall for the shared-memory tile");
+  auto kern = k_helm_smooth<T, XIN, PRO>;
+  static bool attr_set = false;
+  if (!attr_set) {
+    LFG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)kSmemCap));
+    attr_set = true;
+  }
+  const int grid = (op->ncol + tc - 1) / tc;
+  kern<<<grid, 256, smem, c->stream>>>(args_of<T>(op), omega, xin, b, xout, parent, xc,
+                                       ncoarse, tc);
+  after_launch(c, "helm_smooth");
 }
 
 template <class T>
 void smooth_t(lfg_helm op, double omega, lfg_field x_in, lfg_field b, lfg_field x_out,
               lfg_intergrid ig, lfg_field xc) {
   const T om = (T)omega;
-  const T kap = (T)(1.0 / omega - 1.0);
   const T* xi = x_in ? (const T*)x_in->d : nullptr;
   if (!x_in)
-    launch_smooth_nl<T, false, false>(op, om, kap, nullptr, (const T*)b->d, (T*)x_out->d,
-                                      nullptr, nullptr, 0);
-  else if (!ig)
-    launch_smooth_nl<T, true, false>(op, om, kap, xi, (const T*)b->d, (T*)x_out->d, nullptr,
+    launch_smooth_t<T, false, false>(op, om, nullptr, (const T*)b->d, (T*)x_out->d, nullptr,
                                      nullptr, 0);
+  else if (!ig)
+    launch_smooth_t<T, true, false>(op, om, xi, (const T*)b->d, (T*)x_out->d, nullptr,
+                                    nullptr, 0);
   else
-    launch_smooth_nl<T, true, true>(op, om, kap, xi, (const T*)b->d, (T*)x_out->d, ig->parent,
-                                    (const T*)xc->d, ig->ncoarse);
+    launch_smooth_t<T, true, true>(op, om, xi, (const T*)b->d, (T*)x_out->d, ig->parent,
+                                   (const T*)xc->d, ig->ncoarse);
 }
 
 void check_field(lfg_helm op, lfg_field f, const char* what) {
@@ -349,8 +334,7 @@ void helm_apply(lfg_helm op, lfg_field y, lfg_field x, lfg_field dot_with, int s
   check_field(op, y, "helm_apply");
   check_field(op, x, "helm_apply");
   lfg_ctx c = op->ctx;
-  const int bs = 128, grid = (op->ncol + bs - 1) / bs;
-  LFG_REQUIRE(grid <= kMaxRedBlocks || slot < 0, "helm_apply: mesh too large for a fused dot");
+  const int bs = 256, grid = c->stream_grid((size_t)op->ncol * op->nl, bs);
   Red r = slot >= 0 ? c->red(slot) : Red{nullptr, nullptr, nullptr};
   if (op->kind == LFG_R_DOUBLE) {
     using T = double;
@@ -373,8 +357,7 @@ void helm_residual(lfg_helm op, lfg_field r_out, lfg_field x, lfg_field b, int s
   check_field(op, x, "helm_residual");
   check_field(op, b, "helm_residual");
   lfg_ctx c = op->ctx;
-  const int bs = 128, grid = (op->ncol + bs - 1) / bs;
-  LFG_REQUIRE(grid <= kMaxRedBlocks || slot < 0, "helm_residual: mesh too large for a fused norm");
+  const int bs = 256, grid = c->stream_grid((size_t)op->ncol * op->nl, bs);
   Red r = slot >= 0 ? c->red(slot) : Red{nullptr, nullptr, nullptr};
   if (op->kind == LFG_R_DOUBLE) {
     using T = double;
@@ -417,7 +400,7 @@ void helm_residual_restrict(lfg_helm op, lfg_intergrid ig, lfg_field x, lfg_fiel
                   bc->kind == op->kind && ig->nx * ig->ny <= 4,
               "residual_restrict: bad coarse field");
   lfg_ctx c = op->ctx;
-  const int bs = 128, grid = (ig->ncoarse + bs - 1) / bs;
+  const int bs = 256, grid = c->stream_grid((size_t)ig->ncoarse * op->nl, bs);
   if (op->kind == LFG_R_DOUBLE)
     k_helm_resid_restrict<double><<<grid, bs, 0, c->stream>>>(args_of<double>(op), (const double*)x->d, (const double*)b->d, (double*)bc->d, ig->child, ig->ncoarse, ig->nx * ig->ny);
   else
