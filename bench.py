@@ -252,11 +252,13 @@ def main():
         op32.smooth(0.8, xs, bs, ys)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.nvtx.range_push("smoother_roofline")
     e0.record(stream)
     for i in range(nrep):
         op32.smooth(0.8, xs if i % 2 == 0 else ys, bs, ys if i % 2 == 0 else xs)
     e1.record(stream)
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     smooth_ms = e0.elapsed_time(e1) / nrep
     smooth_bytes = 10 * N * 4          # x, b, 3 bands, 4 couplings read; x_out written
     peak, peak_kind = measured_hbm_peak()

@@ -31,12 +31,15 @@ struct HelmArgs {
   const T* __restrict__ sup;
   const T* __restrict__ h;       // [4][nl][ncol]
   const int* __restrict__ links; // [4][ncol]
+  const T* __restrict__ inv;     // Thomas inverse denominators [nl][ncol]
+  const T* __restrict__ cp;      // Thomas c' [nl][ncol]
 };
 
 template <class T>
 HelmArgs<T> args_of(lfg_helm op) {
   return HelmArgs<T>{op->ncol, op->nl, (const T*)op->sub, (const T*)op->diag,
-                     (const T*)op->sup, (const T*)op->h, op->mesh->links};
+                     (const T*)op->sup, (const T*)op->h, op->mesh->links,
+                     (const T*)op->inv, (const T*)op->cp};
 }
 
 // (A x)(c,k) with the reference's order: T' row first (sub, diag, super,
@@ -54,141 +57,254 @@ __device__ __forceinline__ T helm_row(const HelmArgs<T>& A, size_t i, int k, T x
   return acc;
 }
 
+// Levels per thread in the element-parallel kernels: a thread keeps its
+// column's neighbour ids in registers over KC consecutive levels, whose
+// loads are all independent.
+constexpr int KC = 2;
+
+// (A x)(c,k) from values already in registers: the T' row (sub, diag,
+// super, in the columnwise_op_app order) then minus the four couplings.
+// has_m / has_p select the sub / super terms without a branch.
+template <class T>
+__device__ __forceinline__ T helm_row_v(T sb, T dg, T sp, const T (&hv)[4], T xm, T x0, T xp,
+                                        const T (&xn)[4], bool has_m, bool has_p) {
+  T acc = has_m ? sb * xm : (T)0;
+  acc = acc + dg * x0;
+  if (has_p) acc = acc + sp * xp;
+#pragma unroll
+  for (int f = 0; f < 4; ++f) acc = acc - hv[f] * xn[f];
+  return acc;
+}
+
 // y = A x (RESID: y = b - A x).  DOT: accumulate <y, w> (w null: <y, y>)
-// into a deterministic reduction.  Grid-stride over all (level, column)
-// elements: no recurrence, so every element is independent and the loads of
-// many elements are in flight at once.
-template <class T, bool RESID, bool DOT>
+// into a deterministic reduction.  Thread = (column, chunk of KC levels);
+// all loads of the chunk are issued before any arithmetic (addresses are
+// clamped into the column, so no load sits behind a branch).
+template <class T, bool RESID, bool DOT, bool HASW = false>
 __global__ void __launch_bounds__(256) k_helm_apply(HelmArgs<T> A, const T* __restrict__ x,
                                                     const T* __restrict__ b, T* __restrict__ y,
                                                     const T* __restrict__ w, Red r) {
   const unsigned N = A.ncol;
-  const unsigned total = N * (unsigned)A.nl;
+  const int nl = A.nl;
+  const size_t plane = (size_t)nl * N;
+  const int nchunk = (nl + KC - 1) / KC;
+  const unsigned total = N * (unsigned)nchunk;
   double acc = 0.0;
-  for (unsigned i = blockIdx.x * blockDim.x + threadIdx.x; i < total; i += gridDim.x * blockDim.x) {
-    const unsigned k = i / N, c = i - k * N;
-    T xn[4];
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const unsigned kc = t / N, c = t - kc * N;
+    int nb[4];
 #pragma unroll
-    for (int f = 0; f < 4; ++f) xn[f] = x[(size_t)k * N + A.links[f * N + c]];
-    const T xm = k > 0 ? x[i - N] : (T)0;
-    const T xp = k + 1 < (unsigned)A.nl ? x[i + N] : (T)0;
-    T v = helm_row(A, i, (int)k, xm, x[i], xp, xn);
-    if (RESID) v = b[i] - v;
-    y[i] = v;
-    if (DOT) {
-      const T ww = w ? w[i] : v;
-      acc += (double)v * (double)ww;
+    for (int f = 0; f < 4; ++f) nb[f] = A.links[f * N + c];
+    const int k0 = kc * KC;
+    const int kn = min(KC, nl - k0);
+    // column values x(k0-1 .. k0+KC) with clamped levels
+    T xv[KC + 2];
+#pragma unroll
+    for (int q = 0; q < KC + 2; ++q) {
+      const int k = min(max(k0 - 1 + q, 0), nl - 1);
+      xv[q] = x[(size_t)k * N + c];
     }
+    // all loads and arithmetic of the chunk first, stores after (the
+    // compiler cannot reorder loads across stores through these pointers)
+    T vout[KC];
+#pragma unroll
+    for (int kk = 0; kk < KC; ++kk) {
+      const int k = min(k0 + kk, nl - 1);
+      const size_t i = (size_t)k * N + c;
+      T xn[4], hv[4];
+#pragma unroll
+      for (int f = 0; f < 4; ++f) {
+        xn[f] = x[(size_t)k * N + nb[f]];
+        hv[f] = A.h[f * plane + i];
+      }
+      T v = helm_row_v(A.sub[i], A.diag[i], A.sup[i], hv, xv[kk], xv[kk + 1], xv[kk + 2], xn,
+                       k > 0, k < nl - 1);
+      if (RESID) v = b[i] - v;
+      vout[kk] = v;
+      if (DOT && kk < kn) acc += (double)v * (double)(HASW ? w[i] : v);
+    }
+#pragma unroll
+    for (int kk = 0; kk < KC; ++kk)
+      if (kk < kn) y[(size_t)(k0 + kk) * N + c] = vout[kk];
   }
   if (DOT) red_finish(r, acc);
 }
 
-// One block-Jacobi column sweep of A x = b:
+// Thomas factors of T' per column with columnwise_op_appinv's arithmetic:
+// inv_k = 1/(diag_k - sub_k c'_{k-1}) (inv_0 = 1/diag_0), c'_k = inv_k sup_k
+// (not formed on the last row).
+template <class T>
+__global__ void k_helm_factor(const T* __restrict__ sub, const T* __restrict__ diag,
+                              const T* __restrict__ sup, T* __restrict__ inv, T* __restrict__ cp,
+                              int ncol, int nl) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncol) return;
+  T cprev = (T)0;
+  for (int k = 0; k < nl; ++k) {
+    const size_t i = (size_t)k * ncol + c;
+    const T iv = k == 0 ? (T)1 / diag[i] : (T)1 / (diag[i] - sub[i] * cprev);
+    const T ck = k < nl - 1 ? iv * sup[i] : (T)0;
+    inv[i] = iv;
+    cp[i] = ck;
+    cprev = ck;
+  }
+}
+
+// The block-Jacobi column sweep of A x = b,
 //   x_out = omega T'^{-1} (b + H_off x_in) + (1 - omega) x_in,
-// which equals x_in + omega T'^{-1} (b - A x_in).  XIN false: x_in = 0.
-// PRO: x_in is the prolongation-corrected iterate x_in + P xc (P adds the
-// parent's coarse value), formed on the fly and never stored.
+// which equals x_in + omega T'^{-1} (b - A x_in), runs as two streaming
+// kernels.  PRO: x_in is the prolongation-corrected iterate x_in + P xc (P
+// adds the parent's coarse value), formed on the fly and never stored.
 //
-// A block owns a tile of tc consecutive columns.  Phase 1: all threads load
-// the tile's x, b and bands for every level into shared memory (coalesced
-// rows of tc columns, many loads in flight) and form the right-hand side
-// with the neighbour couplings.  Phase 2: one thread per column runs the
-// Thomas recurrence of columnwise_op_appinv out of shared memory (c' over
-// the super-diagonal, d' and then the solution over the right-hand side).
-// Phase 3: coalesced write of the relaxed update.  Shared memory holds
-// 5 * nl * tc values.
-template <class T, bool XIN, bool PRO>
-__global__ void __launch_bounds__(256) k_helm_smooth(HelmArgs<T> A, T omega,
-                                                     const T* __restrict__ xin,
-                                                     const T* __restrict__ b,
-                                                     T* __restrict__ xout,
-                                                     const int* __restrict__ parent,
-                                                     const T* __restrict__ xc, int ncoarse,
-                                                     int tc) {
-  extern __shared__ __align__(16) unsigned char smem_raw[];
-  const int nl = A.nl;
+// (1) k_helm_rhs: r = b + H_off x_in, one thread per (column, chunk of KC
+//     levels), loads issued before the stores.
+template <class T, bool PRO>
+__global__ void __launch_bounds__(256) k_helm_rhs(HelmArgs<T> A, const T* __restrict__ xin,
+                                                  const T* __restrict__ b, T* __restrict__ r,
+                                                  const int* __restrict__ parent,
+                                                  const T* __restrict__ xc, int ncoarse) {
   const unsigned N = A.ncol;
+  const int nl = A.nl;
   const size_t plane = (size_t)nl * N;
-  const int tile = nl * tc;
-  T* sx = reinterpret_cast<T*>(smem_raw);
-  T* sr = sx + tile;
-  T* ssub = sr + tile;
-  T* sdg = ssub + tile;
-  T* ssp = sdg + tile;
-  const unsigned c0 = blockIdx.x * tc;
-  auto X = [&](unsigned col, unsigned k) -> T {
-    T v = xin[(size_t)k * N + col];
-    if (PRO) v = v + xc[(size_t)k * ncoarse + parent[col]];
-    return v;
-  };
-  // phase 1
-#pragma unroll 4
-  for (int e = threadIdx.x; e < tile; e += blockDim.x) {
-    const int k = e / tc, j = e - k * tc;
-    const unsigned c = c0 + j;
-    if (c >= N) continue;
-    const size_t i = (size_t)k * N + c;
-    ssub[e] = A.sub[i];
-    sdg[e] = A.diag[i];
-    ssp[e] = A.sup[i];
-    T rhs = b[i];
-    if (XIN) {
-      sx[e] = X(c, k);
+  const int nchunk = (nl + KC - 1) / KC;
+  const unsigned total = N * (unsigned)nchunk;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const unsigned kc = t / N, c = t - kc * N;
+    int nb[4], pn[4] = {0, 0, 0, 0};
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+      nb[f] = A.links[f * N + c];
+      if (PRO) pn[f] = parent[nb[f]];
+    }
+    const int k0 = kc * KC;
+    const int kn = min(KC, nl - k0);
+    T out[KC];
+#pragma unroll
+    for (int kk = 0; kk < KC; ++kk) {
+      const int k = min(k0 + kk, nl - 1);
+      const size_t i = (size_t)k * N + c;
       T hs = (T)0;
 #pragma unroll
-      for (int f = 0; f < 4; ++f) hs = hs + A.h[f * plane + i] * X(A.links[f * N + c], k);
-      rhs = rhs + hs;
-    }
-    sr[e] = rhs;
-  }
-  __syncthreads();
-  // phase 2: Thomas, column j of the tile
-  for (int j = threadIdx.x; j < tc; j += blockDim.x) {
-    if (c0 + j >= N) break;
-    T cprev = (T)0, dprev = (T)0;
-    for (int k = 0; k < nl; ++k) {
-      const int e = k * tc + j;
-      const T a1 = ssub[e], a2 = sdg[e], a3 = ssp[e];
-      T inv, cpk, dpk;
-      if (k == 0) {
-        inv = (T)1 / a2;
-        cpk = inv * a3;
-        dpk = inv * sr[e];
-      } else {
-        inv = (T)1 / (a2 - a1 * cprev);
-        cpk = (k < nl - 1) ? inv * a3 : (T)0;
-        dpk = inv * (sr[e] - a1 * dprev);
+      for (int f = 0; f < 4; ++f) {
+        T xn = xin[(size_t)k * N + nb[f]];
+        if (PRO) xn = xn + xc[(size_t)k * ncoarse + pn[f]];
+        hs = hs + A.h[f * plane + i] * xn;
       }
-      ssp[e] = cpk;
-      sr[e] = dpk;
-      cprev = cpk;
-      dprev = dpk;
+      out[kk] = b[i] + hs;
     }
-    T znext = (T)0;
-    for (int k = nl - 1; k >= 0; --k) {
-      const int e = k * tc + j;
-      T z = sr[e];
-      if (k < nl - 1) z = z - ssp[e] * znext;
-      sr[e] = z;
-      znext = z;
+#pragma unroll
+    for (int kk = 0; kk < KC; ++kk)
+      if (kk < kn) r[(size_t)(k0 + kk) * N + c] = out[kk];
+  }
+}
+
+// (2) k_helm_subst: the substitutions of columnwise_op_appinv with the
+//     per-operator Thomas factors (inverse denominators inv, c'):
+//       d'_k = inv_k (r_k - sub_k d'_{k-1}),  z_k = d'_k - c'_k z_{k+1},
+//     then x_out = omega z + (1 - omega) x_in.  One thread per column; d'
+//     goes to shared memory [level][thread].  The recurrence is two
+//     multiply-adds per level, so the kernel lives on memory-level
+//     parallelism: each sweep walks the column in blocks of SP levels and
+//     loads block b+1 (clamped addresses, no conditional loads) before it
+//     computes block b.
+constexpr int SP = 8;
+
+template <class T, bool XIN, bool PRO>
+__global__ void __launch_bounds__(128) k_helm_subst(
+    int ncol, int nl, const T* __restrict__ r, const T* __restrict__ sub,
+    const T* __restrict__ inv, const T* __restrict__ cp, const T* __restrict__ xin,
+    const int* __restrict__ parent, const T* __restrict__ xc, int ncoarse, T omega,
+    T* __restrict__ xout) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sd = reinterpret_cast<T*>(smem_raw);     // [nl][blockDim]
+  const int t = threadIdx.x, bs = blockDim.x;
+  const unsigned c = blockIdx.x * bs + t;
+  if (c >= (unsigned)ncol) return;
+  const size_t N = ncol;
+  const int nb = (nl + SP - 1) / SP;
+  auto at = [&](int k) { return (size_t)min(max(k, 0), nl - 1) * N + c; };
+  // forward sweep
+  T ar[SP], ai[SP], as[SP], br[SP], bi[SP], bsb[SP];
+#pragma unroll
+  for (int p = 0; p < SP; ++p) {
+    const size_t i = at(p);
+    ar[p] = r[i];
+    ai[p] = inv[i];
+    as[p] = sub[i];
+  }
+  T d = (T)0;
+  for (int blk = 0; blk < nb; ++blk) {
+    const int k0 = blk * SP;
+#pragma unroll
+    for (int p = 0; p < SP; ++p) {
+      const size_t i = at(k0 + SP + p);
+      br[p] = r[i];
+      bi[p] = inv[i];
+      bsb[p] = sub[i];
+    }
+#pragma unroll
+    for (int p = 0; p < SP; ++p) {
+      const int k = k0 + p;
+      const T dn = k == 0 ? ai[p] * ar[p] : ai[p] * (ar[p] - as[p] * d);
+      if (k < nl) {
+        d = dn;
+        sd[k * bs + t] = d;
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < SP; ++p) {
+      ar[p] = br[p];
+      ai[p] = bi[p];
+      as[p] = bsb[p];
     }
   }
-  __syncthreads();
-  // phase 3
+  // backward sweep
+  const int pc = PRO ? parent[c] : 0;
   const T om1 = (T)1 - omega;
-  for (int e = threadIdx.x; e < tile; e += blockDim.x) {
-    const int k = e / tc, j = e - k * tc;
-    const unsigned c = c0 + j;
-    if (c >= N) continue;
-    T v = omega * sr[e];
-    if (XIN) v = v + om1 * sx[e];
-    xout[(size_t)k * N + c] = v;
+  auto xv_at = [&](int k) -> T {
+    const int kk = min(max(k, 0), nl - 1);
+    T v = xin[(size_t)kk * N + c];
+    if (PRO) v = v + xc[(size_t)kk * ncoarse + pc];
+    return v;
+  };
+  T ac[SP], ax[SP], bc[SP], bx[SP];
+  const int ktop = nl - 1;
+#pragma unroll
+  for (int p = 0; p < SP; ++p) {
+    ac[p] = cp[at(ktop - p)];
+    if (XIN) ax[p] = xv_at(ktop - p);
+  }
+  T z = (T)0;
+  for (int blk = 0; blk < nb; ++blk) {
+    const int k0 = ktop - blk * SP;
+#pragma unroll
+    for (int p = 0; p < SP; ++p) {
+      bc[p] = cp[at(k0 - SP - p)];
+      if (XIN) bx[p] = xv_at(k0 - SP - p);
+    }
+#pragma unroll
+    for (int p = 0; p < SP; ++p) {
+      const int k = k0 - p;
+      if (k >= 0) {
+        const T dk = sd[k * bs + t];
+        z = (k == ktop) ? dk : dk - ac[p] * z;
+        T v = omega * z;
+        if (XIN) v = v + om1 * ax[p];
+        xout[(size_t)k * N + c] = v;
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < SP; ++p) {
+      ac[p] = bc[p];
+      if (XIN) ax[p] = bx[p];
+    }
   }
 }
 
 // bc(C,k) = sum over the children q (y outer, x inner) of (b - A x)(child,k):
 // residual fused with restrict_mass_w3 (sci_restrict_mass_w3_kernel_mod.F90:126-179).
-// One thread per coarse element (level, coarse column).
+// Thread = (coarse column, chunk of KR levels), loads issued before use.
+constexpr int KR = 2;
 template <class T>
 __global__ void __launch_bounds__(256) k_helm_resid_restrict(HelmArgs<T> A,
                                                              const T* __restrict__ x,
@@ -197,21 +313,46 @@ __global__ void __launch_bounds__(256) k_helm_resid_restrict(HelmArgs<T> A,
                                                              const int* __restrict__ child,
                                                              int ncoarse, int nq) {
   const unsigned NC = ncoarse, N = A.ncol;
-  const unsigned total = NC * (unsigned)A.nl;
-  for (unsigned e = blockIdx.x * blockDim.x + threadIdx.x; e < total; e += gridDim.x * blockDim.x) {
-    const unsigned k = e / NC, C = e - k * NC;
-    T acc = (T)0;
+  const int nl = A.nl;
+  const size_t plane = (size_t)nl * N;
+  const int nchunk = (nl + KR - 1) / KR;
+  const unsigned total = NC * (unsigned)nchunk;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
+    const unsigned kc = t / NC, C = t - kc * NC;
+    const int k0 = kc * KR;
+    const int kn = min(KR, nl - k0);
+    T acc[KR];
+#pragma unroll
+    for (int kk = 0; kk < KR; ++kk) acc[kk] = (T)0;
     for (int q = 0; q < nq; ++q) {
       const unsigned c = child[q * NC + C];
-      const size_t i = (size_t)k * N + c;
-      const T xm = k > 0 ? x[i - N] : (T)0;
-      const T xp = k + 1 < (unsigned)A.nl ? x[i + N] : (T)0;
-      T xn[4];
+      int nb[4];
 #pragma unroll
-      for (int f = 0; f < 4; ++f) xn[f] = x[(size_t)k * N + A.links[f * N + c]];
-      acc = acc + (b[i] - helm_row(A, i, (int)k, xm, x[i], xp, xn));
+      for (int f = 0; f < 4; ++f) nb[f] = A.links[f * N + c];
+      T xv[KR + 2];
+#pragma unroll
+      for (int u = 0; u < KR + 2; ++u) {
+        const int k = min(max(k0 - 1 + u, 0), nl - 1);
+        xv[u] = x[(size_t)k * N + c];
+      }
+#pragma unroll
+      for (int kk = 0; kk < KR; ++kk) {
+        const int k = min(k0 + kk, nl - 1);
+        const size_t i = (size_t)k * N + c;
+        T xn[4], hv[4];
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+          xn[f] = x[(size_t)k * N + nb[f]];
+          hv[f] = A.h[f * plane + i];
+        }
+        const T v = helm_row_v(A.sub[i], A.diag[i], A.sup[i], hv, xv[kk], xv[kk + 1],
+                               xv[kk + 2], xn, k > 0, k < nl - 1);
+        acc[kk] = acc[kk] + (b[i] - v);
+      }
     }
-    bc[e] = acc;
+#pragma unroll
+    for (int kk = 0; kk < KR; ++kk)
+      if (kk < kn) bc[(size_t)(k0 + kk) * NC + C] = acc[kk];
   }
 }
 
@@ -271,53 +412,59 @@ __global__ void k_convert(TO* __restrict__ y, const TI* __restrict__ x, size_t n
     y[i] = (TO)x[i];
 }
 
-// dynamic shared memory one block may use (B200: up to 227 KB per block)
-constexpr size_t kSmemCap = 200 * 1024;
-
-// Columns per smoother tile: as wide as shared memory allows (at most 64),
-// narrowed on small meshes so that every SM receives blocks.
-int smooth_tile(int ncol, int nl, size_t elem, int nsm) {
-  int tc = 64;
-  while (tc > 8 && (size_t)5 * nl * tc * elem > kSmemCap) tc /= 2;
-  while (tc > 8 && (ncol + tc - 1) / tc < 2 * nsm) tc /= 2;
-  return tc;
-}
-
 template <class T, bool XIN, bool PRO>
-void launch_smooth_t(lfg_helm op, T omega, const T* xin, const T* b, T* xout,
-                     const int* parent, const T* xc, int ncoarse) {
-  lfg_ctx c = op->ctx;
-  const int tc = smooth_tile(op->ncol, op->nl, sizeof(T), c->num_sms);
-  const size_t smem = (size_t)5 * op->nl * tc * sizeof(T);
-  if (smem > kSmemCap)
-    throw Error(LFG_ERR_ARG, "helm_smooth: column too tall for the shared-memory tile");
-  auto kern = k_helm_smooth<T, XIN, PRO>;
+void launch_subst(lfg_ctx c, int ncol, int nl, const T* r, const T* sub, const T* inv,
+                  const T* cp, const T* xin, const int* parent, const T* xc, int ncoarse,
+                  T omega, T* xout) {
+  // spread small meshes over every SM
+  int bs = 128;
+  while (bs > 32 && (ncol + bs - 1) / bs < 2 * c->num_sms) bs /= 2;
+  const size_t smem = (size_t)nl * bs * sizeof(T);
+  constexpr size_t cap = 200 * 1024;
+  if ((size_t)nl * 32 * sizeof(T) > cap)
+    throw Error(LFG_ERR_ARG, "helm_smooth: column too tall for shared memory");
+  while ((size_t)nl * bs * sizeof(T) > cap) bs /= 2;
+  auto kern = k_helm_subst<T, XIN, PRO>;
   static bool attr_set = false;
   if (!attr_set) {
-    LFG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)kSmemCap));
+    LFG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap));
     attr_set = true;
   }
-  const int grid = (op->ncol + tc - 1) / tc;
-  kern<<<grid, 256, smem, c->stream>>>(args_of<T>(op), omega, xin, b, xout, parent, xc,
-                                       ncoarse, tc);
-  after_launch(c, "helm_smooth");
+  kern<<<(ncol + bs - 1) / bs, bs, (size_t)nl * bs * sizeof(T), c->stream>>>(
+      ncol, nl, r, sub, inv, cp, xin, parent, xc, ncoarse, omega, xout);
+  (void)smem;
+  after_launch(c, "helm_subst");
 }
 
 template <class T>
 void smooth_t(lfg_helm op, double omega, lfg_field x_in, lfg_field b, lfg_field x_out,
-              lfg_intergrid ig, lfg_field xc) {
+              lfg_intergrid ig, lfg_field xc, void* rbuf) {
+  lfg_ctx c = op->ctx;
   const T om = (T)omega;
-  const T* xi = x_in ? (const T*)x_in->d : nullptr;
-  if (!x_in)
-    launch_smooth_t<T, false, false>(op, om, nullptr, (const T*)b->d, (T*)x_out->d, nullptr,
-                                     nullptr, 0);
-  else if (!ig)
-    launch_smooth_t<T, true, false>(op, om, xi, (const T*)b->d, (T*)x_out->d, nullptr,
-                                    nullptr, 0);
-  else
-    launch_smooth_t<T, true, true>(op, om, xi, (const T*)b->d, (T*)x_out->d, ig->parent,
-                                   (const T*)xc->d, ig->ncoarse);
+  const T* sub = (const T*)op->sub;
+  const T* inv = (const T*)op->inv;
+  const T* cp = (const T*)op->cp;
+  if (!x_in) {
+    launch_subst<T, false, false>(c, op->ncol, op->nl, (const T*)b->d, sub, inv, cp, nullptr,
+                                  nullptr, nullptr, 0, om, (T*)x_out->d);
+    return;
+  }
+  T* r = (T*)rbuf;
+  const int grid = c->stream_grid((size_t)op->ncol * ((op->nl + KC - 1) / KC), 256);
+  if (!ig) {
+    k_helm_rhs<T, false><<<grid, 256, 0, c->stream>>>(args_of<T>(op), (const T*)x_in->d,
+                                                       (const T*)b->d, r, nullptr, nullptr, 0);
+    after_launch(c, "helm_rhs");
+    launch_subst<T, true, false>(c, op->ncol, op->nl, r, sub, inv, cp, (const T*)x_in->d,
+                                 nullptr, nullptr, 0, om, (T*)x_out->d);
+  } else {
+    k_helm_rhs<T, true><<<grid, 256, 0, c->stream>>>(args_of<T>(op), (const T*)x_in->d,
+                                                      (const T*)b->d, r, ig->parent,
+                                                      (const T*)xc->d, ig->ncoarse);
+    after_launch(c, "helm_rhs");
+    launch_subst<T, true, true>(c, op->ncol, op->nl, r, sub, inv, cp, (const T*)x_in->d,
+                                ig->parent, (const T*)xc->d, ig->ncoarse, om, (T*)x_out->d);
+  }
 }
 
 void check_field(lfg_helm op, lfg_field f, const char* what) {
@@ -334,18 +481,22 @@ void helm_apply(lfg_helm op, lfg_field y, lfg_field x, lfg_field dot_with, int s
   check_field(op, y, "helm_apply");
   check_field(op, x, "helm_apply");
   lfg_ctx c = op->ctx;
-  const int bs = 256, grid = c->stream_grid((size_t)op->ncol * op->nl, bs);
+  const int bs = 256, grid = c->stream_grid((size_t)op->ncol * ((op->nl + KC - 1) / KC), bs);
   Red r = slot >= 0 ? c->red(slot) : Red{nullptr, nullptr, nullptr};
   if (op->kind == LFG_R_DOUBLE) {
     using T = double;
-    if (slot >= 0)
-      k_helm_apply<T, false, true><<<grid, bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, nullptr, (T*)y->d, dot_with ? (const T*)dot_with->d : nullptr, r);
+    if (slot >= 0 && dot_with)
+      k_helm_apply<T, false, true, true><<<grid, bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, nullptr, (T*)y->d, (const T*)dot_with->d, r);
+    else if (slot >= 0)
+      k_helm_apply<T, false, true, false><<<grid, bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, nullptr, (T*)y->d, nullptr, r);
     else
       k_helm_apply<T, false, false><<<grid, bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, nullptr, (T*)y->d, nullptr, r);
   } else {
     using T = float;
-    if (slot >= 0)
-      k_helm_apply<T, false, true><<<grid, bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, nullptr, (T*)y->d, dot_with ? (const T*)dot_with->d : nullptr, r);
+    if (slot >= 0 && dot_with)
+      k_helm_apply<T, false, true, true><<<grid, bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, nullptr, (T*)y->d, (const T*)dot_with->d, r);
+    else if (slot >= 0)
+      k_helm_apply<T, false, true, false><<<grid, bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, nullptr, (T*)y->d, nullptr, r);
     else
       k_helm_apply<T, false, false><<<grid, bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, nullptr, (T*)y->d, nullptr, r);
   }
@@ -357,7 +508,7 @@ void helm_residual(lfg_helm op, lfg_field r_out, lfg_field x, lfg_field b, int s
   check_field(op, x, "helm_residual");
   check_field(op, b, "helm_residual");
   lfg_ctx c = op->ctx;
-  const int bs = 256, grid = c->stream_grid((size_t)op->ncol * op->nl, bs);
+  const int bs = 256, grid = c->stream_grid((size_t)op->ncol * ((op->nl + KC - 1) / KC), bs);
   Red r = slot >= 0 ? c->red(slot) : Red{nullptr, nullptr, nullptr};
   if (op->kind == LFG_R_DOUBLE) {
     using T = double;
@@ -376,7 +527,7 @@ void helm_residual(lfg_helm op, lfg_field r_out, lfg_field x, lfg_field b, int s
 }
 
 void helm_smooth(lfg_helm op, double omega, lfg_field x_in, lfg_field b, lfg_field x_out,
-                 lfg_intergrid ig, lfg_field xc) {
+                 lfg_intergrid ig, lfg_field xc, void* rbuf) {
   check_field(op, b, "helm_smooth");
   check_field(op, x_out, "helm_smooth");
   if (x_in) {
@@ -388,8 +539,9 @@ void helm_smooth(lfg_helm op, double omega, lfg_field x_in, lfg_field b, lfg_fie
                     xc->nlev == op->nl && xc->kind == op->kind,
                 "helm_smooth: bad prolongation arguments");
   }
-  if (op->kind == LFG_R_DOUBLE) smooth_t<double>(op, omega, x_in, b, x_out, ig, xc);
-  else smooth_t<float>(op, omega, x_in, b, x_out, ig, xc);
+  if (x_in && !rbuf) rbuf = op->ctx->scratch((size_t)op->ncol * op->nl * op->kind);
+  if (op->kind == LFG_R_DOUBLE) smooth_t<double>(op, omega, x_in, b, x_out, ig, xc, rbuf);
+  else smooth_t<float>(op, omega, x_in, b, x_out, ig, xc, rbuf);
 }
 
 void helm_residual_restrict(lfg_helm op, lfg_intergrid ig, lfg_field x, lfg_field b,
@@ -400,7 +552,7 @@ void helm_residual_restrict(lfg_helm op, lfg_intergrid ig, lfg_field x, lfg_fiel
                   bc->kind == op->kind && ig->nx * ig->ny <= 4,
               "residual_restrict: bad coarse field");
   lfg_ctx c = op->ctx;
-  const int bs = 256, grid = c->stream_grid((size_t)ig->ncoarse * op->nl, bs);
+  const int bs = 256, grid = c->stream_grid((size_t)ig->ncoarse * ((op->nl + KR - 1) / KR), bs);
   if (op->kind == LFG_R_DOUBLE)
     k_helm_resid_restrict<double><<<grid, bs, 0, c->stream>>>(args_of<double>(op), (const double*)x->d, (const double*)b->d, (double*)bc->d, ig->child, ig->ncoarse, ig->nx * ig->ny);
   else
@@ -437,12 +589,27 @@ static lfg_helm new_helm(lfg_ctx c, lfg_mesh mesh, int kind, int nl) {
     op->diag = dmalloc(n * kind);
     op->sup = dmalloc(n * kind);
     op->h = dmalloc(4 * n * kind);
+    op->inv = dmalloc(n * kind);
+    op->cp = dmalloc(n * kind);
   } catch (...) {
-    dfree(op->sub); dfree(op->diag); dfree(op->sup); dfree(op->h);
+    dfree(op->sub); dfree(op->diag); dfree(op->sup); dfree(op->h); dfree(op->inv);
+    dfree(op->cp);
     delete op;
     throw;
   }
   return op;
+}
+
+// Thomas factors of the operator's T' (after its bands change).
+static void factor_helm(lfg_helm op) {
+  lfg_ctx c = op->ctx;
+  const int bs = 128, grid = (op->ncol + bs - 1) / bs;
+  if (op->kind == LFG_R_DOUBLE)
+    k_helm_factor<double><<<grid, bs, 0, c->stream>>>((const double*)op->sub, (const double*)op->diag, (const double*)op->sup, (double*)op->inv, (double*)op->cp, op->ncol, op->nl);
+  else
+    k_helm_factor<float><<<grid, bs, 0, c->stream>>>((const float*)op->sub, (const float*)op->diag, (const float*)op->sup, (float*)op->inv, (float*)op->cp, op->ncol, op->nl);
+  after_launch(c, "helm_factor");
+  LFG_CUDA(cudaStreamSynchronize(c->stream));
 }
 
 extern "C" {
@@ -512,6 +679,7 @@ int lfg_helm_create(lfg_ctx c, int kind, lfg_mesh mesh, int nl, const double* cm
       put(op->diag, dg);
       put(op->sup, sp);
       put(op->h, h);
+      factor_helm(op);
     } catch (...) {
       lfg_helm_destroy(op);
       throw;
@@ -526,6 +694,8 @@ int lfg_helm_destroy(lfg_helm op) {
   dfree(op->diag);
   dfree(op->sup);
   dfree(op->h);
+  dfree(op->inv);
+  dfree(op->cp);
   delete op;
   return LFG_OK;
 }
@@ -537,7 +707,7 @@ int lfg_helm_apply(lfg_helm op, lfg_field y, lfg_field x) {
 
 int lfg_helm_smooth(lfg_helm op, double omega, lfg_field x_in, lfg_field b, lfg_field x_out) {
   if (!op) return LFG_ERR_ARG;
-  return guard(op->ctx, [&] { helm_smooth(op, omega, x_in, b, x_out, nullptr, nullptr); });
+  return guard(op->ctx, [&] { helm_smooth(op, omega, x_in, b, x_out, nullptr, nullptr, nullptr); });
 }
 
 int lfg_helm_coarsen(lfg_helm fine, lfg_intergrid ig, lfg_mesh cmesh, int kind,
@@ -556,7 +726,7 @@ int lfg_helm_coarsen(lfg_helm fine, lfg_intergrid ig, lfg_mesh cmesh, int kind,
                                            (double*)c64->h, ig->child, cmesh->ncol);
     try {
       after_launch(c, "galerkin");
-      LFG_CUDA(cudaStreamSynchronize(c->stream));
+      factor_helm(c64);
     } catch (...) {
       lfg_helm_destroy(c64);
       throw;
@@ -593,7 +763,12 @@ int lfg_helm_copy_kind(lfg_helm src, int kind, lfg_helm* out) {
         k_convert<double, float><<<g, kThreads, 0, c->stream>>>((double*)d_arr[a], (const float*)s_arr[a], m);
       if (src->kind != kind) after_launch(c, "convert");
     }
-    LFG_CUDA(cudaStreamSynchronize(c->stream));
+    try {
+      factor_helm(d);
+    } catch (...) {
+      lfg_helm_destroy(d);
+      throw;
+    }
     *out = d;
   });
 }

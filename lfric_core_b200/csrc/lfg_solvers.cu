@@ -21,7 +21,11 @@
 
 #include <algorithm>
 #include <cfloat>
+#include <cstdlib>
+#include <map>
+#include <set>
 #include <memory>
+#include <utility>
 
 using namespace lfg;
 
@@ -118,7 +122,7 @@ struct MgPrec : lfg_prec_s {
   std::vector<lfg_intergrid> maps;
   int n_pre, n_post, n_coarse;
   double omega;
-  std::vector<FieldPtr> bc, xa, xb;  // per level (index 0 unused for bc/xa)
+  std::vector<FieldPtr> bc, xa, xb, rr;  // per level (index 0 unused for bc/xa)
 
   MgPrec(int nlev, const lfg_helm* levels, const lfg_intergrid* ig, int pre, int post,
          int coarse, double om)
@@ -129,6 +133,7 @@ struct MgPrec : lfg_prec_s {
     bc.resize(nlev);
     xa.resize(nlev);
     xb.resize(nlev);
+    rr.resize(nlev);
     for (int l = 0; l < nlev; ++l) {
       const lfg_helm h = ops[l];
       if (l > 0) {
@@ -136,6 +141,7 @@ struct MgPrec : lfg_prec_s {
         xa[l] = make_field(ctx, h->kind, h->ncol, h->nl);
       }
       xb[l] = make_field(ctx, h->kind, h->ncol, h->nl);
+      rr[l] = make_field(ctx, h->kind, h->ncol, h->nl);
     }
   }
 
@@ -146,7 +152,8 @@ struct MgPrec : lfg_prec_s {
     lfg_field src = in;
     for (int i = 0; i < s; ++i) {
       lfg_field dst = ((s - 1 - i) % 2 == 0) ? out : tmp;
-      helm_smooth(ops[l], omega, src, b, dst, i == 0 ? ig : nullptr, i == 0 ? xc : nullptr);
+      helm_smooth(ops[l], omega, src, b, dst, i == 0 ? ig : nullptr, i == 0 ? xc : nullptr,
+                  rr[l]->d);
       src = dst;
     }
   }
@@ -170,13 +177,77 @@ struct MgPrec : lfg_prec_s {
       prolong_add(maps[l], P, xa[l + 1].get());
   }
 
+  // One captured CUDA graph per (input, output) buffer pair: the V-cycle is
+  // a fixed sequence of ~20 launches per level, and the Krylov solvers
+  // apply the preconditioner to a small fixed set of vectors, so replaying
+  // a graph removes the per-kernel launch gaps.
+  struct Graph {
+    cudaGraphExec_t exec = nullptr;
+    uint64_t nodes = 0;
+  };
+  std::map<std::pair<void*, void*>, Graph> graphs;
+  std::set<std::pair<void*, void*>> seen;
+  cudaStream_t graph_stream = nullptr;
+  bool use_graphs = std::getenv("LFG_NO_GRAPHS") == nullptr;
+
+  void drop_graphs() {
+    for (auto& kv : graphs)
+      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    graphs.clear();
+    seen.clear();
+  }
+  ~MgPrec() override { drop_graphs(); }
+
   void apply(lfg_field x, lfg_field y) override {
     const lfg_helm h = ops[0];
     LFG_REQUIRE(x->ncol == h->ncol && x->nlev == h->nl && x->kind == h->kind &&
                     y->ncol == h->ncol && y->nlev == h->nl && y->kind == h->kind,
                 "multigrid apply: fields do not match the finest operator");
     LFG_REQUIRE(x->d != y->d, "multigrid apply: x and y may not alias");
-    vcycle(0, x, y);
+    cudaStream_t st = ctx->stream;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    LFG_CUDA(cudaStreamIsCapturing(st, &cs));
+    if (!use_graphs || cs != cudaStreamCaptureStatusNone) {
+      vcycle(0, x, y);
+      return;
+    }
+    if (graph_stream != st) {  // graphs are replayed on the stream they target
+      drop_graphs();
+      graph_stream = st;
+    }
+    auto key = std::make_pair(x->d, y->d);
+    auto it = graphs.find(key);
+    if (it == graphs.end() && !seen.count(key)) {
+      // first use of this pair runs eagerly (one-time kernel set-up such as
+      // shared-memory attributes happens outside any capture)
+      seen.insert(key);
+      vcycle(0, x, y);
+      return;
+    }
+    if (it == graphs.end()) {
+      Graph g;
+      const uint64_t n0 = ctx->launches;
+      LFG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      try {
+        vcycle(0, x, y);
+      } catch (...) {
+        cudaGraph_t dummy = nullptr;
+        cudaStreamEndCapture(st, &dummy);
+        if (dummy) cudaGraphDestroy(dummy);
+        throw;
+      }
+      cudaGraph_t graph = nullptr;
+      LFG_CUDA(cudaStreamEndCapture(st, &graph));
+      cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess)
+        throw Error(LFG_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+      g.nodes = ctx->launches - n0;
+      ctx->launches = n0;
+      it = graphs.emplace(key, g).first;
+    }
+    LFG_CUDA(cudaGraphLaunch(it->second.exec, st));
+    ctx->launches += it->second.nodes;
   }
 };
 
