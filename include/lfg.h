@@ -149,6 +149,25 @@ int lfg_cma_apply_inverse(lfg_cma cma, lfg_field lhs, lfg_field x);
 int lfg_tri_solve(lfg_field y, lfg_field x, lfg_field tri_0, lfg_field tri_plus,
                   lfg_field tri_minus);
 
+/* Thomas solve of the tri_solve kernel for callers that cannot allocate
+ * device memory.  No counterpart in the reference: it exists for hosts whose
+ * device memory is owned by another allocator (an application that reserves
+ * the GPU's memory up front, a caching pool) or that are recovering from an
+ * out-of-memory error, and so cannot call cudaMalloc or create a context.
+ * The caller passes level-major device arrays (nlev*ncol values of `kind`)
+ * and a cudaStream_t (NULL: the legacy default stream).  Working storage is
+ * one file-scope device array of LFG_NOALLOC_SCRATCH_BYTES that every GPU
+ * loading the library keeps until exit; a call needs 2*nlev*ncol*kind bytes
+ * of it and fails with LFG_ERR_ARG beyond that.  The first call on a device
+ * looks up the array's device address.  All calls share the array: calls
+ * whose kernels overlap on the GPU (different streams, or other host
+ * threads) race on it.  Nothing in it needs clearing; each call writes its
+ * part before reading it. */
+#define LFG_NOALLOC_SCRATCH_BYTES (32u << 20)
+int lfg_tri_solve_noalloc(int kind, int ncol, int nlev, const void* x, const void* tri_0,
+                          const void* tri_plus, const void* tri_minus, void* y,
+                          void* stream);
+
 /* ------------------------------------------------------------ LMA operators
  * operator_type local_stencil(ncell*nlayers, ndf_to, ndf_from) in Fortran
  * order (infrastructure/source/operator/operator_mod.t90:113-119) with the

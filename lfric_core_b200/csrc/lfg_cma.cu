@@ -15,6 +15,7 @@
 #include "lfg_internal.cuh"
 
 #include <algorithm>
+#include <mutex>
 
 using namespace lfg;
 
@@ -280,9 +281,53 @@ void dispatch(int kind, F&& f) {
   else f(float{});
 }
 
+// Working storage of lfg_tri_solve_noalloc: c' and d' of every column.  In
+// host code this name only stands for the array; the kernel is given the
+// device address looked up with cudaGetSymbolAddress.
+__device__ __align__(256) unsigned char g_noalloc_scratch[LFG_NOALLOC_SCRATCH_BYTES];
+
+std::mutex g_noalloc_mu;
+std::vector<void*> g_noalloc_addr;  // per device ordinal, null until looked up
+
 }  // namespace
 
 extern "C" {
+
+int lfg_tri_solve_noalloc(int kind, int ncol, int nlev, const void* x, const void* tri_0,
+                          const void* tri_plus, const void* tri_minus, void* y,
+                          void* stream) {
+  if ((kind != LFG_R_DOUBLE && kind != LFG_R_SINGLE) || ncol <= 0 || nlev <= 0 || !x ||
+      !tri_0 || !tri_plus || !tri_minus || !y)
+    return LFG_ERR_ARG;
+  if ((size_t)2 * nlev * ncol * kind > (size_t)LFG_NOALLOC_SCRATCH_BYTES) return LFG_ERR_ARG;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return LFG_ERR_CUDA;
+  void* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if ((int)g_noalloc_addr.size() <= dev) g_noalloc_addr.resize(dev + 1, nullptr);
+    if (!g_noalloc_addr[dev]) {
+      void* p = nullptr;
+      if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return LFG_ERR_CUDA;
+      g_noalloc_addr[dev] = p;
+    }
+    scratch = g_noalloc_addr[dev];
+  }
+  const int bs = 128, grid = (ncol + bs - 1) / bs;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (kind == LFG_R_DOUBLE) {
+    TriSrc<double> s{ncol, nlev, nullptr, (const double*)tri_0, (const double*)tri_plus,
+                     (const double*)tri_minus, nullptr, 0};
+    k_thomas_scratch<double, SRC_FIELDS><<<grid, bs, 0, st>>>(s, (const double*)x, (double*)y,
+                                                               (double*)scratch);
+  } else {
+    TriSrc<float> s{ncol, nlev, nullptr, (const float*)tri_0, (const float*)tri_plus,
+                    (const float*)tri_minus, nullptr, 0};
+    k_thomas_scratch<float, SRC_FIELDS><<<grid, bs, 0, st>>>(s, (const float*)x, (float*)y,
+                                                              (float*)scratch);
+  }
+  return cudaGetLastError() == cudaSuccess ? LFG_OK : LFG_ERR_CUDA;
+}
 
 // ------------------------------------------------------------- CMA objects
 int lfg_cma_create(lfg_ctx c, int kind, int ncol, int nrow, int ncolumn, int bw, int alpha,
