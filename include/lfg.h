@@ -142,6 +142,9 @@ int lfg_cma_create(lfg_ctx ctx, int kind, int ncol, int nrow, int ncolumn, int b
 int lfg_cma_destroy(lfg_cma cma);
 /* lhs += A x (sci_columnwise_op_app_kernel_mod.F90:73-124). */
 int lfg_cma_apply(lfg_cma cma, lfg_field lhs, lfg_field x);
+/* lhs += A^T x: the adjoint of lfg_cma_apply (lhs on the from-space, x on
+ * the to-space); each output row gathers the band entries that reach it. */
+int lfg_cma_apply_transpose(lfg_cma cma, lfg_field lhs, lfg_field x);
 /* lhs = A^{-1} x for a tridiagonal A (bandwidth 3), Thomas algorithm
  * (sci_columnwise_op_appinv_kernel_mod.F90:77-145). */
 int lfg_cma_apply_inverse(lfg_cma cma, lfg_field lhs, lfg_field x);
@@ -222,6 +225,8 @@ int lfg_helm_copy_kind(lfg_helm src, int kind, lfg_helm* dst);
  *   (sci_iterative_solver_mod.f90:38-57). */
 int lfg_linop_from_helm(lfg_helm helm, lfg_linop* op);
 int lfg_linop_from_lma(lfg_lma lma, lfg_linop* op);        /* mass_matrix_operator */
+/* The transposed operator y = A^T x (transpose_matrix_vector), for adjoint solves. */
+int lfg_linop_from_lma_transpose(lfg_lma lma, lfg_linop* op);
 int lfg_linop_destroy(lfg_linop op);
 int lfg_linop_apply(lfg_linop op, lfg_field x, lfg_field y);          /* y = A x */
 

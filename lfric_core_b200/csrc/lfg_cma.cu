@@ -205,6 +205,28 @@ __global__ void k_cma_app(const T* __restrict__ bands, const int* __restrict__ i
   lhs[o] = acc;
 }
 
+// lhs(ind_from(j)) += sum over rows i whose band reaches column j of
+// band(j - j_minus(i), i) x(ind_to(i)): the transpose of k_cma_app.  The
+// rows reaching each column are listed per column (CSR, rows ascending).
+template <class T>
+__global__ void k_cma_app_t(const T* __restrict__ bands, const int* __restrict__ ind_to,
+                            const int* __restrict__ ind_from, const int* __restrict__ jminus,
+                            const int* __restrict__ tptr, const int* __restrict__ trow,
+                            int ncol, int nrow, const T* __restrict__ x, T* __restrict__ lhs) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (c >= ncol) return;
+  const size_t N = ncol, plane = (size_t)nrow * N;
+  const size_t o = (size_t)ind_from[j] * N + c;
+  T acc = lhs[o];
+  for (int q = tptr[j]; q < tptr[j + 1]; ++q) {
+    const int i = trow[q];
+    acc = acc + bands[(size_t)(j - jminus[i]) * plane + (size_t)i * N + c] *
+                    x[(size_t)ind_to[i] * N + c];
+  }
+  lhs[o] = acc;
+}
+
 // ------------------------------------------------------------- intergrid
 // coarse(C,k) from the fine children, y outer and x inner (slot q = y*nx+x).
 template <class T, int MODE>
@@ -389,6 +411,17 @@ int lfg_cma_create(lfg_ctx c, int kind, int ncol, int nrow, int ncolumn, int bw,
       m->jminus = (int*)dmalloc(nrow * sizeof(int));
       m->jplus = (int*)dmalloc(nrow * sizeof(int));
       upload(m->jplus, jp.data(), nrow * sizeof(int));
+      // rows reaching each column, for the transposed apply
+      std::vector<int> tptr(ncolumn + 1, 0), trow;
+      for (int j = 0; j < ncolumn; ++j) {
+        for (int i = 0; i < nrow; ++i)
+          if (j >= std::max(0, jm[i]) && j <= std::min(ncolumn - 1, jp[i])) trow.push_back(i);
+        tptr[j + 1] = (int)trow.size();
+      }
+      m->tptr = (int*)dmalloc(tptr.size() * sizeof(int));
+      m->trow = (int*)dmalloc(std::max<size_t>(1, trow.size()) * sizeof(int));
+      upload(m->tptr, tptr.data(), tptr.size() * sizeof(int));
+      if (!trow.empty()) upload(m->trow, trow.data(), trow.size() * sizeof(int));
       upload(m->ind_to, it.data(), nrow * sizeof(int));
       upload(m->ind_from, iff.data(), ncolumn * sizeof(int));
       upload(m->jminus, jm.data(), nrow * sizeof(int));
@@ -407,6 +440,8 @@ int lfg_cma_destroy(lfg_cma m) {
   dfree(m->ind_from);
   dfree(m->jminus);
   dfree(m->jplus);
+  dfree(m->tptr);
+  dfree(m->trow);
   delete m;
   return LFG_OK;
 }
@@ -427,6 +462,25 @@ int lfg_cma_apply(lfg_cma m, lfg_field lhs, lfg_field x) {
                                                 m->ncolumn, (const T*)x->d, (T*)lhs->d);
     });
     after_launch(c, "cma_app");
+  });
+}
+
+int lfg_cma_apply_transpose(lfg_cma m, lfg_field lhs, lfg_field x) {
+  if (!m) return LFG_ERR_ARG;
+  lfg_ctx c = m->ctx;
+  return guard(c, [&] {
+    LFG_REQUIRE(lhs && x && lhs->ncol == m->ncol && x->ncol == m->ncol &&
+                    lhs->nlev >= m->max_ind_from && x->nlev >= m->max_ind_to &&
+                    lhs->kind == m->kind && x->kind == m->kind,
+                "cma_apply_transpose: fields do not match the operator");
+    dim3 grid((m->ncol + 127) / 128, m->ncolumn);
+    dispatch(m->kind, [&](auto tag) {
+      using T = decltype(tag);
+      k_cma_app_t<T><<<grid, 128, 0, c->stream>>>((const T*)m->bands, m->ind_to, m->ind_from,
+                                                  m->jminus, m->tptr, m->trow, m->ncol, m->nrow,
+                                                  (const T*)x->d, (T*)lhs->d);
+    });
+    after_launch(c, "cma_app_t");
   });
 }
 

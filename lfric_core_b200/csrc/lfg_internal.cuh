@@ -198,6 +198,8 @@ struct lfg_cma_s {
   int* jminus = nullptr;      // [nrow] first band column of each row (0-based)
   int* jplus = nullptr;       // [nrow] last band column of each row
   int max_ind_to = 0, max_ind_from = 0;  // largest 1-based column offsets
+  int* tptr = nullptr;        // [ncolumn+1] rows reaching each column (transpose)
+  int* trow = nullptr;
 };
 
 struct lfg_lma_s {

@@ -63,14 +63,22 @@ struct HelmLinop : lfg_linop_s {
 // the WRITE-mode gather starts every dof from zero, which is the same.
 struct LmaLinop : lfg_linop_s {
   lfg_lma m;
-  explicit LmaLinop(lfg_lma mm) : m(mm) {
+  bool transpose;
+  LmaLinop(lfg_lma mm, bool t) : m(mm), transpose(t) {
     ctx = m->ctx;
     kind = m->kind;
     ncol = m->nent_to;
     nlev = m->nlev_to;
   }
   void apply(lfg_field x, lfg_field y) override {
-    int st = lfg_lma_apply(m, LFG_LMA_WRITE, y, x);
+    int st;
+    if (!transpose) {
+      st = lfg_lma_apply(m, LFG_LMA_WRITE, y, x);
+    } else {
+      // transpose_matrix_vector increments: start from zero
+      vec_set(y, sc_const(0.0));
+      st = lfg_lma_apply(m, LFG_LMA_TRANSPOSE, y, x);
+    }
     if (st != LFG_OK) throw Error(st, ctx->last_error);
   }
 };
@@ -769,7 +777,17 @@ int lfg_linop_from_lma(lfg_lma m, lfg_linop* out) {
     LFG_REQUIRE(m->ndf_to == m->ndf_from && m->nent_to == m->nent_from &&
                     m->nlev_to == m->nlev_from,
                 "linop_from_lma: the operator must map a space onto itself");
-    *out = new LmaLinop(m);
+    *out = new LmaLinop(m, false);
+  });
+}
+
+int lfg_linop_from_lma_transpose(lfg_lma m, lfg_linop* out) {
+  if (!m || !out) return LFG_ERR_ARG;
+  return guard(m->ctx, [&] {
+    LFG_REQUIRE(m->ndf_to == m->ndf_from && m->nent_to == m->nent_from &&
+                    m->nlev_to == m->nlev_from,
+                "linop_from_lma_transpose: the operator must map a space onto itself");
+    *out = new LmaLinop(m, true);
   });
 }
 

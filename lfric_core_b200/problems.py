@@ -232,16 +232,19 @@ def w0_element_matrices(mesh) -> tuple[np.ndarray, np.ndarray]:
 
 
 def w0_problem(n: int, nlayers: int, seed: int, top: float, kappa_sigma: float = 0.0,
-               stretching: str = "uniform", radius: float = EARTH_RADIUS_DEFAULT) -> W0Problem:
-    """W0 diffusion problem: A = M + kappa K; kappa = exp(sigma g), g ~ N(0,1)
-    per 3D cell (kappa = 1 when sigma = 0); right-hand side N(0,1)."""
+               stretching: str = "uniform", radius: float = EARTH_RADIUS_DEFAULT,
+               kappa_scale: float = 1.0) -> W0Problem:
+    """W0 diffusion problem: A = M + kappa K; kappa = kappa_scale exp(sigma g),
+    g ~ N(0,1) per 3D cell (kappa = kappa_scale when sigma = 0); right-hand
+    side N(0,1).  kappa_scale = dz^2 makes the diffusion across one layer
+    comparable to the mass term."""
     from .mesh import extruded_mesh
     mesh = extruded_mesh(n, nlayers, top, stretching, radius=radius)
     mass, stiff = w0_element_matrices(mesh)
     rng = np.random.default_rng(seed)
     ncell = mesh.ncell
-    kappa = (np.exp(kappa_sigma * rng.standard_normal((ncell, nlayers)))
-             if kappa_sigma > 0 else np.ones((ncell, nlayers)))
+    kappa = kappa_scale * (np.exp(kappa_sigma * rng.standard_normal((ncell, nlayers)))
+                           if kappa_sigma > 0 else np.ones((ncell, nlayers)))
     rhs = rng.standard_normal(mesh.w0_ndof())
     return W0Problem(ncell=ncell, nlayers=nlayers, nvert=mesh.surface.nvert,
                      map=mesh.w0_dofmap(), mass=mass, stiff=stiff, kappa=kappa, rhs=rhs)
