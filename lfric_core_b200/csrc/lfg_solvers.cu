@@ -678,10 +678,13 @@ struct GmresSolver : lfg_solver_s {
     LFG_CUDA(cudaMemcpyAsync(tmp.data(), ctx->red_results + hs, tmp.size() * sizeof(double),
                              cudaMemcpyDeviceToHost, ctx->stream));
     LFG_CUDA(cudaStreamSynchronize(ctx->stream));
-    // slots hold column iv, rows 0..iv+1; the rest of h is zero
+    // slots hold column iv, rows 0..iv, and |w|^2 in row iv+1 (h(iv+1,iv) =
+    // |w|, w%norm() in the reference); the rest of h is zero
     std::fill(h.begin(), h.end(), 0.0);
-    for (int iv = 0; iv < k; ++iv)
-      for (int i = 0; i <= iv + 1; ++i) h[(size_t)i + (size_t)(k + 1) * iv] = tmp[(size_t)iv * (k + 1) + i];
+    for (int iv = 0; iv < k; ++iv) {
+      for (int i = 0; i <= iv; ++i) h[(size_t)i + (size_t)(k + 1) * iv] = tmp[(size_t)iv * (k + 1) + i];
+      h[(size_t)iv + 1 + (size_t)(k + 1) * iv] = std::sqrt(tmp[(size_t)iv * (k + 1) + iv + 1]);
+    }
   }
 };
 

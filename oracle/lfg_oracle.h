@@ -81,6 +81,10 @@ void ora_restrict_w0_code(int nlayers, const int* cell_map, int nx, int ny, int 
 void ora_prolong_w0_code(int nlayers, const int* cell_map, int nx, int ny, int ncell_fine,
                          double* fine, const double* coarse, int ndf, int undf_fine,
                          const int* map_fine, int undf_coarse, const int* map_coarse);
+/* OpenMP threads of the whole-mesh routines: sets n (> 0) and returns the
+ * number in use (1 without OpenMP). */
+int ora_threads(int n);
+
 void ora_cma_params(int nlayers, int nint_to, int nface_to, int nint_from, int nface_from,
                     const int* offsets_to, const int* offsets_from, int* out7,
                     int* indirection_to, int* indirection_from);
@@ -170,6 +174,18 @@ typedef struct {
                                       ora_apply_##S prec, void* pctx, int monitor, T* x,\
                                       const T* b, T* work /* 2n */,                     \
                                       ora_solve_info* info);                            \
+  int ora_bicgstab_solve_##S(long n, ora_apply_##S linop, void* lctx, ora_apply_##S prec,\
+                             void* pctx, double r_tol, double a_tol, int max_iter,      \
+                             int monitor, T* x, const T* b, T* work /* 8n */,           \
+                             ora_solve_info* info);                                     \
+  int ora_gmres_solve_##S(long n, ora_apply_##S linop, void* lctx, ora_apply_##S prec,   \
+                          void* pctx, int k, double r_tol, double a_tol, int max_iter,  \
+                          int monitor, T* x, const T* b, T* work /* (4 + k) n */,       \
+                          ora_solve_info* info);                                        \
+  int ora_fgmres_solve_##S(long n, ora_apply_##S linop, void* lctx, ora_apply_##S prec,  \
+                           void* pctx, int k, double r_tol, double a_tol, int max_iter, \
+                           int monitor, T* x, const T* b, T* work /* (5 + 2k) n */,     \
+                           ora_solve_info* info);                                       \
   void ora_helm_apply_cb_##S(void* op, const T* x, T* y);                               \
   void ora_mg_apply_cb_##S(void* mg, const T* x, T* y);
 ORA_DECL_SOLVERS(double, d)
@@ -205,6 +221,14 @@ typedef struct {
 int ora_mixed_gcr_mg_solve(const ora_helm_d* op64, ora_mg_f* mg32, const double* b,
                            double* x, double tol, int max_outer, int gcrk,
                            double inner_tol, int inner_max_iter, ora_mixed_info* info);
+
+/* Mixed-precision refinement with an inner FP32 CG preconditioned by the
+ * exact column solve T'^{-1}: x = 0; r = b - A x (FP64) until
+ * ||r|| <= tol ||b|| or max_outer corrections; each correction e is
+ * cg_solve (monitor on, a_tol 0) on A_32 e = float(r) to inner_tol. */
+int ora_mixed_cg_col_solve(const ora_helm_d* op64, const ora_helm_f* op32, const double* b,
+                           double* x, double tol, int max_outer, double inner_tol,
+                           int max_inner, ora_mixed_info* info);
 
 #ifdef __cplusplus
 }

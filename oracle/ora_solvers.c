@@ -6,9 +6,17 @@
 #include <math.h>
 #include <stdlib.h>
 #include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
 #include "lfg_oracle.h"
 
 #define ORA_MAX_NL 4096
+/* Loops over more than ORA_OMP_MIN values run on OpenMP threads when the
+ * library is built with -fopenmp; inner products sum ORA_DOT_CHUNKS partial
+ * sums in a fixed order, so results do not depend on the thread count. */
+#define ORA_OMP_MIN 32768
+#define ORA_DOT_CHUNKS 256
 
 #define REAL double
 #define S d
@@ -141,4 +149,71 @@ int ora_mixed_gcr_mg_solve(const ora_helm_d* op64, ora_mg_f* mg32, const double*
 done:
   free(r); free(r32); free(e32); free(work);
   return status;
+}
+
+/* Column preconditioner z = T'^{-1} r: one block-Jacobi sweep from zero
+ * with omega = 1 (columnwise_op_appinv on every column). */
+typedef struct {
+  const ora_helm_f* op;
+  float* work;
+} ora_colprec_f;
+static void ora_colprec_apply_f(void* ctx, const float* r, float* z) {
+  const ora_colprec_f* c = (const ora_colprec_f*)ctx;
+  ora_helm_smooth_f(c->op, 1.0, NULL, r, z, c->work);
+}
+
+/* Mixed-precision refinement with an inner column-preconditioned CG
+ * (project-defined; the batched solver's per-problem algorithm):
+ *   x = 0; loop: r = b - A_64 x (FP64); stop when ||r|| <= tol ||b|| or
+ *   after max_outer corrections; e = cg_solve_32(A_32, T'^{-1}; float(r))
+ *   from zero to inner_tol relative (max_inner iterations); x += e. */
+int ora_mixed_cg_col_solve(const ora_helm_d* op64, const ora_helm_f* op32, const double* b,
+                           double* x, double tol, int max_outer, double inner_tol,
+                           int max_inner, ora_mixed_info* info) {
+  const long n = (long)op64->ncol * op64->nl;
+  double* r = (double*)malloc(sizeof(double) * n);
+  float* r32 = (float*)malloc(sizeof(float) * n);
+  float* e32 = (float*)malloc(sizeof(float) * n);
+  float* work = (float*)malloc(sizeof(float) * 3 * n);
+  ora_colprec_f cp = {op32, (float*)malloc(sizeof(float) * (n + 2 * op32->nl))};
+  int status = ORA_NOT_CONVERGED;
+  double bnorm = 0.0;
+  memset(x, 0, sizeof(double) * n);
+  info->outer_iterations = 0;
+  info->inner_iterations = 0;
+  info->final_rel_residual = 0.0;
+  for (int o = 0;; ++o) {
+    ora_helm_residual_d(op64, x, b, r);
+    const double rn = ora_norm_d(n, r);
+    if (o == 0) {
+      bnorm = rn;
+      if (rn < DBL_EPSILON) { status = ORA_OK; break; }
+    }
+    info->final_rel_residual = rn / bnorm;
+    if (isnan(info->final_rel_residual)) { status = ORA_NAN; break; }
+    if (info->final_rel_residual <= tol) { status = ORA_OK; break; }
+    if (o >= max_outer) { status = ORA_NOT_CONVERGED; break; }
+    for (long i = 0; i < n; ++i) r32[i] = (float)r[i];
+    memset(e32, 0, sizeof(float) * n);
+    ora_solve_info si;
+    ora_cg_solve_f(n, ora_helm_apply_cb_f, (void*)op32, ora_colprec_apply_f, &cp, inner_tol,
+                   0.0, max_inner, 1, e32, r32, work, &si);
+    info->inner_iterations += si.iterations;
+    for (long i = 0; i < n; ++i) x[i] = x[i] + (double)e32[i];
+    info->outer_iterations = o + 1;
+  }
+  free(r); free(r32); free(e32); free(work); free(cp.work);
+  return status;
+}
+
+/* Sets the number of OpenMP threads (n > 0) and returns the number in use;
+ * 1 when the library was built without OpenMP. */
+int ora_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+  return omp_get_max_threads();
+#else
+  (void)n;
+  return 1;
+#endif
 }

@@ -190,6 +190,19 @@ class Helmholtz:
         return x, st, info
 
 
+    def mixed_cg_col_solve(self, b, tol=1e-8, max_outer=10, inner_tol=1e-5, max_inner=200):
+        """Refinement with an inner FP32 CG preconditioned by T'^{-1}."""
+        L = lib()
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        x = np.zeros_like(b)
+        info = MixedInfo()
+        op64, op32 = self.op(0, np.float64), self.op(0, np.float32)
+        st = L.ora_mixed_cg_col_solve(C.byref(op64), C.byref(op32), ptr(b), ptr(x),
+                                      C.c_double(tol), max_outer, C.c_double(inner_tol),
+                                      max_inner, C.byref(info))
+        return x, st, info
+
+
 def _setup_signatures(L):
     L.ora_gcr_solve_d.argtypes = [C.c_long, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _dp, _dp,
@@ -197,6 +210,13 @@ def _setup_signatures(L):
     L.ora_gcr_solve_f.argtypes = [C.c_long, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _fp, _fp,
                                   _fp, C.c_void_p]
+    for nm in ("gmres", "fgmres"):
+        getattr(L, f"ora_{nm}_solve_d").argtypes = [
+            C.c_long, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double,
+            C.c_double, C.c_int, C.c_int, _dp, _dp, _dp, C.c_void_p]
+    L.ora_bicgstab_solve_d.argtypes = [C.c_long, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
+                                       C.c_double, C.c_double, C.c_int, C.c_int, _dp, _dp, _dp,
+                                       C.c_void_p]
     L.ora_cg_solve_d.argtypes = [C.c_long, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                  C.c_double, C.c_double, C.c_int, C.c_int, _dp, _dp, _dp,
                                  C.c_void_p]

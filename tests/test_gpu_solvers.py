@@ -90,18 +90,21 @@ def test_relaxation_solvers_parity(ctx, helm24, method):
     assert out.iterations == info.iterations
 
 
-def test_cg_jacobi_w0_parity(ctx):
-    """Config-1 style: W0 mass + stiffness, Jacobi-preconditioned CG to 1e-8."""
+@pytest.mark.parametrize("n,nl", [(6, 5), (24, 20)])
+def test_cg_jacobi_w0_parity(ctx, n, nl):
+    """W0 mass + stiffness with a constant coefficient 1.0, uniform 1 km
+    layers, Jacobi-preconditioned CG to 1e-8; (24, 20) is the full C24 x 20
+    plain-method workload."""
     import ctypes as C
     from oracle.oracle import lib, ptr, SolveInfo
-    p = w0_problem(6, 5, seed=1, top=5e3)
+    p = w0_problem(n, nl, seed=1, top=nl * 1e3)
     A = p.matrix()
     nent, nlev = p.nvert, p.nlayers + 1
     lma = api.LocalOperator(ctx, R_DOUBLE, p.ncell, p.nlayers, A, p.map, nent, nlev)
     diag = Field(ctx, R_DOUBLE, nent, nlev)
     lma.diagonal(diag)
     sol = api.IterativeSolver(api.LinearOperator.from_lma(lma), api.Preconditioner.diagonal(diag),
-                              diag, "cg", r_tol=1e-8, max_iter=500)
+                              diag, "cg", r_tol=1e-8, max_iter=2000)
     B, X = field_from(ctx, p.rhs, nent, nlev), Field(ctx, R_DOUBLE, nent, nlev)
     out = sol.apply(X, B)
     L = lib()
@@ -123,11 +126,48 @@ def test_cg_jacobi_w0_parity(ctx):
     info = SolveInfo()
     st = L.ora_cg_solve_d(C.c_long(p.ndof), C.cast(L.ora_lma_apply_cb, C.c_void_p), C.byref(lo),
                           C.cast(L.ora_diag_prec_apply, C.c_void_p), C.byref(dp),
-                          C.c_double(1e-8), C.c_double(0.0), 500, 1, ptr(x), ptr(np.ascontiguousarray(p.rhs)),
+                          C.c_double(1e-8), C.c_double(0.0), 2000, 1, ptr(x), ptr(np.ascontiguousarray(p.rhs)),
                           ptr(work), C.byref(info))
     assert out.status == st == 0
     assert out.iterations == info.iterations
     assert rel(X.export(), x) < 1e-12
+
+
+@pytest.mark.parametrize("method,iters", [("bicgstab", 6), ("gmres", 2), ("fgmres", 2)])
+def test_krylov_variants_parity(ctx, helm24, method, iters):
+    """bicgstab / gmres / fgmres with the multigrid preconditioner against the
+    oracle's restatement, a fixed number of iterations (gcrk = 8)."""
+    import ctypes as C
+    from oracle.oracle import lib, ptr, SolveInfo
+    p = helm24
+    ora = OraHelm(p)
+    S = api.HelmholtzSystem(ctx, p, mixed=False)
+    k = 8
+    sol = api.IterativeSolver(api.LinearOperator.from_helmholtz(S.op64), S.mg64, S.x64, method,
+                              r_tol=1e-30, max_iter=iters, gcrk=k, fail_on_non_converged=False)
+    x0 = np.random.default_rng(11).standard_normal(p.ndof) * 1e-3   # non-zero first guess
+    B, X = S.op64.field(p.rhs), S.op64.field(x0)
+    out = sol.apply(X, B)
+    L = lib()
+    op, mg = ora.op(0), ora.mg()
+    n = p.ndof
+    x = x0.copy()
+    info = SolveInfo()
+    cb_a = C.cast(L.ora_helm_apply_cb_d, C.c_void_p)
+    cb_p = C.cast(L.ora_mg_apply_cb_d, C.c_void_p)
+    b = np.ascontiguousarray(p.rhs)
+    if method == "bicgstab":
+        work = np.zeros(8 * n)
+        L.ora_bicgstab_solve_d(n, cb_a, C.byref(op), cb_p, C.byref(mg), 1e-30, 0.0, iters, 1,
+                               ptr(x), ptr(b), ptr(work), C.byref(info))
+    else:
+        work = np.zeros((5 + 2 * k) * n)
+        getattr(L, f"ora_{method}_solve_d")(n, cb_a, C.byref(op), cb_p, C.byref(mg), k, 1e-30,
+                                            0.0, iters, 1, ptr(x), ptr(b), ptr(work),
+                                            C.byref(info))
+    assert out.iterations == info.iterations
+    assert rel(X.export(), x) < 1e-12
+    assert abs(out.final_err - info.final_err) <= 1e-6 * abs(info.final_err) + 1e-15
 
 
 @pytest.mark.parametrize("method", ["bicgstab", "gmres", "fgmres", "cg"])
