@@ -282,6 +282,55 @@ int lfg_mixed_destroy(lfg_mixed mixed);
 int lfg_mixed_apply(lfg_mixed mixed, lfg_field x, lfg_field b, int* outer_iterations,
                     int* inner_iterations, double* rel_residual);
 
+/* ------------------------------------------------- batched solves
+ * Many independent W3 Helmholtz problems A_i x_i = b_i solved together in
+ * one persistent (cooperative) kernel launch, replayed from a CUDA graph.
+ * Each problem runs the mixed refinement above with an inner FP32
+ * cg_solve (sci_iterative_solver_mod.f90:495-592, monitor on, a_tol 0)
+ * preconditioned by the exact column solve T'^{-1} (columnwise_op_appinv,
+ * sci_columnwise_op_appinv_kernel_mod.F90:77-145): per outer iteration
+ * r = b - A x (FP64), inner CG on A e = float(r) to inner_tol relative or
+ * max_inner iterations, x += e (FP64), until ||b - A x|| <= tol ||b||.
+ * Problems may share an operator (several right-hand sides).  The batch
+ * has no counterpart in the reference, whose solvers handle one problem per
+ * call; each problem's arithmetic is that of the single solve. */
+typedef struct lfg_batch_s* lfg_batch;
+typedef struct {
+  double tol;           /* outer FP64 relative residual (1e-8) */
+  double inner_tol;     /* inner FP32 CG relative residual (1e-5) */
+  int max_outer;        /* refinement steps before LFG_NOT_CONVERGED (10) */
+  int max_inner;        /* inner CG iterations per refinement step (200) */
+  int tile_cols;        /* columns per tile: 64, 128, 256; 0 = autotune */
+  int blocks_per_sm;    /* co-resident CTAs per SM; 0 = autotune */
+  int use_graph;        /* 1: replay the launch from a captured CUDA graph */
+  long long spin_limit; /* bound on each grid-barrier wait, in spins; 0 = default */
+} lfg_batch_cfg;
+/* ops[i]: the r_double operator of problem i (borrowed; must outlive the
+ * batch).  cfg NULL: the defaults in parentheses above, use_graph 1. */
+int lfg_batch_create(lfg_ctx ctx, int nproblems, const lfg_helm* ops, const lfg_batch_cfg* cfg,
+                     lfg_batch* batch);
+int lfg_batch_destroy(lfg_batch batch);
+/* Device views (owned by the batch) of problem i's right-hand side and
+ * solution, for lfg_field_import / lfg_field_export. */
+int lfg_batch_rhs(lfg_batch batch, int problem, lfg_field* rhs);
+int lfg_batch_solution(lfg_batch batch, int problem, lfg_field* x);
+/* Enqueue one solve of every problem from x = 0 on the context's stream
+ * (the first call autotunes the launch shape and captures the graph). */
+int lfg_batch_launch(lfg_batch batch);
+/* Wait for it; nfailed = problems that did not reach tol.  LFG_ERR_STATE
+ * when a grid-barrier wait ran out or the phase limit was reached. */
+int lfg_batch_wait(lfg_batch batch, int* nfailed);
+int lfg_batch_solve(lfg_batch batch, int* nfailed);   /* launch + wait */
+int lfg_batch_result(lfg_batch batch, int problem, int* status, int* outer_iterations,
+                     int* inner_iterations, double* rel_residual);
+/* Launch shape in use and the phases (grid barriers) of the last solve. */
+int lfg_batch_tuning(lfg_batch batch, int* tile_cols, int* blocks_per_sm, int* grid_blocks,
+                     int* phases);
+/* Test hook: the grid barrier waits for extra_arrivals CTAs beyond the
+ * grid, so every wait runs out after spin_limit spins and the next solve
+ * must end with LFG_ERR_STATE.  0 restores normal operation. */
+int lfg_batch_test_stall(lfg_batch batch, int extra_arrivals);
+
 #ifdef __cplusplus
 }
 #endif

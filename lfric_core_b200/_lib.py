@@ -23,6 +23,12 @@ class lfg_solver_cfg(C.Structure):
                 ("rho_relax", C.c_double), ("lmin", C.c_double), ("lmax", C.c_double)]
 
 
+class lfg_batch_cfg(C.Structure):
+    _fields_ = [("tol", C.c_double), ("inner_tol", C.c_double), ("max_outer", C.c_int),
+                ("max_inner", C.c_int), ("tile_cols", C.c_int), ("blocks_per_sm", C.c_int),
+                ("use_graph", C.c_int), ("spin_limit", C.c_longlong)]
+
+
 def _ctype(tok: str):
     t = " ".join(tok.replace("const ", "").split())
     table = {
@@ -31,6 +37,7 @@ def _ctype(tok: str):
         "uint64_t*": C.POINTER(C.c_uint64), "char*": C.c_char_p,
         "void**": C.POINTER(C.c_void_p),
         "lfg_solver_cfg*": C.POINTER(lfg_solver_cfg),
+        "lfg_batch_cfg*": C.POINTER(lfg_batch_cfg),
     }
     t = t.replace(" *", "*")
     if t in table:

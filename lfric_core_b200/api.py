@@ -11,6 +11,7 @@ Each class owns one ABI handle and mirrors a reference type:
   Preconditioner     abstract_preconditioner_type (solver/sci_preconditioner_mod.f90)
   IterativeSolver    abstract_iterative_solver_type and its solvers
                      (solver/sci_iterative_solver_mod.f90)
+  BatchedHelmholtz   many independent Helmholtz solves in one persistent launch
 
 Errors come back as LfgError carrying the ABI status; the solver's
 NOT_CONVERGED / NAN statuses are returned, not raised, as the reference's
@@ -24,7 +25,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import _lib
-from ._lib import lfg_solver_cfg
+from ._lib import lfg_batch_cfg, lfg_solver_cfg
 
 R_SINGLE, R_DOUBLE = 4, 8
 OK, NOT_CONVERGED, NAN_STATUS = 0, 1, 2
@@ -108,9 +109,11 @@ class _Handle:
         self.ctx, self.h, self._keep = ctx, h, list(keep)
 
     def close(self):
-        if getattr(self, "h", None) and self._destroy:
+        # after the context is gone its objects may not be touched (their
+        # memory went with the device context); drop the handle only
+        if getattr(self, "h", None) and self._destroy and getattr(self.ctx, "h", None):
             getattr(self.ctx.lib, self._destroy)(self.h)
-            self.h = None
+        self.h = None
 
     def __del__(self):
         try:
@@ -471,6 +474,97 @@ class MixedSolver(_Handle):
         if st not in (OK, NOT_CONVERGED, NAN_STATUS):
             self.ctx.check(st, "mixed_apply")
         return MixedResult(st, o.value, i.value, r.value)
+
+
+@dataclass
+class BatchResult:
+    status: int
+    outer_iterations: int
+    inner_iterations: int
+    rel_residual: float
+
+
+class BatchedHelmholtz(_Handle):
+    """Independent problems A_i x_i = b_i (r_double Helmholtz operators,
+    shared or not) solved together by lfg_batch_*: one persistent launch,
+    mixed refinement with an inner column-preconditioned FP32 CG."""
+
+    _destroy = "lfg_batch_destroy"
+
+    def __init__(self, ctx: Context, ops: list, tol=1e-8, inner_tol=1e-5, max_outer=10,
+                 max_inner=200, tile_cols=0, blocks_per_sm=0, use_graph=True, spin_limit=0):
+        if not ops or any(o.kind != R_DOUBLE for o in ops):
+            raise ValueError("BatchedHelmholtz: needs r_double Helmholtz operators")
+        cfg = lfg_batch_cfg(tol, inner_tol, max_outer, max_inner, tile_cols, blocks_per_sm,
+                            int(bool(use_graph)), spin_limit)
+        arr = (C.c_void_p * len(ops))(*[o.h.value if isinstance(o.h, C.c_void_p) else o.h
+                                        for o in ops])
+        h = C.c_void_p()
+        ctx.check(ctx.lib.lfg_batch_create(ctx.h, len(ops), arr, C.byref(cfg), C.byref(h)),
+                  "batch_create")
+        super().__init__(ctx, h, list(ops))
+        self.ops = list(ops)
+
+    class _Views:
+        """Field views of every problem's rhs or solution; each view keeps
+        the batch alive (the batch holds no reference back)."""
+
+        def __init__(self, batch, fn):
+            self.batch, self.fn = batch, fn
+
+        def __len__(self):
+            return len(self.batch.ops)
+
+        def __getitem__(self, i) -> Field:
+            B = self.batch
+            if not 0 <= i < len(B.ops):
+                raise IndexError(i)
+            v = C.c_void_p()
+            B.ctx.check(getattr(B.ctx.lib, self.fn)(B.h, i, C.byref(v)), self.fn)
+            p = C.c_void_p()
+            B.ctx.check(B.ctx.lib.lfg_field_device_ptr(v, C.byref(p)))
+            o = B.ops[i]
+            return Field(B.ctx, R_DOUBLE, o.ncol, o.nlayers, device_ptr=p.value, keep=[B])
+
+    @property
+    def rhs(self) -> "_Views":
+        return BatchedHelmholtz._Views(self, "lfg_batch_rhs")
+
+    @property
+    def sol(self) -> "_Views":
+        return BatchedHelmholtz._Views(self, "lfg_batch_solution")
+
+    def __len__(self):
+        return len(self.ops)
+
+    def launch(self):
+        self.ctx.check(self.ctx.lib.lfg_batch_launch(self.h), "batch_launch")
+
+    def wait(self) -> int:
+        nf = C.c_int()
+        self.ctx.check(self.ctx.lib.lfg_batch_wait(self.h, C.byref(nf)), "batch_wait")
+        return nf.value
+
+    def solve(self) -> int:
+        """Solve every problem from x = 0; returns how many did not reach tol."""
+        nf = C.c_int()
+        self.ctx.check(self.ctx.lib.lfg_batch_solve(self.h, C.byref(nf)), "batch_solve")
+        return nf.value
+
+    def result(self, i: int) -> BatchResult:
+        st, o, n, r = C.c_int(), C.c_int(), C.c_int(), C.c_double()
+        self.ctx.check(self.ctx.lib.lfg_batch_result(self.h, i, C.byref(st), C.byref(o),
+                                                     C.byref(n), C.byref(r)), "batch_result")
+        return BatchResult(st.value, o.value, n.value, r.value)
+
+    def tuning(self) -> dict:
+        v = [C.c_int() for _ in range(4)]
+        self.ctx.check(self.ctx.lib.lfg_batch_tuning(self.h, *[C.byref(x) for x in v]))
+        return dict(zip(("tile_cols", "blocks_per_sm", "grid_blocks", "phases"),
+                        (x.value for x in v)))
+
+    def test_stall(self, extra: int):
+        self.ctx.check(self.ctx.lib.lfg_batch_test_stall(self.h, extra), "batch_test_stall")
 
 
 class HelmholtzSystem:

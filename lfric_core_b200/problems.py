@@ -142,6 +142,43 @@ def helmholtz_problem(n: int, nlayers: int, seed: int, mg_levels: int = 4,
                             mg_links=mg_links, mg_child=mg_child)
 
 
+@dataclass
+class BatchWorkload:
+    """Independent W3 Helmholtz problems: operators[j] and, per problem i,
+    the index of its operator and its right-hand side (reference layout)."""
+
+    operators: list
+    problem_op: list
+    rhs: list
+
+    @property
+    def ndof(self) -> int:
+        return sum(self.operators[j].ncol * self.operators[j].nlayers for j in self.problem_op)
+
+
+def batch_workload(seed: int = 5, n_rhs: int = 64, n_shared: int = 48, l_shared: int = 30,
+                   n_uneven: int = 32, n_range=(12, 96), l_range=(10, 70)) -> BatchWorkload:
+    """n_rhs seeded right-hand sides (seeds seed+i) on one C_{n_shared} x
+    l_shared operator, plus n_uneven independent problems with n and L drawn
+    uniformly from n_range and l_range (operator and rhs seeds seed+n_rhs+j)."""
+    ops = [helmholtz_problem(n_shared, l_shared, seed=seed, mg_levels=1)]
+    problem_op, rhs = [], []
+    nd = ops[0].ncol * l_shared
+    for i in range(n_rhs):
+        problem_op.append(0)
+        rhs.append(np.random.default_rng(seed + i).standard_normal(nd))
+    draw = np.random.default_rng(seed)
+    for j in range(n_uneven):
+        n = int(draw.integers(n_range[0], n_range[1] + 1))
+        nl = int(draw.integers(l_range[0], l_range[1] + 1))
+        s = seed + n_rhs + j
+        p = helmholtz_problem(n, nl, seed=s, mg_levels=1)
+        ops.append(p)
+        problem_op.append(len(ops) - 1)
+        rhs.append(p.rhs)
+    return BatchWorkload(ops, problem_op, rhs)
+
+
 def to_level_major(v: np.ndarray, ncol: int, nlayers: int) -> np.ndarray:
     """Reference column-contiguous field -> (level, column) layout."""
     return np.ascontiguousarray(np.asarray(v).reshape(ncol, nlayers).T).ravel()
