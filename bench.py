@@ -238,9 +238,13 @@ def main():
 
     # ---- mixed (headline, device-resident inputs)
     with ClockSampler(dev) as clk:
+        torch.cuda.nvtx.range_push("timed_mixed")
         ms_mixed, launches, res_m = timed(system.solve_mixed, args.steps)
+        torch.cuda.nvtx.range_pop()
     # ---- plain FP64 drop-in
+    torch.cuda.nvtx.range_push("timed_fp64")
     ms_fp64, launches64, res_64 = timed(system.solve_fp64, args.steps)
+    torch.cuda.nvtx.range_pop()
 
     # ---- e2e through the ABI with host buffers (pinned)
     b_host = torch.from_numpy(prob.rhs.astype(np.float64)).pin_memory()

@@ -62,6 +62,9 @@ __device__ __forceinline__ T helm_row(const HelmArgs<T>& A, size_t i, int k, T x
 // loads are all independent.
 constexpr int KC = 2;
 
+// Levels a thread keeps in registers in the segmented coarse-level sweep.
+constexpr int kSegLevels = 12;
+
 // (A x)(c,k) from values already in registers: the T' row (sub, diag,
 // super, in the columnwise_op_app order) then minus the four couplings.
 // has_m / has_p select the sub / super terms without a branch.
@@ -412,6 +415,155 @@ __global__ void k_convert(TO* __restrict__ y, const TI* __restrict__ x, size_t n
     y[i] = (TO)x[i];
 }
 
+// Whole sweep for meshes with few columns (the coarse multigrid levels),
+// where one thread per column leaves most of the GPU idle and every level of
+// the serial recurrences costs a memory latency.  S threads share a column,
+// each owning L = ceil(nl/S) consecutive levels (at most LMAX, kept in
+// registers), and the block has 128/S columns.  The right-hand side
+// r = b + H_off x_eff (x_eff = x_in, plus the parent's coarse value when PRO)
+// is formed in place, so the sweep is one kernel.  Both recurrences of the
+// substitution,
+//   d_k = (r_k - sub_k d_{k-1}) inv_k,   z_k = d_k - c'_k z_{k+1},
+// are affine in the carried value: each thread composes its segment's map,
+// an inclusive scan of the maps over the S segments (shuffles of width S)
+// gives every segment its incoming value, and each segment then replays
+// its levels with exactly the sequential formulas from that value.
+template <class T, bool XIN, bool PRO, int S>
+__global__ void __launch_bounds__(128) k_helm_sweep_seg(HelmArgs<T> A, const T* __restrict__ b,
+                                                        const T* __restrict__ xin,
+                                                        const int* __restrict__ parent,
+                                                        const T* __restrict__ xc, int ncoarse,
+                                                        T omega, T* __restrict__ xout) {
+  constexpr int LMAX = kSegLevels;
+  const int tid = threadIdx.x, j = tid % S;
+  const unsigned c = blockIdx.x * (128 / S) + tid / S;
+  const size_t N = A.ncol;
+  const int nl = A.nl;
+  const size_t plane = (size_t)nl * N;
+  const int L = (nl + S - 1) / S, k0 = j * L;
+  const int nmy = c < N ? max(0, min(L, nl - k0)) : 0;
+  int nb[4] = {0, 0, 0, 0}, pn[4] = {0, 0, 0, 0}, pc = 0;
+  if (XIN && nmy > 0) {
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+      nb[f] = A.links[f * N + c];
+      if (PRO) pn[f] = parent[nb[f]];
+    }
+  }
+  if (PRO && nmy > 0) pc = parent[c];
+  T d[LMAX], iv[LMAX], sb[LMAX];
+#pragma unroll
+  for (int u = 0; u < LMAX; ++u) {
+    if (u < nmy) {
+      const int k = k0 + u;
+      const size_t i = (size_t)k * N + c;
+      T rv = b[i];
+      if (XIN) {
+        T hs = (T)0;
+#pragma unroll
+        for (int f = 0; f < 4; ++f) {
+          T xn = xin[(size_t)k * N + nb[f]];
+          if (PRO) xn = xn + xc[(size_t)k * ncoarse + pn[f]];
+          hs = hs + A.h[f * plane + i] * xn;
+        }
+        rv = rv + hs;
+      }
+      d[u] = rv;
+      iv[u] = A.inv[i];
+      sb[u] = A.sub[i];
+    }
+  }
+  // forward: this segment's map d_out = D + M d_in
+  T D = (T)0, M = (T)1;
+#pragma unroll
+  for (int u = 0; u < LMAX; ++u)
+    if (u < nmy) {
+      D = (d[u] - sb[u] * D) * iv[u];
+      M = M * (-sb[u] * iv[u]);
+    }
+#pragma unroll
+  for (int off = 1; off < S; off <<= 1) {
+    const T Dp = __shfl_up_sync(0xffffffffu, D, off, S);
+    const T Mp = __shfl_up_sync(0xffffffffu, M, off, S);
+    if (j >= off) {
+      D = D + M * Dp;
+      M = M * Mp;
+    }
+  }
+  T dv = __shfl_up_sync(0xffffffffu, D, 1, S);
+  if (j == 0) dv = (T)0;
+#pragma unroll
+  for (int u = 0; u < LMAX; ++u)
+    if (u < nmy) {
+      dv = k0 + u == 0 ? iv[u] * d[u] : iv[u] * (d[u] - sb[u] * dv);
+      d[u] = dv;
+    }
+  // backward: z_in of a segment is z at the first level of the next one
+  T cc[LMAX];
+#pragma unroll
+  for (int u = 0; u < LMAX; ++u)
+    if (u < nmy) cc[u] = A.cp[(size_t)(k0 + u) * N + c];
+  T E = (T)0, Nn = (T)1;
+#pragma unroll
+  for (int u = LMAX - 1; u >= 0; --u)
+    if (u < nmy) {
+      E = d[u] - cc[u] * E;
+      Nn = Nn * (-cc[u]);
+    }
+#pragma unroll
+  for (int off = 1; off < S; off <<= 1) {
+    const T Ep = __shfl_down_sync(0xffffffffu, E, off, S);
+    const T Np = __shfl_down_sync(0xffffffffu, Nn, off, S);
+    if (j + off < S) {
+      E = E + Nn * Ep;
+      Nn = Nn * Np;
+    }
+  }
+  T z = __shfl_down_sync(0xffffffffu, E, 1, S);
+  if (j == S - 1) z = (T)0;
+  const T om1 = (T)1 - omega;
+#pragma unroll
+  for (int u = LMAX - 1; u >= 0; --u)
+    if (u < nmy) {
+      const int k = k0 + u;
+      const size_t i = (size_t)k * N + c;
+      z = k == nl - 1 ? d[u] : d[u] - cc[u] * z;
+      T v = omega * z;
+      if (XIN) {
+        T xs = xin[i];
+        if (PRO) xs = xs + xc[(size_t)k * ncoarse + pc];
+        v = v + om1 * xs;
+      }
+      xout[i] = v;
+    }
+}
+
+// Threads per column for the segmented sweep (0: use the per-column kernels):
+// enough threads to cover the GPU, and segments of at most kSegLevels.
+inline int seg_threads(lfg_ctx c, int ncol, int nl) {
+  const long want = 2L * c->num_sms * 128;
+  if ((long)ncol >= want) return 0;
+  int S = 1;
+  while ((long)ncol * S < want && S < 32) S *= 2;
+  while ((nl + S - 1) / S > kSegLevels && S < 32) S *= 2;
+  if ((nl + S - 1) / S > kSegLevels || S < 4) return 0;
+  return S;
+}
+
+template <class T, bool XIN, bool PRO>
+void launch_sweep_seg(lfg_ctx c, int S, HelmArgs<T> A, const T* b, const T* xin,
+                      const int* parent, const T* xc, int ncoarse, T omega, T* xout) {
+  const int cols = 128 / S;
+  const unsigned grid = (unsigned)((A.ncol + cols - 1) / cols);
+  switch (S) {
+    case 4: k_helm_sweep_seg<T, XIN, PRO, 4><<<grid, 128, 0, c->stream>>>(A, b, xin, parent, xc, ncoarse, omega, xout); break;
+    case 8: k_helm_sweep_seg<T, XIN, PRO, 8><<<grid, 128, 0, c->stream>>>(A, b, xin, parent, xc, ncoarse, omega, xout); break;
+    case 16: k_helm_sweep_seg<T, XIN, PRO, 16><<<grid, 128, 0, c->stream>>>(A, b, xin, parent, xc, ncoarse, omega, xout); break;
+    default: k_helm_sweep_seg<T, XIN, PRO, 32><<<grid, 128, 0, c->stream>>>(A, b, xin, parent, xc, ncoarse, omega, xout); break;
+  }
+  after_launch(c, "helm_sweep_seg");
+}
+
 template <class T, bool XIN, bool PRO>
 void launch_subst(lfg_ctx c, int ncol, int nl, const T* r, const T* sub, const T* inv,
                   const T* cp, const T* xin, const int* parent, const T* xc, int ncoarse,
@@ -444,6 +596,19 @@ void smooth_t(lfg_helm op, double omega, lfg_field x_in, lfg_field b, lfg_field 
   const T* sub = (const T*)op->sub;
   const T* inv = (const T*)op->inv;
   const T* cp = (const T*)op->cp;
+  if (const int S = seg_threads(c, op->ncol, op->nl)) {
+    const HelmArgs<T> A = args_of<T>(op);
+    if (!x_in)
+      launch_sweep_seg<T, false, false>(c, S, A, (const T*)b->d, nullptr, nullptr, nullptr, 0, om,
+                                        (T*)x_out->d);
+    else if (!ig)
+      launch_sweep_seg<T, true, false>(c, S, A, (const T*)b->d, (const T*)x_in->d, nullptr,
+                                       nullptr, 0, om, (T*)x_out->d);
+    else
+      launch_sweep_seg<T, true, true>(c, S, A, (const T*)b->d, (const T*)x_in->d, ig->parent,
+                                      (const T*)xc->d, ig->ncoarse, om, (T*)x_out->d);
+    return;
+  }
   if (!x_in) {
     launch_subst<T, false, false>(c, op->ncol, op->nl, (const T*)b->d, sub, inv, cp, nullptr,
                                   nullptr, nullptr, 0, om, (T*)x_out->d);
