@@ -210,7 +210,7 @@ __global__ void __launch_bounds__(256) k_helm_rhs(HelmArgs<T> A, const T* __rest
 //     parallelism: each sweep walks the column in blocks of SP levels and
 //     loads block b+1 (clamped addresses, no conditional loads) before it
 //     computes block b.
-constexpr int SP = 8;
+constexpr int SP = 16;
 
 template <class T, bool XIN, bool PRO>
 __global__ void __launch_bounds__(128) k_helm_subst(
