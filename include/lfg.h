@@ -6,7 +6,8 @@
  * crossing the ABI are plain host pointers with explicit sizes, except the
  * *_device_ptr / lfg_field_wrap entry points, which exchange raw CUDA device
  * pointers.  Index arrays are 0-based (the Fortran iso_c_binding shim
- * subtracts one).  A Fortran caller binds these with bind(C) interfaces; see
+ * subtracts one), except the CMA's indirection maps and column-banded
+ * dofmaps, which keep the reference's 1-based row and column numbers.  A Fortran caller binds these with bind(C) interfaces; see
  * INTEGRATION.md for the module that extends the reference's abstract types.
  *
  * Field layout.  A field is the set of dofs of one function space on an
@@ -140,6 +141,10 @@ int lfg_cma_create(lfg_ctx ctx, int kind, int ncol, int nrow, int ncolumn, int b
                    const int* indirection_to, const int* indirection_from,
                    const double* columnwise_matrix, lfg_cma* cma);
 int lfg_cma_destroy(lfg_cma cma);
+/* The bands in the reference layout columnwise_matrix(bandwidth, nrow, ncell)
+ * (columnwise_operator_mod.f90:411-413); lfg_cma_create takes the same
+ * layout (NULL: all zero). */
+int lfg_cma_get(lfg_cma cma, double* columnwise_matrix);
 /* lhs += A x (sci_columnwise_op_app_kernel_mod.F90:73-124). */
 int lfg_cma_apply(lfg_cma cma, lfg_field lhs, lfg_field x);
 /* lhs += A^T x: the adjoint of lfg_cma_apply (lhs on the from-space, x on
@@ -170,6 +175,30 @@ int lfg_tri_solve(lfg_field y, lfg_field x, lfg_field tri_0, lfg_field tri_plus,
 int lfg_tri_solve_noalloc(int kind, int ncol, int nlev, const void* x, const void* tri_0,
                           const void* tri_plus, const void* tri_minus, void* y,
                           void* stream);
+
+/* ------------------------------------------------- CMA assembly
+ * column_banded_dofmap(ndf, nlayers) is 1-based, df fastest: the row (or
+ * column) of dof df of layer k in the column matrix, (k-1)(ndof_interior +
+ * ndof_face) + df as columnwise_operator_type builds it
+ * (columnwise_operator_mod.f90:377-393).  The LMA's cells are the CMA's
+ * columns. */
+/* C = the LMA's element matrices placed in the bands
+ * (columnwise_op_asm_kernel_code, sci_columnwise_op_asm_kernel_mod.F90). */
+int lfg_cma_assemble(lfg_cma c, lfg_lma a, const int* column_banded_dofmap_to,
+                     const int* column_banded_dofmap_from);
+/* C += A B (columnwise_op_mul_kernel_code, sci_columnwise_op_mul_kernel_mod.F90). */
+int lfg_cma_multiply(lfg_cma c, lfg_cma a, lfg_cma b);
+/* C = alpha A + beta B (columnwise_op_scaledadd_kernel_code,
+ * sci_columnwise_op_scaledadd_kernel_mod.F90). */
+int lfg_cma_scaled_add(lfg_cma c, lfg_cma a, lfg_cma b, double alpha, double beta);
+/* C = per-cell Dh M2h^-1 Dh^T with M2h taken diagonal
+ * (columnwise_op_asm_diag_hmht_kernel_code,
+ * sci_columnwise_op_asm_diag_hmht_kernel_mod.F90); dh maps W2h -> W3. */
+int lfg_cma_assemble_diag_hmht(lfg_cma c, lfg_lma dh, lfg_lma m2h,
+                               const int* column_banded_dofmap);
+/* C = inverse of the lumped diagonal of M (columnwise_op_asm_m2v_lumped_inv_krnl_code,
+ * sci_columnwise_op_asm_m2v_lumped_inv_krnl_mod.F90). */
+int lfg_cma_assemble_m2v_lumped_inv(lfg_cma c, lfg_lma m, const int* column_banded_dofmap);
 
 /* ------------------------------------------------------------ LMA operators
  * operator_type local_stencil(ncell*nlayers, ndf_to, ndf_from) in Fortran

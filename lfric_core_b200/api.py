@@ -263,16 +263,54 @@ class ColumnwiseOperator(_Handle):
 
     def __init__(self, ctx: Context, kind: int, ncol: int, nrow: int, ncolumn: int, bandwidth: int,
                  alpha: int, beta: int, gamma_m: int, gamma_p: int, ind_to, ind_from,
-                 columnwise_matrix: np.ndarray):
+                 columnwise_matrix: np.ndarray | None = None):
         it = np.ascontiguousarray(ind_to, dtype=np.int32)
         iff = np.ascontiguousarray(ind_from, dtype=np.int32)
-        cm = np.ascontiguousarray(columnwise_matrix, dtype=np.float64).ravel()
         h = C.c_void_p()
+        cm = None
+        if columnwise_matrix is not None:
+            cm = np.ascontiguousarray(columnwise_matrix, dtype=np.float64).ravel()
         ctx.check(ctx.lib.lfg_cma_create(ctx.h, kind, ncol, nrow, ncolumn, bandwidth, alpha,
                                          beta, gamma_m, gamma_p, _iptr(it), _iptr(iff),
-                                         _dptr(cm), C.byref(h)), "cma_create")
+                                         None if cm is None else _dptr(cm), C.byref(h)),
+                  "cma_create")
         super().__init__(ctx, h)
         self.kind, self.ncol, self.nrow, self.ncolumn = kind, ncol, nrow, ncolumn
+        self.bandwidth = bandwidth
+        self.alpha, self.beta, self.gamma_m, self.gamma_p = alpha, beta, gamma_m, gamma_p
+
+    def get(self) -> np.ndarray:
+        """columnwise_matrix(bw, nrow, ncol) as a Fortran-ordered array."""
+        out = np.empty(self.bandwidth * self.nrow * self.ncol)
+        self.ctx.check(self.ctx.lib.lfg_cma_get(self.h, _dptr(out)), "cma_get")
+        return out.reshape((self.bandwidth, self.nrow, self.ncol), order="F")
+
+    # CMA assembly and algebra (components/science/source/kernel/columnwise_operators/)
+    def assemble(self, lma: "LocalOperator", cb_to, cb_from):
+        t = np.asfortranarray(cb_to, dtype=np.int32)
+        f = np.asfortranarray(cb_from, dtype=np.int32)
+        self.ctx.check(self.ctx.lib.lfg_cma_assemble(self.h, lma.h, _iptr(t.ravel(order="F")),
+                                                     _iptr(f.ravel(order="F"))), "cma_assemble")
+
+    def multiply(self, a: "ColumnwiseOperator", b: "ColumnwiseOperator"):     # C += A B
+        self.ctx.check(self.ctx.lib.lfg_cma_multiply(self.h, a.h, b.h), "cma_multiply")
+
+    def scaled_add(self, a: "ColumnwiseOperator", b: "ColumnwiseOperator", alpha: float,
+                   beta: float):                                                # C = aA + bB
+        self.ctx.check(self.ctx.lib.lfg_cma_scaled_add(self.h, a.h, b.h, alpha, beta),
+                       "cma_scaled_add")
+
+    def assemble_diag_hmht(self, dh: "LocalOperator", m2h: "LocalOperator", cb):
+        t = np.asfortranarray(cb, dtype=np.int32)
+        self.ctx.check(self.ctx.lib.lfg_cma_assemble_diag_hmht(self.h, dh.h, m2h.h,
+                                                               _iptr(t.ravel(order="F"))),
+                       "cma_assemble_diag_hmht")
+
+    def assemble_m2v_lumped_inv(self, m: "LocalOperator", cb):
+        t = np.asfortranarray(cb, dtype=np.int32)
+        self.ctx.check(self.ctx.lib.lfg_cma_assemble_m2v_lumped_inv(self.h, m.h,
+                                                                    _iptr(t.ravel(order="F"))),
+                       "cma_assemble_m2v_lumped_inv")
 
     def apply(self, lhs: Field, x: Field):           # lhs += A x
         self.ctx.check(self.ctx.lib.lfg_cma_apply(self.h, lhs.h, x.h), "cma_apply")

@@ -359,7 +359,7 @@ int lfg_cma_create(lfg_ctx c, int kind, int ncol, int nrow, int ncolumn, int bw,
   return guard(c, [&] {
     LFG_REQUIRE(kind == LFG_R_DOUBLE || kind == LFG_R_SINGLE, "cma_create: bad kind");
     LFG_REQUIRE(ncol > 0 && nrow > 0 && ncolumn > 0 && bw > 0 && beta > 0 && ind_to &&
-                    ind_from && cm,
+                    ind_from,
                 "cma_create: bad arguments");
     std::vector<int> it(nrow), iff(ncolumn), jm(nrow), jp(nrow);
     for (int i = 0; i < nrow; ++i) {
@@ -398,7 +398,7 @@ int lfg_cma_create(lfg_ctx c, int kind, int ncol, int nrow, int ncolumn, int bw,
     for (int col = 0; col < ncol; ++col)
       for (int i = 0; i < nrow; ++i)
         for (int b = 0; b < bw; ++b)
-          dev[((size_t)b * nrow + i) * ncol + col] = cm[((size_t)col * nrow + i) * bw + b];
+          dev[((size_t)b * nrow + i) * ncol + col] = cm ? cm[((size_t)col * nrow + i) * bw + b] : 0.0;
     try {
       m->bands = dmalloc(n * kind);
       if (kind == LFG_R_DOUBLE) upload(m->bands, dev.data(), n * sizeof(double));

@@ -1,0 +1,376 @@
+// Columnwise (CMA) operator assembly on the device: the kernels that build
+// the banded column matrices from LMA element matrices and combine them.
+//
+//   lfg_cma_assemble            columnwise_op_asm_kernel_code
+//                               (sci_columnwise_op_asm_kernel_mod.F90)
+//   lfg_cma_multiply            columnwise_op_mul_kernel_code          C += A B
+//   lfg_cma_scaled_add          columnwise_op_scaledadd_kernel_code    C = a A + b B
+//   lfg_cma_assemble_diag_hmht  columnwise_op_asm_diag_hmht_kernel_code
+//                               C = diag-weighted D M2h^{-1} D^T per cell
+//   lfg_cma_assemble_m2v_lumped_inv
+//                               columnwise_op_asm_m2v_lumped_inv_krnl_code
+//
+// Layout: bands [bw][nrow][ncol] and LMA values [df_to][df_from][layer][cell]
+// (level-major, one thread per column or per (row, column), so a warp
+// touches 32 consecutive columns).  Every column is written by one thread
+// in the reference's loop order, so sums keep the reference's order.
+// column_banded_dofmap(df, k) is the 1-based row (or column) of dof df of
+// layer k within the column matrix, as columnwise_operator_type builds it
+// (infrastructure/source/operator/columnwise_operator_mod.f90:377-393).
+#include <cuda_runtime.h>
+
+#include <vector>
+
+#include "lfg_internal.cuh"
+
+namespace {
+
+using namespace lfg;
+
+template <class F>
+void dispatch_kind(int kind, F&& f) {
+  if (kind == LFG_R_DOUBLE) f(double{});
+  else f(float{});
+}
+
+// columnwise_op_asm_kernel_code: zero the column, then for every layer k,
+// to-dof df1 and from-dof df2 add local_stencil(ik, df1, df2) at row
+// i = cb_to(df1, k), band j - j_minus(i) with j = cb_from(df2, k).
+template <class T, class TL>
+__global__ void k_cma_asm(T* __restrict__ bands, const int* __restrict__ jminus, int ncol,
+                          int nrow, int bw, const TL* __restrict__ a, int ndf_to, int ndf_from,
+                          int nl, const int* __restrict__ cb_to, const int* __restrict__ cb_from) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncol) return;
+  const size_t plane = (size_t)nrow * ncol;
+  for (int b = 0; b < bw; ++b)
+    for (int i = 0; i < nrow; ++i) bands[b * plane + (size_t)i * ncol + c] = (T)0;
+  for (int k = 0; k < nl; ++k)
+    for (int d1 = 0; d1 < ndf_to; ++d1) {
+      const int i = cb_to[k * ndf_to + d1] - 1;
+      const int jm = jminus[i];
+      for (int d2 = 0; d2 < ndf_from; ++d2) {
+        const int b = cb_from[k * ndf_from + d2] - 1 - jm;
+        const size_t o = b * plane + (size_t)i * ncol + c;
+        bands[o] = bands[o] + (T)a[(((size_t)d1 * ndf_from + d2) * nl + k) * ncol + c];
+      }
+    }
+}
+
+// columnwise_op_mul_kernel_code, one thread per (row i of C, column):
+// C(j, i) += sum over ell in A's band of row i of A(ell, i) B(j, ell), for
+// the ell whose B band reaches j.
+template <class T>
+__global__ void k_cma_mul(T* __restrict__ cb, const int* __restrict__ jmC,
+                          const int* __restrict__ jpC, int ncolC, int bwC,
+                          const T* __restrict__ ab, const int* __restrict__ jmA,
+                          const int* __restrict__ jpA, int ncolA,
+                          const T* __restrict__ bb, const int* __restrict__ jmB,
+                          const int* __restrict__ jpB, int nrowA, int nrowB, int ncol) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y;
+  if (c >= ncol) return;
+  const int j0 = max(0, jmC[i]), j1 = min(ncolC - 1, jpC[i]);
+  const int l0 = max(0, jmA[i]), l1 = min(ncolA - 1, jpA[i]);
+  for (int j = j0; j <= j1; ++j) {
+    T e = (T)0;
+    for (int l = l0; l <= l1; ++l) {
+      if (jmB[l] <= j && j <= jpB[l])
+        e = e + ab[((size_t)(l - jmA[i]) * nrowA + i) * ncol + c] *
+                    bb[((size_t)(j - jmB[l]) * nrowB + l) * ncol + c];
+    }
+    const size_t o = ((size_t)(j - jmC[i]) * gridDim.y + i) * ncol + c;
+    cb[o] = cb[o] + e;
+  }
+  (void)bwC;
+}
+
+// columnwise_op_scaledadd_kernel_code, one thread per (row i of C, column):
+// the row is zeroed, then a A(j, i) added over A's band and b B(j, i) over
+// B's band (both clipped to A's column count, as in the reference).
+template <class T>
+__global__ void k_cma_scaledadd(T* __restrict__ cb, const int* __restrict__ jmC, int nrowC,
+                                int bwC, const T* __restrict__ ab, const int* __restrict__ jmA,
+                                const int* __restrict__ jpA, int nrowA, int ncolA,
+                                const T* __restrict__ bb, const int* __restrict__ jmB,
+                                const int* __restrict__ jpB, int nrowB, int ncol, T alpha,
+                                T beta) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y;
+  if (c >= ncol) return;
+  for (int b = 0; b < bwC; ++b) cb[((size_t)b * nrowC + i) * ncol + c] = (T)0;
+  if (i >= nrowA) return;
+  for (int j = max(0, jmA[i]); j <= min(ncolA - 1, jpA[i]); ++j) {
+    const size_t o = ((size_t)(j - jmC[i]) * nrowC + i) * ncol + c;
+    cb[o] = cb[o] + alpha * ab[((size_t)(j - jmA[i]) * nrowA + i) * ncol + c];
+  }
+  for (int j = max(0, jmB[i]); j <= min(ncolA - 1, jpB[i]); ++j) {
+    const size_t o = ((size_t)(j - jmC[i]) * nrowC + i) * ncol + c;
+    cb[o] = cb[o] + beta * bb[((size_t)(j - jmB[i]) * nrowB + i) * ncol + c];
+  }
+}
+
+// columnwise_op_asm_diag_hmht_kernel_code: per layer, the W3 x W3 block
+// sum_df3 Dh(df1,df3) Dh(df2,df3) / M2h(df3,df3), placed like the asm kernel.
+template <class T, class TL>
+__global__ void k_cma_asm_hmht(T* __restrict__ bands, const int* __restrict__ jminus, int ncol,
+                               int nrow, int bw, const TL* __restrict__ dh,
+                               const TL* __restrict__ m2h, int ndf3, int ndf2h, int nl,
+                               const int* __restrict__ cbm) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncol) return;
+  const size_t plane = (size_t)nrow * ncol;
+  for (int b = 0; b < bw; ++b)
+    for (int i = 0; i < nrow; ++i) bands[b * plane + (size_t)i * ncol + c] = (T)0;
+  auto D = [&](int d1, int d3, int k) {
+    return dh[(((size_t)d1 * ndf2h + d3) * nl + k) * ncol + c];
+  };
+  for (int k = 0; k < nl; ++k)
+    for (int d1 = 0; d1 < ndf3; ++d1) {
+      const int i = cbm[k * ndf3 + d1] - 1;
+      const int jm = jminus[i];
+      for (int d2 = 0; d2 < ndf3; ++d2) {
+        TL tmp = (TL)0;
+        for (int d3 = 0; d3 < ndf2h; ++d3)
+          tmp = tmp + D(d1, d3, k) * D(d2, d3, k) /
+                          m2h[(((size_t)d3 * ndf2h + d3) * nl + k) * ncol + c];
+        const int b = cbm[k * ndf3 + d2] - 1 - jm;
+        const size_t o = b * plane + (size_t)i * ncol + c;
+        bands[o] = bands[o] + (T)tmp;
+      }
+    }
+}
+
+// columnwise_op_asm_m2v_lumped_inv_krnl_code: band 1 of row cb(df, k)
+// accumulates M(df, df); then every non-zero entry of the column is inverted.
+template <class T, class TL>
+__global__ void k_cma_asm_m2v(T* __restrict__ bands, int ncol, int nrow, int bw,
+                              const TL* __restrict__ m, int ndf, int nl,
+                              const int* __restrict__ cbm) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncol) return;
+  const size_t plane = (size_t)nrow * ncol;
+  for (int b = 0; b < bw; ++b)
+    for (int i = 0; i < nrow; ++i) bands[b * plane + (size_t)i * ncol + c] = (T)0;
+  for (int k = 0; k < nl; ++k)
+    for (int d = 0; d < ndf; ++d) {
+      const int i = cbm[k * ndf + d] - 1;
+      const size_t o = (size_t)i * ncol + c;
+      bands[o] = bands[o] + (T)m[(((size_t)d * ndf + d) * nl + k) * ncol + c];
+    }
+  for (int b = 0; b < bw; ++b)
+    for (int i = 0; i < nrow; ++i) {
+      const size_t o = b * plane + (size_t)i * ncol + c;
+      if (bands[o] != (T)0) bands[o] = (T)1 / bands[o];
+    }
+}
+
+// Host copy of the per-row band limits (0-based first / last column).
+std::vector<int> host_ints(const int* d, int n) {
+  std::vector<int> h(n);
+  LFG_CUDA(cudaMemcpy(h.data(), d, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  return h;
+}
+
+// Checks a column-banded dofmap (ndf x nl, 1-based) against the matrix it
+// indexes: rows within [1, nrow]; with to/from maps, every entry lands
+// inside the band of its row.  Returns a device copy (caller frees).
+int* checked_dofmap(const int* cb, int ndf, int nl, int nmax, const char* what) {
+  LFG_REQUIRE(cb && ndf > 0 && nl > 0, std::string(what) + ": missing column-banded dofmap");
+  for (int e = 0; e < ndf * nl; ++e)
+    LFG_REQUIRE(cb[e] >= 1 && cb[e] <= nmax,
+                std::string(what) + ": column-banded dofmap entry out of range");
+  int* d = (int*)dmalloc(sizeof(int) * ndf * nl);
+  upload(d, cb, sizeof(int) * ndf * nl);
+  return d;
+}
+
+void check_bands(lfg_cma m, const int* cb_to, int ndf_to, const int* cb_from, int ndf_from,
+                 int nl, const char* what) {
+  const std::vector<int> jm = host_ints(m->jminus, m->nrow);
+  for (int k = 0; k < nl; ++k)
+    for (int d1 = 0; d1 < ndf_to; ++d1) {
+      const int i = cb_to[k * ndf_to + d1] - 1;
+      for (int d2 = 0; d2 < ndf_from; ++d2) {
+        const int b = cb_from[k * ndf_from + d2] - 1 - jm[i];
+        LFG_REQUIRE(b >= 0 && b < m->bw, std::string(what) +
+                                             ": a dof pair falls outside the band of its row");
+      }
+    }
+}
+
+struct DevInts {
+  int* p = nullptr;
+  ~DevInts() { dfree(p); }
+};
+
+}  // namespace
+
+extern "C" {
+
+int lfg_cma_get(lfg_cma m, double* cm) {
+  if (!m || !cm) return LFG_ERR_ARG;
+  lfg_ctx c = m->ctx;
+  return guard(c, [&] {
+    const size_t n = (size_t)m->bw * m->nrow * m->ncol;
+    std::vector<double> dev(n);
+    LFG_CUDA(cudaStreamSynchronize(c->stream));
+    if (m->kind == LFG_R_DOUBLE) {
+      LFG_CUDA(cudaMemcpy(dev.data(), m->bands, n * sizeof(double), cudaMemcpyDeviceToHost));
+    } else {
+      std::vector<float> f(n);
+      LFG_CUDA(cudaMemcpy(f.data(), m->bands, n * sizeof(float), cudaMemcpyDeviceToHost));
+      for (size_t e = 0; e < n; ++e) dev[e] = f[e];
+    }
+    for (int col = 0; col < m->ncol; ++col)
+      for (int i = 0; i < m->nrow; ++i)
+        for (int b = 0; b < m->bw; ++b)
+          cm[((size_t)col * m->nrow + i) * m->bw + b] =
+              dev[((size_t)b * m->nrow + i) * m->ncol + col];
+  });
+}
+
+int lfg_cma_assemble(lfg_cma m, lfg_lma a, const int* cb_to, const int* cb_from) {
+  if (!m || !a) return LFG_ERR_ARG;
+  lfg_ctx c = m->ctx;
+  return guard(c, [&] {
+    LFG_REQUIRE(a->ctx == c && a->ncell == m->ncol, "cma_assemble: LMA and CMA cell counts differ");
+    DevInts dto, dfrom;
+    dto.p = checked_dofmap(cb_to, a->ndf_to, a->nl, m->nrow, "cma_assemble");
+    dfrom.p = checked_dofmap(cb_from, a->ndf_from, a->nl, m->ncolumn, "cma_assemble");
+    check_bands(m, cb_to, a->ndf_to, cb_from, a->ndf_from, a->nl, "cma_assemble");
+    const int grid = (m->ncol + 127) / 128;
+    dispatch_kind(m->kind, [&](auto t) {
+      using T = decltype(t);
+      dispatch_kind(a->kind, [&](auto tl) {
+        using TL = decltype(tl);
+        k_cma_asm<T, TL><<<grid, 128, 0, c->stream>>>((T*)m->bands, m->jminus, m->ncol, m->nrow,
+                                                      m->bw, (const TL*)a->a, a->ndf_to,
+                                                      a->ndf_from, a->nl, dto.p, dfrom.p);
+      });
+    });
+    after_launch(c, "cma_asm");
+    LFG_CUDA(cudaStreamSynchronize(c->stream));  // the dofmap copies are freed on return
+  });
+}
+
+int lfg_cma_multiply(lfg_cma C, lfg_cma A, lfg_cma B) {
+  if (!C || !A || !B) return LFG_ERR_ARG;
+  lfg_ctx c = C->ctx;
+  return guard(c, [&] {
+    LFG_REQUIRE(A->ctx == c && B->ctx == c, "cma_multiply: operators of another context");
+    LFG_REQUIRE(A->kind == C->kind && B->kind == C->kind, "cma_multiply: kinds differ");
+    LFG_REQUIRE(A->ncol == C->ncol && B->ncol == C->ncol, "cma_multiply: cell counts differ");
+    LFG_REQUIRE(A->nrow == C->nrow && A->ncolumn == B->nrow && B->ncolumn == C->ncolumn,
+                "cma_multiply: shapes do not chain (C nrow x ncol = A nrow x B ncol)");
+    // every product entry must have a slot in C's band
+    {
+      const auto jmA = host_ints(A->jminus, A->nrow), jpA = host_ints(A->jplus, A->nrow);
+      const auto jmB = host_ints(B->jminus, B->nrow), jpB = host_ints(B->jplus, B->nrow);
+      const auto jmC = host_ints(C->jminus, C->nrow), jpC = host_ints(C->jplus, C->nrow);
+      for (int i = 0; i < C->nrow; ++i) {
+        LFG_REQUIRE(jpC[i] - jmC[i] + 1 <= C->bw, "cma_multiply: C band too narrow");
+        for (int l = std::max(0, jmA[i]); l <= std::min(A->ncolumn - 1, jpA[i]); ++l)
+          for (int j = std::max(jmB[l], std::max(0, jmC[i]));
+               j <= std::min(jpB[l], std::min(C->ncolumn - 1, jpC[i])); ++j)
+            LFG_REQUIRE(j - jmC[i] >= 0 && j - jmC[i] < C->bw, "cma_multiply: band overflow");
+      }
+    }
+    dim3 grid((C->ncol + 127) / 128, C->nrow);
+    dispatch_kind(C->kind, [&](auto t) {
+      using T = decltype(t);
+      k_cma_mul<T><<<grid, 128, 0, c->stream>>>(
+          (T*)C->bands, C->jminus, C->jplus, C->ncolumn, C->bw, (const T*)A->bands, A->jminus,
+          A->jplus, A->ncolumn, (const T*)B->bands, B->jminus, B->jplus, A->nrow, B->nrow,
+          C->ncol);
+    });
+    after_launch(c, "cma_mul");
+  });
+}
+
+int lfg_cma_scaled_add(lfg_cma C, lfg_cma A, lfg_cma B, double alpha, double beta) {
+  if (!C || !A || !B) return LFG_ERR_ARG;
+  lfg_ctx c = C->ctx;
+  return guard(c, [&] {
+    LFG_REQUIRE(A->ctx == c && B->ctx == c, "cma_scaled_add: operators of another context");
+    LFG_REQUIRE(A->kind == C->kind && B->kind == C->kind, "cma_scaled_add: kinds differ");
+    LFG_REQUIRE(A->ncol == C->ncol && B->ncol == C->ncol, "cma_scaled_add: cell counts differ");
+    LFG_REQUIRE(A->nrow <= C->nrow && A->nrow <= B->nrow,
+                "cma_scaled_add: C and B need at least A's rows");
+    {
+      const auto jmA = host_ints(A->jminus, A->nrow), jpA = host_ints(A->jplus, A->nrow);
+      const auto jmB = host_ints(B->jminus, B->nrow), jpB = host_ints(B->jplus, B->nrow);
+      const auto jmC = host_ints(C->jminus, C->nrow);
+      for (int i = 0; i < A->nrow; ++i) {
+        for (int j = std::max(0, jmA[i]); j <= std::min(A->ncolumn - 1, jpA[i]); ++j)
+          LFG_REQUIRE(j - jmC[i] >= 0 && j - jmC[i] < C->bw, "cma_scaled_add: A outside C's band");
+        for (int j = std::max(0, jmB[i]); j <= std::min(A->ncolumn - 1, jpB[i]); ++j) {
+          LFG_REQUIRE(j - jmC[i] >= 0 && j - jmC[i] < C->bw, "cma_scaled_add: B outside C's band");
+          LFG_REQUIRE(j - jmB[i] < B->bw, "cma_scaled_add: B band too narrow");
+        }
+      }
+    }
+    dim3 grid((C->ncol + 127) / 128, C->nrow);
+    dispatch_kind(C->kind, [&](auto t) {
+      using T = decltype(t);
+      k_cma_scaledadd<T><<<grid, 128, 0, c->stream>>>(
+          (T*)C->bands, C->jminus, C->nrow, C->bw, (const T*)A->bands, A->jminus, A->jplus,
+          A->nrow, A->ncolumn, (const T*)B->bands, B->jminus, B->jplus, B->nrow, C->ncol,
+          (T)alpha, (T)beta);
+    });
+    after_launch(c, "cma_scaledadd");
+  });
+}
+
+int lfg_cma_assemble_diag_hmht(lfg_cma m, lfg_lma dh, lfg_lma m2h, const int* cbm) {
+  if (!m || !dh || !m2h) return LFG_ERR_ARG;
+  lfg_ctx c = m->ctx;
+  return guard(c, [&] {
+    LFG_REQUIRE(dh->ctx == c && m2h->ctx == c, "cma_assemble_diag_hmht: another context");
+    LFG_REQUIRE(dh->ncell == m->ncol && m2h->ncell == m->ncol && dh->nl == m2h->nl,
+                "cma_assemble_diag_hmht: cell or layer counts differ");
+    LFG_REQUIRE(dh->ndf_from == m2h->ndf_to && m2h->ndf_to == m2h->ndf_from,
+                "cma_assemble_diag_hmht: Dh must map W2h -> W3 and M2h be W2h x W2h");
+    LFG_REQUIRE(dh->kind == m2h->kind, "cma_assemble_diag_hmht: LMA kinds differ");
+    DevInts d;
+    d.p = checked_dofmap(cbm, dh->ndf_to, dh->nl, m->nrow, "cma_assemble_diag_hmht");
+    check_bands(m, cbm, dh->ndf_to, cbm, dh->ndf_to, dh->nl, "cma_assemble_diag_hmht");
+    const int grid = (m->ncol + 127) / 128;
+    dispatch_kind(m->kind, [&](auto t) {
+      using T = decltype(t);
+      dispatch_kind(dh->kind, [&](auto tl) {
+        using TL = decltype(tl);
+        k_cma_asm_hmht<T, TL><<<grid, 128, 0, c->stream>>>(
+            (T*)m->bands, m->jminus, m->ncol, m->nrow, m->bw, (const TL*)dh->a,
+            (const TL*)m2h->a, dh->ndf_to, dh->ndf_from, dh->nl, d.p);
+      });
+    });
+    after_launch(c, "cma_asm_diag_hmht");
+    LFG_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+int lfg_cma_assemble_m2v_lumped_inv(lfg_cma m, lfg_lma mm, const int* cbm) {
+  if (!m || !mm) return LFG_ERR_ARG;
+  lfg_ctx c = m->ctx;
+  return guard(c, [&] {
+    LFG_REQUIRE(mm->ctx == c && mm->ncell == m->ncol && mm->ndf_to == mm->ndf_from,
+                "cma_assemble_m2v_lumped_inv: LMA must be square with the CMA's cells");
+    DevInts d;
+    d.p = checked_dofmap(cbm, mm->ndf_to, mm->nl, m->nrow, "cma_assemble_m2v_lumped_inv");
+    const int grid = (m->ncol + 127) / 128;
+    dispatch_kind(m->kind, [&](auto t) {
+      using T = decltype(t);
+      dispatch_kind(mm->kind, [&](auto tl) {
+        using TL = decltype(tl);
+        k_cma_asm_m2v<T, TL><<<grid, 128, 0, c->stream>>>((T*)m->bands, m->ncol, m->nrow, m->bw,
+                                                          (const TL*)mm->a, mm->ndf_to, mm->nl,
+                                                          d.p);
+      });
+    });
+    after_launch(c, "cma_asm_m2v_lumped_inv");
+    LFG_CUDA(cudaStreamSynchronize(c->stream));
+  });
+}
+
+}  // extern "C"

@@ -49,6 +49,27 @@ extern "C" {
                                            int gamma_m, int gamma_p, int ndf, int undf, \
                                            const int* map, const int* ind, T* c_prime,  \
                                            T* d_prime);                                 \
+  void ora_columnwise_op_asm_code_##SFX(int cell, int nlayers, int ncell_2d, int ncell_3d,\
+      const T* local_stencil, T* columnwise_matrix, int nrow, int ncol, int bandwidth,  \
+      int alpha, int beta, int gamma_m, int gamma_p, int ndf_to, const int* cbm_to,     \
+      int ndf_from, const int* cbm_from);                                               \
+  void ora_columnwise_op_mul_code_##SFX(int cell, int ncell_2d, const T* A, int nrow_A,  \
+      int ncol_A, int bw_A, int alpha_A, int beta_A, int gm_A, int gp_A, const T* B,    \
+      int nrow_B, int ncol_B, int bw_B, int alpha_B, int beta_B, int gm_B, int gp_B,    \
+      T* C, int nrow_C, int ncol_C, int bw_C, int alpha_C, int beta_C, int gm_C,        \
+      int gp_C);                                                                        \
+  void ora_columnwise_op_scaledadd_code_##SFX(int cell, int ncell_2d, const T* A,        \
+      int nrow_A, int ncol_A, int bw_A, int alpha_A, int beta_A, int gm_A, int gp_A,    \
+      const T* B, int nrow_B, int ncol_B, int bw_B, int alpha_B, int beta_B, int gm_B,  \
+      int gp_B, T* C, int nrow_C, int ncol_C, int bw_C, int alpha_C, int beta_C,        \
+      int gm_C, int gp_C, T alpha, T beta);                                             \
+  void ora_columnwise_op_asm_diag_hmht_code_##SFX(int cell, int nlayers, int ncell_2d,   \
+      int ncell_3d, const T* dh, const T* m2h, T* columnwise_matrix, int nrow,          \
+      int bandwidth, int alpha, int beta, int gamma_m, int gamma_p, int ndf_w3,         \
+      const int* cbm, int ndf_w2h);                                                     \
+  void ora_columnwise_op_asm_m2v_lumped_inv_code_##SFX(int cell, int nlayers,            \
+      int ncell_2d, int ncell_3d, const T* local_stencil, T* columnwise_matrix,         \
+      int nrow, int bandwidth, int ndf, const int* cbm);                                \
   void ora_tri_solve_code_##SFX(int nlayers, T* y, const T* x, const T* tri_0,          \
                                 const T* tri_plus, const T* tri_minus, int ndf,         \
                                 int undf, const int* map, T* x_new, T* tri_plus_new);   \

@@ -133,6 +133,165 @@ DEF_MM_DIAGONAL(float, r_single)
 DEF_CMA_APP(double, r_double)
 DEF_CMA_APP(float, r_single)
 
+/* CMA assembly and algebra (components/science/source/kernel/
+ * columnwise_operators/): the reference's per-cell loops with local_stencil
+ * (ncell_3d, ndf_to, ndf_from) and columnwise_matrix (bandwidth, nrow,
+ * ncell_2d) in Fortran order; j_minus / j_plus in the kind T as the
+ * reference evaluates them in r_solver. */
+#define ORA_JMINUS(T, a, i, gp, b) ((int)ceil((T)((a) * (i) - (gp)) / ((T)1 * (T)(b))))
+#define ORA_JPLUS(T, a, i, gm, b) ((int)floor((T)((a) * (i) + (gm)) / ((T)1 * (T)(b))))
+
+/* sci_columnwise_op_asm_kernel_mod.F90, columnwise_op_asm_kernel_code */
+#define DEF_CMA_ASM(T, SFX)                                                           \
+  void ora_columnwise_op_asm_code_##SFX(                                              \
+      int cell, int nlayers, int ncell_2d, int ncell_3d, const T* local_stencil,      \
+      T* columnwise_matrix, int nrow, int ncol, int bandwidth, int alpha, int beta,   \
+      int gamma_m, int gamma_p, int ndf_to, const int* cbm_to, int ndf_from,          \
+      const int* cbm_from) {                                                          \
+    (void)ncell_2d; (void)ncol; (void)gamma_m;                                        \
+    for (int i = 1; i <= nrow; ++i)                                                   \
+      for (int b = 1; b <= bandwidth; ++b)                                            \
+        A3(columnwise_matrix, b, i, cell, bandwidth, nrow) = (T)0;                    \
+    for (int k = 1; k <= nlayers; ++k) {                                              \
+      int ik = (cell - 1) * nlayers + k;                                              \
+      for (int df1 = 1; df1 <= ndf_to; ++df1) {                                       \
+        int i = A2(cbm_to, df1, k, ndf_to);                                           \
+        int j_minus = ORA_JMINUS(T, alpha, i, gamma_p, beta);                         \
+        for (int df2 = 1; df2 <= ndf_from; ++df2) {                                   \
+          int j = A2(cbm_from, df2, k, ndf_from);                                     \
+          A3(columnwise_matrix, j - j_minus + 1, i, cell, bandwidth, nrow) =          \
+              A3(columnwise_matrix, j - j_minus + 1, i, cell, bandwidth, nrow) +      \
+              A3(local_stencil, ik, df1, df2, ncell_3d, ndf_to);                      \
+        }                                                                             \
+      }                                                                               \
+    }                                                                                 \
+  }
+DEF_CMA_ASM(double, r_double)
+DEF_CMA_ASM(float, r_single)
+
+/* sci_columnwise_op_mul_kernel_mod.F90, columnwise_op_mul_kernel_code: C += A B */
+#define DEF_CMA_MUL(T, SFX)                                                           \
+  void ora_columnwise_op_mul_code_##SFX(                                              \
+      int cell, int ncell_2d, const T* A, int nrow_A, int ncol_A, int bw_A,           \
+      int alpha_A, int beta_A, int gm_A, int gp_A, const T* B, int nrow_B,            \
+      int ncol_B, int bw_B, int alpha_B, int beta_B, int gm_B, int gp_B, T* C,        \
+      int nrow_C, int ncol_C, int bw_C, int alpha_C, int beta_C, int gm_C,            \
+      int gp_C) {                                                                     \
+    (void)ncell_2d; (void)ncol_B;                                                     \
+    for (int i = 1; i <= nrow_C; ++i) {                                               \
+      int jmA = ORA_JMINUS(T, alpha_A, i, gp_A, beta_A);                              \
+      int jpA = ORA_JPLUS(T, alpha_A, i, gm_A, beta_A);                               \
+      int jmC = ORA_JMINUS(T, alpha_C, i, gp_C, beta_C);                              \
+      int jpC = ORA_JPLUS(T, alpha_C, i, gm_C, beta_C);                               \
+      for (int j = (jmC > 1 ? jmC : 1); j <= (jpC < ncol_C ? jpC : ncol_C); ++j) {     \
+        T e = (T)0;                                                                   \
+        for (int l = (jmA > 1 ? jmA : 1); l <= (jpA < ncol_A ? jpA : ncol_A); ++l) {   \
+          int jmB = ORA_JMINUS(T, alpha_B, l, gp_B, beta_B);                          \
+          int jpB = ORA_JPLUS(T, alpha_B, l, gm_B, beta_B);                           \
+          if (jmB <= j && j <= jpB)                                                   \
+            e = e + A3(A, l - jmA + 1, i, cell, bw_A, nrow_A) *                       \
+                        A3(B, j - jmB + 1, l, cell, bw_B, nrow_B);                    \
+        }                                                                             \
+        A3(C, j - jmC + 1, i, cell, bw_C, nrow_C) =                                   \
+            A3(C, j - jmC + 1, i, cell, bw_C, nrow_C) + e;                            \
+      }                                                                               \
+    }                                                                                 \
+  }
+DEF_CMA_MUL(double, r_double)
+DEF_CMA_MUL(float, r_single)
+
+/* sci_columnwise_op_scaledadd_kernel_mod.F90, columnwise_op_scaledadd_kernel_code:
+ * C = alpha A + beta B (B's loop is clipped to A's column count, as there). */
+#define DEF_CMA_SCALEDADD(T, SFX)                                                     \
+  void ora_columnwise_op_scaledadd_code_##SFX(                                        \
+      int cell, int ncell_2d, const T* A, int nrow_A, int ncol_A, int bw_A,           \
+      int alpha_A, int beta_A, int gm_A, int gp_A, const T* B, int nrow_B,            \
+      int ncol_B, int bw_B, int alpha_B, int beta_B, int gm_B, int gp_B, T* C,        \
+      int nrow_C, int ncol_C, int bw_C, int alpha_C, int beta_C, int gm_C,            \
+      int gp_C, T alpha, T beta) {                                                    \
+    (void)ncell_2d; (void)ncol_B; (void)ncol_C; (void)gm_C;                           \
+    for (int i = 1; i <= nrow_C; ++i)                                                 \
+      for (int b = 1; b <= bw_C; ++b) A3(C, b, i, cell, bw_C, nrow_C) = (T)0;         \
+    for (int i = 1; i <= nrow_A; ++i) {                                               \
+      int jmA = ORA_JMINUS(T, alpha_A, i, gp_A, beta_A);                              \
+      int jpA = ORA_JPLUS(T, alpha_A, i, gm_A, beta_A);                               \
+      int jmB = ORA_JMINUS(T, alpha_B, i, gp_B, beta_B);                              \
+      int jpB = ORA_JPLUS(T, alpha_B, i, gm_B, beta_B);                               \
+      int jmC = ORA_JMINUS(T, alpha_C, i, gp_C, beta_C);                              \
+      for (int j = (jmA > 1 ? jmA : 1); j <= (jpA < ncol_A ? jpA : ncol_A); ++j)       \
+        A3(C, j - jmC + 1, i, cell, bw_C, nrow_C) =                                   \
+            A3(C, j - jmC + 1, i, cell, bw_C, nrow_C) +                               \
+            alpha * A3(A, j - jmA + 1, i, cell, bw_A, nrow_A);                        \
+      for (int j = (jmB > 1 ? jmB : 1); j <= (jpB < ncol_A ? jpB : ncol_A); ++j)       \
+        A3(C, j - jmC + 1, i, cell, bw_C, nrow_C) =                                   \
+            A3(C, j - jmC + 1, i, cell, bw_C, nrow_C) +                               \
+            beta * A3(B, j - jmB + 1, i, cell, bw_B, nrow_B);                         \
+    }                                                                                 \
+  }
+DEF_CMA_SCALEDADD(double, r_double)
+DEF_CMA_SCALEDADD(float, r_single)
+
+/* sci_columnwise_op_asm_diag_hmht_kernel_mod.F90,
+ * columnwise_op_asm_diag_hmht_kernel_code */
+#define DEF_CMA_HMHT(T, SFX)                                                          \
+  void ora_columnwise_op_asm_diag_hmht_code_##SFX(                                    \
+      int cell, int nlayers, int ncell_2d, int ncell_3d, const T* dh,                 \
+      const T* m2h, T* columnwise_matrix, int nrow, int bandwidth, int alpha,         \
+      int beta, int gamma_m, int gamma_p, int ndf_w3, const int* cbm,                 \
+      int ndf_w2h) {                                                                  \
+    (void)ncell_2d; (void)gamma_m;                                                    \
+    for (int i = 1; i <= nrow; ++i)                                                   \
+      for (int b = 1; b <= bandwidth; ++b)                                            \
+        A3(columnwise_matrix, b, i, cell, bandwidth, nrow) = (T)0;                    \
+    for (int k = 1; k <= nlayers; ++k) {                                              \
+      int ik = (cell - 1) * nlayers + k;                                              \
+      for (int df1 = 1; df1 <= ndf_w3; ++df1) {                                       \
+        int i = A2(cbm, df1, k, ndf_w3);                                              \
+        int j_minus = ORA_JMINUS(T, alpha, i, gamma_p, beta);                         \
+        for (int df2 = 1; df2 <= ndf_w3; ++df2) {                                     \
+          T tmp = (T)0;                                                               \
+          for (int df3 = 1; df3 <= ndf_w2h; ++df3)                                    \
+            tmp = tmp + A3(dh, ik, df1, df3, ncell_3d, ndf_w3) *                      \
+                            A3(dh, ik, df2, df3, ncell_3d, ndf_w3) /                  \
+                            A3(m2h, ik, df3, df3, ncell_3d, ndf_w2h);                 \
+          int j = A2(cbm, df2, k, ndf_w3);                                            \
+          A3(columnwise_matrix, j - j_minus + 1, i, cell, bandwidth, nrow) =          \
+              A3(columnwise_matrix, j - j_minus + 1, i, cell, bandwidth, nrow) + tmp; \
+        }                                                                             \
+      }                                                                               \
+    }                                                                                 \
+  }
+DEF_CMA_HMHT(double, r_double)
+DEF_CMA_HMHT(float, r_single)
+
+/* sci_columnwise_op_asm_m2v_lumped_inv_krnl_mod.F90,
+ * columnwise_op_asm_m2v_lumped_inv_krnl_code */
+#define DEF_CMA_M2V(T, SFX)                                                           \
+  void ora_columnwise_op_asm_m2v_lumped_inv_code_##SFX(                               \
+      int cell, int nlayers, int ncell_2d, int ncell_3d, const T* local_stencil,      \
+      T* columnwise_matrix, int nrow, int bandwidth, int ndf, const int* cbm) {       \
+    (void)ncell_2d;                                                                   \
+    for (int i = 1; i <= nrow; ++i)                                                   \
+      for (int b = 1; b <= bandwidth; ++b)                                            \
+        A3(columnwise_matrix, b, i, cell, bandwidth, nrow) = (T)0;                    \
+    for (int k = 1; k <= nlayers; ++k) {                                              \
+      int ik = (cell - 1) * nlayers + k;                                              \
+      for (int df1 = 1; df1 <= ndf; ++df1) {                                          \
+        int i = A2(cbm, df1, k, ndf);                                                 \
+        A3(columnwise_matrix, 1, i, cell, bandwidth, nrow) =                          \
+            A3(columnwise_matrix, 1, i, cell, bandwidth, nrow) +                      \
+            A3(local_stencil, ik, df1, df1, ncell_3d, ndf);                           \
+      }                                                                               \
+    }                                                                                 \
+    for (int i = 1; i <= nrow; ++i)                                                   \
+      for (int b = 1; b <= bandwidth; ++b)                                            \
+        if (A3(columnwise_matrix, b, i, cell, bandwidth, nrow) != (T)0)               \
+          A3(columnwise_matrix, b, i, cell, bandwidth, nrow) =                        \
+              (T)1 / A3(columnwise_matrix, b, i, cell, bandwidth, nrow);              \
+  }
+DEF_CMA_M2V(double, r_double)
+DEF_CMA_M2V(float, r_single)
+
 /* components/science/source/kernel/columnwise_operators/sci_columnwise_op_appinv_kernel_mod.F90:77-145
  * Thomas algorithm; lhs is overwritten with the solution. */
 #define DEF_CMA_APPINV(T, SFX)                                                        \

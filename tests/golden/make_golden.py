@@ -180,6 +180,52 @@ def main(ref: Path) -> None:
         "tol": tol_literal(t),
     })
 
+    # ------------------------------------------- CMA assembly and algebra
+    cw = ref / UT / "columnwise_operators"
+
+    def scalar(text, name):
+        m = re.search(rf"\b{name}\s*=\s*([-+0-9.eE_a-z]+)", text)
+        return _eval_num(m.group(1))
+
+    asm = _source(cw / "columnwise_op_asm_kernel_mod_test.pf")
+    stencil = re.search(r"reshape\(\s*\(/(.*?)/\)", asm).group(1)
+    mul = _source(cw / "columnwise_op_mul_kernel_mod_test.pf")
+    sadd = _source(cw / "columnwise_op_scaledadd_kernel_mod_test.pf")
+    hm = _source(cw / "columnwise_op_asm_diag_hmht_kernel_mod_test.pf")
+    m2v = _source(cw / "columnwise_op_asm_m2v_lumped_inv_kernel_mod_test.pf")
+    m2v_stencil = re.search(r"reshape\(\s*\(/(.*?)/\)", m2v).group(1)
+    write("cma_assembly_kat.json", {
+        "source": [f"{UT}/columnwise_operators/columnwise_op_asm_kernel_mod_test.pf",
+                   f"{UT}/columnwise_operators/columnwise_op_mul_kernel_mod_test.pf",
+                   f"{UT}/columnwise_operators/columnwise_op_scaledadd_kernel_mod_test.pf",
+                   f"{UT}/columnwise_operators/columnwise_op_asm_diag_hmht_kernel_mod_test.pf",
+                   f"{UT}/columnwise_operators/columnwise_op_asm_m2v_lumped_inv_kernel_mod_test.pf",
+                   "components/science/unit-test/support/get_unit_test_m3x3_cma_data_mod.f90"],
+        "nlayers": int(scalar(asm, "nlayers")),
+        # columnwise_op_asm: Wtheta->Wtheta, every cell's 2x2 stencil (Fortran order)
+        "asm_stencil_fortran_order": [_eval_num(v) for v in stencil.split(",")],
+        "asm_first_row": [_eval_num("1.0_r_solver/3.0_r_solver"),
+                          _eval_num("1.0_r_solver/6.0_r_solver")],
+        "asm_interior_row": [_eval_num("1.0_r_solver/6.0_r_solver"),
+                             _eval_num("2.0_r_solver/3.0_r_solver"),
+                             _eval_num("1.0_r_solver/6.0_r_solver")],
+        "asm_last_row": [_eval_num("1.0_r_solver/6.0_r_solver"),
+                         _eval_num("1.0_r_solver/3.0_r_solver")],
+        # columnwise_op_mul: D (W3 <- Wtheta) bands (+1, -1), D^T bands (-1, +1)
+        "mul_D_bands": [1.0, -1.0], "mul_DT_bands": [-1.0, 1.0],
+        "mul_nlayers": int(scalar(mul, "nlayers")),
+        # columnwise_op_scaledadd: C = mu M + nu DTD, M = I (W3), DTD bands (1, 2, 1)
+        "scaledadd_mu": scalar(sadd, "mu"), "scaledadd_nu": scalar(sadd, "nu"),
+        "scaledadd_DTD_bands": [1.0, 2.0, 1.0],
+        # columnwise_op_asm_diag_hmht: Dh row (rho), diagonal M2h (sigma); answer sum rho^2/sigma
+        "hmht_rho": [scalar(hm, rf"rho\({i}\)") for i in range(1, 5)],
+        "hmht_sigma": [scalar(hm, rf"sigma\({i}\)") for i in range(1, 5)],
+        # columnwise_op_asm_m2v_lumped_inv: W2v 2x2 stencil; ends 3, interior 3/2
+        "m2v_stencil_fortran_order": [_eval_num(v) for v in m2v_stencil.split(",")],
+        "m2v_end_rows": 3.0, "m2v_interior_rows": 1.5,
+        "tol": tol_literal(asm),
+    })
+
     # ------------------------------------------------------- intergrid KATs
     im = ref / UT / "inter_mesh"
     kats = {}

@@ -194,3 +194,130 @@ def w0_transfer(direction: str, child, fine_corners, coarse_corners, src, nl, ds
             L.ora_prolong_w0_code(nl, _p(cmap), nx, ny, mf.shape[0], _p(out), _p(src), 8,
                                   out.size, _p(mf), src.size, _p(mcc))
     return out
+
+
+# ---------------------------------------------------------------- CMA assembly
+def _pF(a):
+    """Pointer to a Fortran-ordered array (through a 1-D view, so writes land
+    in the array)."""
+    v = a.ravel(order="F")
+    assert np.shares_memory(v, a)
+    return ptr(v)
+
+
+def cma_size(nlayers, ndf_to, ndf_from, nface_to, nint_to, nface_from, nint_from):
+    """The CMA parameters of a to-space / from-space pair, as
+    get_cma_size (components/science/unit-test/support/
+    get_unit_test_m3x3_cma_data_mod.f90:130-159) computes them."""
+    nrow = nlayers * nint_to + (nlayers + 1) * nface_to
+    ncol = nlayers * nint_from + (nlayers + 1) * nface_from
+    alpha = nface_from + nint_from
+    beta = nface_to + nint_to
+    g_m = (ndf_from - 1) * (nint_to + nface_to)
+    g_p = (ndf_to - 1) * (nint_from + nface_from)
+    bw = 1 + int(np.ceil((g_m + g_p) / beta))
+    return dict(alpha=alpha, beta=beta, gm=g_m, gp=g_p, bw=bw, ncol=ncol, nrow=nrow)
+
+
+def cma_prod_size(a, b):
+    """Parameters of the product A B (get_cma_prod_size, :same file)."""
+    alpha, beta = a["alpha"] * b["alpha"], a["beta"] * b["beta"]
+    gm = b["alpha"] * a["gm"] + a["beta"] * b["gm"]
+    gp = b["alpha"] * a["gp"] + a["beta"] * b["gp"]
+    bw = 1 + int(np.ceil((gm + gp) / beta))
+    return dict(alpha=alpha, beta=beta, gm=gm, gp=gp, bw=bw, ncol=b["ncol"], nrow=a["nrow"])
+
+
+def banded_dofmap(nlayers, ndf, nint, nface):
+    """column_banded_dofmap(ndf, nlayers), 1-based
+    (columnwise_operator_mod.f90:377-393)."""
+    k = np.arange(nlayers)[None, :]
+    df = np.arange(1, ndf + 1)[:, None]
+    return np.asfortranarray(k * (nint + nface) + df, dtype=np.int32)
+
+
+def _cma_args(p):
+    return [p["nrow"], p["ncol"], p["bw"], p["alpha"], p["beta"], p["gm"], p["gp"]]
+
+
+def cma_asm(ls, p, ncell, nlayers, cb_to, cb_from, dtype=np.float64):
+    """columnwise_op_asm over all cells; ls: (ncell*nlayers, ndf_to, ndf_from) F order."""
+    L = lib()
+    ls = np.asfortranarray(ls, dtype=dtype)
+    cm = np.zeros((p["bw"], p["nrow"], ncell), dtype=dtype, order="F")
+    fn = getattr(L, f"ora_columnwise_op_asm_code_{_sfx(dtype)}")
+    cbt, cbf = np.asfortranarray(cb_to, np.int32), np.asfortranarray(cb_from, np.int32)
+    for cell in range(1, ncell + 1):
+        fn(cell, nlayers, ncell, ncell * nlayers, _pF(ls), _pF(cm), p["nrow"], p["ncol"],
+           p["bw"], p["alpha"], p["beta"], p["gm"], p["gp"], cbt.shape[0],
+           cbt.ctypes.data_as(_ip), cbf.shape[0], cbf.ctypes.data_as(_ip))
+    return cm
+
+
+def cma_mul(A, pa, B, pb, C0, pc, ncell):
+    """C += A B over all cells (columnwise_op_mul)."""
+    L = lib()
+    dt = A.dtype
+    out = np.array(C0, dtype=dt, order="F")
+    fn = getattr(L, f"ora_columnwise_op_mul_code_{_sfx(dt)}")
+    A, B = np.asfortranarray(A), np.asfortranarray(B)
+    for cell in range(1, ncell + 1):
+        fn(cell, ncell, _pF(A), pa["nrow"], pa["ncol"], pa["bw"], pa["alpha"], pa["beta"],
+           pa["gm"], pa["gp"], _pF(B), pb["nrow"], pb["ncol"], pb["bw"], pb["alpha"],
+           pb["beta"], pb["gm"], pb["gp"], _pF(out), pc["nrow"], pc["ncol"], pc["bw"],
+           pc["alpha"], pc["beta"], pc["gm"], pc["gp"])
+    return out
+
+
+def cma_scaledadd(A, pa, B, pb, pc, ncell, alpha, beta):
+    """C = alpha A + beta B over all cells (columnwise_op_scaledadd)."""
+    L = lib()
+    dt = A.dtype
+    out = np.zeros((pc["bw"], pc["nrow"], ncell), dtype=dt, order="F")
+    fn = getattr(L, f"ora_columnwise_op_scaledadd_code_{_sfx(dt)}")
+    ct = C.c_double if dt == np.float64 else C.c_float
+    A, B = np.asfortranarray(A), np.asfortranarray(B)
+    for cell in range(1, ncell + 1):
+        fn(cell, ncell, _pF(A), pa["nrow"], pa["ncol"], pa["bw"], pa["alpha"], pa["beta"],
+           pa["gm"], pa["gp"], _pF(B), pb["nrow"], pb["ncol"], pb["bw"], pb["alpha"],
+           pb["beta"], pb["gm"], pb["gp"], _pF(out), pc["nrow"], pc["ncol"], pc["bw"],
+           pc["alpha"], pc["beta"], pc["gm"], pc["gp"], ct(alpha), ct(beta))
+    return out
+
+
+def cma_hmht(dh, m2h, p, ncell, nlayers, cb, dtype=np.float64):
+    """columnwise_op_asm_diag_hmht over all cells."""
+    L = lib()
+    dh, m2h = np.asfortranarray(dh, dtype=dtype), np.asfortranarray(m2h, dtype=dtype)
+    cm = np.zeros((p["bw"], p["nrow"], ncell), dtype=dtype, order="F")
+    fn = getattr(L, f"ora_columnwise_op_asm_diag_hmht_code_{_sfx(dtype)}")
+    cb = np.asfortranarray(cb, np.int32)
+    for cell in range(1, ncell + 1):
+        fn(cell, nlayers, ncell, ncell * nlayers, _pF(dh), _pF(m2h), _pF(cm), p["nrow"], p["bw"],
+           p["alpha"], p["beta"], p["gm"], p["gp"], cb.shape[0], cb.ctypes.data_as(_ip),
+           dh.shape[2])
+    return cm
+
+
+def cma_m2v(ls, p, ncell, nlayers, cb, dtype=np.float64):
+    """columnwise_op_asm_m2v_lumped_inv over all cells."""
+    L = lib()
+    ls = np.asfortranarray(ls, dtype=dtype)
+    cm = np.zeros((p["bw"], p["nrow"], ncell), dtype=dtype, order="F")
+    fn = getattr(L, f"ora_columnwise_op_asm_m2v_lumped_inv_code_{_sfx(dtype)}")
+    cb = np.asfortranarray(cb, np.int32)
+    for cell in range(1, ncell + 1):
+        fn(cell, nlayers, ncell, ncell * nlayers, _pF(ls), _pF(cm), p["nrow"], p["bw"],
+           cb.shape[0], cb.ctypes.data_as(_ip))
+    return cm
+
+
+def cma_dense(cm, p, cell=0):
+    """The dense nrow x ncol matrix of one column of a CMA operator."""
+    D = np.zeros((p["nrow"], p["ncol"]))
+    for i in range(1, p["nrow"] + 1):
+        jm = int(np.ceil((p["alpha"] * i - p["gp"]) / p["beta"]))
+        jp = int(np.floor((p["alpha"] * i + p["gm"]) / p["beta"]))
+        for j in range(max(1, jm), min(p["ncol"], jp) + 1):
+            D[i - 1, j - 1] = cm[j - jm, i - 1, cell]
+    return D

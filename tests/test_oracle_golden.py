@@ -224,3 +224,107 @@ def test_w0_kats():
     child, fc, cc = _w0_tables(k)
     out = oh.w0_transfer("prolong", child, fc, cc, np.array(k["coarse"]), k["nlayers"])
     assert np.allclose(out, k["fine"], atol=k["tol"])
+
+
+# ------------------------------------------------- CMA assembly and algebra
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_cma_asm_m3x3(dtype):
+    # columnwise_op_asm_kernel_mod_test.pf: Wtheta -> Wtheta, 3 layers, every
+    # cell stencil (1/3 1/6; 1/6 1/3): rows 1/3 1/6 | 1/6 2/3 1/6 | 1/6 1/3
+    g = load("cma_assembly_kat.json")
+    nl = g["nlayers"]
+    p = oh.cma_size(nl, 2, 2, 1, 0, 1, 0)
+    assert (p["alpha"], p["beta"], p["gm"], p["gp"], p["bw"]) == (1, 1, 1, 1, 3)
+    ls = np.tile(np.array(g["asm_stencil_fortran_order"]).reshape(2, 2, order="F"), (nl, 1, 1))
+    cb = oh.banded_dofmap(nl, 2, 0, 1)
+    cm = oh.cma_asm(ls, p, 1, nl, cb, cb, dtype)
+    tol = 1e-15 if dtype == np.float64 else 1e-7
+    for i in range(p["nrow"]):
+        if i == 0:
+            got, want = cm[1:3, i, 0], g["asm_first_row"]
+        elif i == p["nrow"] - 1:
+            got, want = cm[0:2, i, 0], g["asm_last_row"]
+        else:
+            got, want = cm[:, i, 0], g["asm_interior_row"]
+        assert np.allclose(got, want, rtol=0, atol=tol * 4)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_cma_mul_dtd(dtype):
+    # columnwise_op_mul_kernel_mod_test.pf: D (W3 <- Wtheta) bands (+1,-1),
+    # D^T (Wtheta <- W3) bands (-1,+1); C = D^T D against the dense product
+    g = load("cma_assembly_kat.json")
+    nl = g["mul_nlayers"]
+    pTT = oh.cma_size(nl, 2, 2, 1, 0, 1, 0)
+    pT3 = oh.cma_size(nl, 2, 1, 1, 0, 0, 1)
+    p3T = oh.cma_size(nl, 1, 2, 0, 1, 1, 0)
+    assert pT3["alpha"] == p3T["beta"] and pT3["bw"] == p3T["bw"]
+    assert pT3["gm"] == p3T["gp"] and pT3["gp"] == p3T["gm"]
+    D = np.zeros((p3T["bw"], p3T["nrow"], 1), dtype=dtype, order="F")
+    D[0, :, 0], D[1, :, 0] = g["mul_D_bands"]
+    DT = np.zeros((pT3["bw"], pT3["nrow"], 1), dtype=dtype, order="F")
+    DT[0, :, 0], DT[1, :, 0] = g["mul_DT_bands"]
+    C0 = np.zeros((pTT["bw"], pTT["nrow"], 1), dtype=dtype, order="F")
+    C = oh.cma_mul(DT, pT3, D, p3T, C0, pTT, 1)
+    Dd = np.zeros((p3T["nrow"], p3T["ncol"]))
+    for i in range(p3T["nrow"]):
+        Dd[i, i], Dd[i, i + 1] = 1.0, -1.0
+    assert np.allclose(oh.cma_dense(C, pTT), Dd.T @ Dd, rtol=0, atol=g["tol"])
+    assert np.array_equal(oh.cma_dense(C, pTT), Dd.T @ Dd)  # small integers: exact
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_cma_scaledadd(dtype):
+    # columnwise_op_scaledadd_kernel_mod_test.pf: C = mu M + nu DTD with M = I
+    # on W3 and DTD = tridiag(1, 2, 1) in the product pattern
+    g = load("cma_assembly_kat.json")
+    nl = g["nlayers"]
+    p33 = oh.cma_size(nl, 1, 1, 0, 1, 0, 1)
+    p3T = oh.cma_size(nl, 1, 2, 0, 1, 1, 0)
+    pT3 = oh.cma_size(nl, 2, 1, 1, 0, 0, 1)
+    pp = oh.cma_prod_size(p3T, pT3)
+    M = np.zeros((p33["bw"], p33["nrow"], 1), dtype=dtype, order="F")
+    M[0, :, 0] = 1.0
+    DTD = np.zeros((pp["bw"], pp["nrow"], 1), dtype=dtype, order="F")
+    for b, v in enumerate(g["scaledadd_DTD_bands"]):
+        DTD[b, :, 0] = v
+    mu, nu = g["scaledadd_mu"], g["scaledadd_nu"]
+    C = oh.cma_scaledadd(M, p33, DTD, pp, pp, 1, mu, nu)
+    dense = mu * np.eye(p33["nrow"]) + nu * (2 * np.eye(pp["nrow"]) + np.eye(pp["nrow"], k=1)
+                                            + np.eye(pp["nrow"], k=-1))
+    tol = 1e-14 if dtype == np.float64 else 2e-6
+    assert np.allclose(oh.cma_dense(C, pp), dense, rtol=0, atol=tol * 10)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_cma_asm_diag_hmht(dtype):
+    # columnwise_op_asm_diag_hmht_kernel_mod_test.pf: Dh = (rho), M2h =
+    # diag(sigma) per cell; every diagonal entry is sum rho^2 / sigma
+    g = load("cma_assembly_kat.json")
+    nl = g["nlayers"]
+    p = oh.cma_size(nl, 1, 1, 0, 1, 0, 1)
+    rho, sigma = np.array(g["hmht_rho"]), np.array(g["hmht_sigma"])
+    dh = np.tile(rho.reshape(1, 1, 4), (nl, 1, 1))
+    m2h = np.tile(np.diag(sigma)[None], (nl, 1, 1))
+    cb = oh.banded_dofmap(nl, 1, 1, 0)
+    cm = oh.cma_hmht(dh, m2h, p, 1, nl, cb, dtype)
+    answer = float(np.sum(rho ** 2 / sigma))
+    tol = 1e-14 if dtype == np.float64 else 1e-6
+    assert np.allclose(cm[0, :, 0], answer, rtol=tol, atol=0)
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_cma_asm_m2v_lumped_inv(dtype):
+    # columnwise_op_asm_m2v_lumped_inv_kernel_mod_test.pf: W2v, stencil
+    # (1/3 1/6; 1/6 1/3): band 1 holds 3 on the end rows, 3/2 inside
+    g = load("cma_assembly_kat.json")
+    nl = g["nlayers"]
+    p = oh.cma_size(nl, 2, 2, 1, 0, 1, 0)
+    ls = np.tile(np.array(g["m2v_stencil_fortran_order"]).reshape(2, 2, order="F"), (nl, 1, 1))
+    cb = oh.banded_dofmap(nl, 2, 0, 1)
+    cm = oh.cma_m2v(ls, p, 1, nl, cb, dtype)
+    want = np.full(p["nrow"], g["m2v_interior_rows"])
+    want[[0, -1]] = g["m2v_end_rows"]
+    tol = 1e-14 if dtype == np.float64 else 1e-6
+    assert np.allclose(cm[0, :, 0], want, rtol=tol, atol=0)
+    assert not np.any(cm[1:, :, 0])
