@@ -277,6 +277,7 @@ int lfg_prec_apply(lfg_prec prec, lfg_field x, lfg_field y);         /* y = P^{-
 #define LFG_SOLVER_BICGSTAB 5         /* bicgstab_solve :645-779      */
 #define LFG_SOLVER_GMRES 6            /* gmres_solve :830-1003        */
 #define LFG_SOLVER_FGMRES 7           /* fgmres_solve :1055-1237      */
+#define LFG_SOLVER_BLOCK_GCR 8        /* block_gcr_solve :1461-1628   */
 /* Mirrors the constructor arguments of the reference solver types
  * (sci_iterative_solver_mod.f90:100-113, 250-264) and solver_config. */
 typedef struct {
@@ -293,6 +294,12 @@ typedef struct {
 int lfg_solver_create(lfg_linop op, lfg_prec prec, const lfg_solver_cfg* cfg,
                       lfg_field like, lfg_solver* solver);
 int lfg_solver_destroy(lfg_solver solver);
+/* Block GCR only: the vector is a field_vector of n_fields fields stored as
+ * consecutive segments of the device field; segment n is elements
+ * [offsets[n], offsets[n+1]) of the level-major array (offsets[0] = 0,
+ * offsets[n_fields] = ncol*nlev).  Convergence is tested per field
+ * (field_norm(n), block_gcr_solve :1509, :1560-1570).  Default: one field. */
+int lfg_solver_set_fields(lfg_solver solver, int n_fields, const int64_t* offsets);
 /* Solve A x = b.  Returns LFG_OK, or LFG_NOT_CONVERGED / LFG_NAN as the
  * reference would log at LOG_LEVEL_ERROR; iterations and the last monitored
  * relative residual are returned when the pointers are non-NULL. */

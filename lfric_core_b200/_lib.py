@@ -34,7 +34,8 @@ def _ctype(tok: str):
     table = {
         "int": C.c_int, "double": C.c_double, "void*": C.c_void_p, "void *": C.c_void_p,
         "int*": C.POINTER(C.c_int), "double*": C.POINTER(C.c_double),
-        "uint64_t*": C.POINTER(C.c_uint64), "char*": C.c_char_p,
+        "uint64_t*": C.POINTER(C.c_uint64), "int64_t*": C.POINTER(C.c_int64),
+        "char*": C.c_char_p,
         "void**": C.POINTER(C.c_void_p),
         "lfg_solver_cfg*": C.POINTER(lfg_solver_cfg),
         "lfg_batch_cfg*": C.POINTER(lfg_batch_cfg),

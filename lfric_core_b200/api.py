@@ -32,7 +32,7 @@ OK, NOT_CONVERGED, NAN_STATUS = 0, 1, 2
 LMA_INC, LMA_WRITE, LMA_TRANSPOSE = 0, 1, 2
 RESTRICT_UNWEIGHTED, RESTRICT_WEIGHTED, RESTRICT_MASS_W3 = 0, 1, 2
 SOLVERS = {"cg": 0, "gcr": 1, "jacobi": 2, "chebyshev": 3, "precondition_only": 4,
-           "bicgstab": 5, "gmres": 6, "fgmres": 7}
+           "bicgstab": 5, "gmres": 6, "fgmres": 7, "block_gcr": 8}
 
 
 class LfgError(RuntimeError):
@@ -480,6 +480,13 @@ class IterativeSolver(_Handle):
                   "solver_create")
         super().__init__(ctx, h, [lin_op, prec])
         self.method, self.kind = method, like.kind
+
+    def set_fields(self, offsets):
+        """Block GCR: field n is elements [offsets[n], offsets[n+1]) of the
+        level-major device vector (a field_vector packed by segments)."""
+        off = np.ascontiguousarray(offsets, dtype=np.int64)
+        self.ctx.check(self.ctx.lib.lfg_solver_set_fields(
+            self.h, len(off) - 1, off.ctypes.data_as(C.POINTER(C.c_int64))), "solver_set_fields")
 
     def apply(self, x: Field, b: Field) -> SolveResult:
         it, err = C.c_int(), C.c_double()

@@ -404,6 +404,79 @@ struct GcrSolver : lfg_solver_s {
   }
 };
 
+// block_gcr_solve, sci_iterative_solver_mod.f90:1461-1628.  The vector is
+// a field_vector of n_fields fields packed as consecutive segments of one
+// device field (segment n = elements [off[n], off[n+1]) of the level-major
+// array); field_norm(n) is the norm over segment n.  x starts from P b and
+// is updated in place; the inner loop leaves as soon as every field has
+// converged, testing fields from the last one down as the reference does.
+struct BlockGcrSolver : lfg_solver_s {
+  std::vector<size_t> off;  // n_fields + 1 offsets; empty: one field
+  double field_norm(lfg_field f, int n, int slot) {
+    if (off.empty()) return std::sqrt(dot(f, f, slot));
+    lfg_field_s seg = *f;
+    seg.owned = false;
+    seg.d = (char*)f->d + off[n] * f->kind;
+    seg.ncol = (int)(off[n + 1] - off[n]);
+    seg.nlev = 1;
+    return std::sqrt(dot(&seg, &seg, slot));
+  }
+  int solve(lfg_field x, lfg_field b, int* iters, double* err_out) override {
+    const int k = cfg.gcrk;
+    const int nf = off.empty() ? 1 : (int)off.size() - 1;
+    lfg_field res = W(0), Ax = W(1);
+    auto V = [&](int i) { return W(2 + i); };
+    auto PV = [&](int i) { return W(2 + k + i); };
+    const int s_a = slot0, s_r = slot0 + 1, s_f = slot0 + 2, s_m = slot0 + 3;
+    const double* R = ctx->red_results;
+    std::vector<double> ie(nf, 1.0), fe(nf, 0.0);
+    std::vector<char> conv(nf, 0);
+    double err = NAN;
+    vec_set(x, sc_const(0.0));
+    prec->apply(b, x);
+    op->apply(x, Ax);
+    vec_axpby(res, sc_const(1.0), b, sc_const(-1.0), Ax);
+    if (cfg.monitor_convergence)
+      for (int n = 0; n < nf; ++n) ie[n] = std::max(field_norm(b, n, s_f), cfg.a_tol * cfg.r_tol);
+    int iter, steps = 0;
+    bool all_conv = false;
+    for (iter = 1; iter <= cfg.max_iter; ++iter) {
+      for (int iv = 0; iv < k; ++iv) {
+        prec->apply(res, PV(iv));
+        op->apply_dot(PV(iv), V(iv), iv == 0 ? nullptr : V(0), s_m);
+        for (int j = 0; j < iv; ++j)
+          vec_mgs_step(V(iv), PV(iv), V(j), PV(j), sc_mul(-1.0, R + s_m + j),
+                       j + 1 < iv ? V(j + 1) : nullptr, s_m + j + 1);
+        vec_scale2_dot(V(iv), PV(iv), sc_rsqrt(1.0, R + s_m + iv), res, s_a);
+        vec_update2_norm(x, PV(iv), res, V(iv), sc_mul(1.0, R + s_a), s_r);
+        ++steps;
+        if (cfg.monitor_convergence) {
+          std::fill(fe.begin(), fe.end(), 0.0);
+          for (int n = nf - 1; n >= 0; --n) {
+            fe[n] = nf == 1 ? std::sqrt(host(s_r)) : field_norm(res, n, s_f);
+            if (fe[n] / ie[n] < cfg.r_tol || fe[n] < cfg.a_tol) conv[n] = 1;
+            else break;
+          }
+          err = 0.0;
+          for (int n = 0; n < nf; ++n) err += fe[n] / ie[n];
+          all_conv = std::all_of(conv.begin(), conv.end(), [](char c) { return c != 0; });
+          if (all_conv) break;
+          std::fill(conv.begin(), conv.end(), 0);
+        }
+      }
+      if (cfg.monitor_convergence && all_conv) break;
+    }
+    if (iters) *iters = steps;
+    if (err_out) *err_out = err;
+    if (cfg.monitor_convergence) {
+      if (std::isnan(err)) return LFG_NAN;
+      if (iter >= cfg.max_iter && err > cfg.r_tol && cfg.fail_on_non_converged)
+        return LFG_NOT_CONVERGED;
+    }
+    return LFG_OK;
+  }
+};
+
 // jacobi_solve, sci_iterative_solver_mod.f90:1745-1815
 struct JacobiSolver : lfg_solver_s {
   int solve(lfg_field x, lfg_field b, int* iters, double* err_out) override {
@@ -890,6 +963,11 @@ int lfg_solver_create(lfg_linop op, lfg_prec prec, const lfg_solver_cfg* cfg, lf
         s = new FgmresSolver;
         nvec = 5 + 2 * cfg->gcrk;
         break;
+      case LFG_SOLVER_BLOCK_GCR:
+        LFG_REQUIRE(cfg->gcrk >= 1 && cfg->gcrk + 3 <= 40, "solver_create: gcrk 1..37");
+        s = new BlockGcrSolver;
+        nvec = 2 + 2 * cfg->gcrk;
+        break;
       default: throw Error(LFG_ERR_ARG, "solver_create: unknown method");
     }
     s->ctx = c;
@@ -907,6 +985,24 @@ int lfg_solver_create(lfg_linop op, lfg_prec prec, const lfg_solver_cfg* cfg, lf
       throw;
     }
     *out = s;
+  });
+}
+
+int lfg_solver_set_fields(lfg_solver s, int n_fields, const int64_t* offsets) {
+  if (!s) return LFG_ERR_ARG;
+  return guard(s->ctx, [&] {
+    auto* bg = dynamic_cast<BlockGcrSolver*>(s);
+    LFG_REQUIRE(bg, "solver_set_fields: only block GCR takes fields");
+    LFG_REQUIRE(n_fields >= 1 && offsets, "solver_set_fields: bad arguments");
+    const size_t n = (size_t)s->ncol * s->nlev;
+    std::vector<size_t> off(n_fields + 1);
+    for (int i = 0; i <= n_fields; ++i) {
+      LFG_REQUIRE(offsets[i] >= 0 && (size_t)offsets[i] <= n, "solver_set_fields: offset out of range");
+      off[i] = (size_t)offsets[i];
+      LFG_REQUIRE(i == 0 || off[i] > off[i - 1], "solver_set_fields: offsets must increase");
+    }
+    LFG_REQUIRE(off[0] == 0 && off[n_fields] == n, "solver_set_fields: fields must cover the vector");
+    bg->off = n_fields == 1 ? std::vector<size_t>() : off;
   });
 }
 

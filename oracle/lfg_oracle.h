@@ -207,6 +207,10 @@ typedef struct {
                            void* pctx, int k, double r_tol, double a_tol, int max_iter, \
                            int monitor, T* x, const T* b, T* work /* (5 + 2k) n */,     \
                            ora_solve_info* info);                                       \
+  int ora_block_gcr_solve_##S(long n, ora_apply_##S linop, void* lctx, ora_apply_##S prec,\
+                              void* pctx, int k, double r_tol, double a_tol, int max_iter,\
+                              int monitor, int nf, const int* field_of, T* x, const T* b, \
+                              T* work /* (2 + 2k) n */, ora_solve_info* info);            \
   void ora_helm_apply_cb_##S(void* op, const T* x, T* y);                               \
   void ora_mg_apply_cb_##S(void* mg, const T* x, T* y);
 ORA_DECL_SOLVERS(double, d)

@@ -214,6 +214,10 @@ def _setup_signatures(L):
         getattr(L, f"ora_{nm}_solve_d").argtypes = [
             C.c_long, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int, C.c_double,
             C.c_double, C.c_int, C.c_int, _dp, _dp, _dp, C.c_void_p]
+    L.ora_block_gcr_solve_d.argtypes = [C.c_long, C.c_void_p, C.c_void_p, C.c_void_p,
+                                        C.c_void_p, C.c_int, C.c_double, C.c_double, C.c_int,
+                                        C.c_int, C.c_int, C.POINTER(C.c_int), _dp, _dp, _dp,
+                                        C.c_void_p]
     L.ora_bicgstab_solve_d.argtypes = [C.c_long, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                        C.c_double, C.c_double, C.c_int, C.c_int, _dp, _dp, _dp,
                                        C.c_void_p]

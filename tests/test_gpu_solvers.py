@@ -170,6 +170,43 @@ def test_krylov_variants_parity(ctx, helm24, method, iters):
     assert abs(out.final_err - info.final_err) <= 1e-6 * abs(info.final_err) + 1e-15
 
 
+@pytest.mark.parametrize("nf", [1, 2, 3])
+def test_block_gcr_parity(ctx, helm24, nf):
+    """block_gcr_solve with the multigrid preconditioner against the
+    oracle; the vector is split into nf fields by level ranges (the device
+    vector is level-major, so a level range is one segment)."""
+    import ctypes as C
+    from oracle.oracle import lib, ptr, SolveInfo
+    p = helm24
+    ora = OraHelm(p)
+    S = api.HelmholtzSystem(ctx, p, mixed=False)
+    sol = api.IterativeSolver(api.LinearOperator.from_helmholtz(S.op64), S.mg64, S.x64,
+                              "block_gcr", r_tol=1e-8, max_iter=20, gcrk=6)
+    nl, ncol = p.nlayers, p.ncol
+    cuts = [0] + [round(nl * (i + 1) / nf) for i in range(nf)]
+    sol.set_fields([c * ncol for c in cuts])
+    B, X = S.op64.field(p.rhs), S.op64.field()
+    out = sol.apply(X, B)
+    # the oracle works in the column-contiguous layout: dof c*nl + k
+    level = np.tile(np.arange(nl), ncol)
+    field_of = np.searchsorted(np.array(cuts[1:]), level, side="right").astype(np.int32)
+    L = lib()
+    n = p.ndof
+    x = np.zeros(n)
+    info = SolveInfo()
+    work = np.zeros((2 + 2 * 6) * n)
+    op, mg = ora.op(0), ora.mg()
+    st = L.ora_block_gcr_solve_d(n, C.cast(L.ora_helm_apply_cb_d, C.c_void_p), C.byref(op),
+                                 C.cast(L.ora_mg_apply_cb_d, C.c_void_p), C.byref(mg), 6, 1e-8,
+                                 0.0, 20, 1, nf, field_of.ctypes.data_as(C.POINTER(C.c_int)),
+                                 ptr(x), ptr(np.ascontiguousarray(p.rhs)), ptr(work),
+                                 C.byref(info))
+    assert out.status == st == 0
+    assert out.iterations == info.iterations
+    assert rel(X.export(), x) < 1e-12
+    assert abs(out.final_err - info.final_err) <= 1e-6 * info.final_err
+
+
 @pytest.mark.parametrize("method", ["bicgstab", "gmres", "fgmres", "cg"])
 def test_krylov_variants_converge(ctx, method):
     p = helmholtz_problem(8, 10, seed=5, mg_levels=2)
