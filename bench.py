@@ -52,6 +52,17 @@ def parse():
     return ap.parse_args()
 
 
+def max_over_ranks(value: float, world: int, device: str = "cuda") -> float:
+    """The largest value over all ranks (device times are reported as the
+    slowest rank's); the identity on one rank."""
+    if world <= 1:
+        return value
+    import torch
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -184,7 +195,7 @@ def run_reference(args, rank, world):
 
 
 def measure_batched(ctx, stream, steps: int, warmup: int, n_rhs: int = 64, n_uneven: int = 32,
-                    shape=(0, 0)) -> dict:
+                    shape=(0, 0), world: int = 1) -> dict:
     """The batched workload: 64 seeded right-hand sides on one C48 x 30
     operator plus 32 problems with n in 12..96 and 10..70 levels, all solved
     to 1e-8 in one persistent launch (lfg_batch_*).  Device-resident timing
@@ -217,7 +228,7 @@ def measure_batched(ctx, stream, steps: int, warmup: int, n_rhs: int = 64, n_une
     e1.record(stream)
     nfailed = B.wait()
     launches = (ctx.kernel_launches() - n0) / steps
-    ms = e0.elapsed_time(e1) / steps
+    ms = max_over_ranks(e0.elapsed_time(e1), world) / steps
     res = [B.result(i) for i in range(len(B))]
 
     def e2e_step():
@@ -235,7 +246,7 @@ def measure_batched(ctx, stream, steps: int, warmup: int, n_rhs: int = 64, n_une
         e2e_step()
     e1.record(stream)
     torch.cuda.synchronize()
-    ms_e2e = e0.elapsed_time(e1) / steps
+    ms_e2e = max_over_ranks(e0.elapsed_time(e1), world) / steps
     # algorithmic bytes per problem dof: RESID 96 (FP64 x, b, operator; FP32
     # r, e, z written, sub, inv, c' read), APPLY 44, UPDATE 40, CORRECT 20
     nbytes = 0.0
@@ -321,11 +332,7 @@ def main():
             last = fn()
         e1.record(stream)
         barrier()
-        ms = e0.elapsed_time(e1)
-        if world > 1:
-            t = torch.tensor([ms], device="cuda", dtype=torch.float64)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            ms = float(t.item())
+        ms = max_over_ranks(e0.elapsed_time(e1), world)
         return ms, ctx.kernel_launches() - n0, last
 
     # ---- warm-up (both forms)
@@ -404,7 +411,7 @@ def main():
 
     # ---- batched persistent solves (every rank: replicas)
     torch.cuda.nvtx.range_push("batched")
-    batched = measure_batched(ctx, stream, max(1, args.steps), max(1, args.warmup))
+    batched = measure_batched(ctx, stream, max(1, args.steps), max(1, args.warmup), world=world)
     torch.cuda.nvtx.range_pop()
 
     # ---- CPU baseline (rank 0, N=1 only): the oracle on a bounded sample
