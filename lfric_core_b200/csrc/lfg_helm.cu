@@ -615,15 +615,15 @@ void smooth_t(lfg_helm op, double omega, lfg_field x_in, lfg_field b, lfg_field 
     return;
   }
   T* r = (T*)rbuf;
-  const int grid = c->stream_grid((size_t)op->ncol * ((op->nl + KC - 1) / KC), 256);
+  const size_t work = (size_t)op->ncol * ((op->nl + KC - 1) / KC);
   if (!ig) {
-    k_helm_rhs<T, false><<<grid, 256, 0, c->stream>>>(args_of<T>(op), (const T*)x_in->d,
+    k_helm_rhs<T, false><<<occ_grid(c, (const void*)k_helm_rhs<T, false>, 256, work), 256, 0, c->stream>>>(args_of<T>(op), (const T*)x_in->d,
                                                        (const T*)b->d, r, nullptr, nullptr, 0);
     after_launch(c, "helm_rhs");
     launch_subst<T, true, false>(c, op->ncol, op->nl, r, sub, inv, cp, (const T*)x_in->d,
                                  nullptr, nullptr, 0, om, (T*)x_out->d);
   } else {
-    k_helm_rhs<T, true><<<grid, 256, 0, c->stream>>>(args_of<T>(op), (const T*)x_in->d,
+    k_helm_rhs<T, true><<<occ_grid(c, (const void*)k_helm_rhs<T, true>, 256, work), 256, 0, c->stream>>>(args_of<T>(op), (const T*)x_in->d,
                                                       (const T*)b->d, r, ig->parent,
                                                       (const T*)xc->d, ig->ncoarse);
     after_launch(c, "helm_rhs");
@@ -646,24 +646,25 @@ void helm_apply(lfg_helm op, lfg_field y, lfg_field x, lfg_field dot_with, int s
   check_field(op, y, "helm_apply");
   check_field(op, x, "helm_apply");
   lfg_ctx c = op->ctx;
-  const int bs = 256, grid = c->stream_grid((size_t)op->ncol * ((op->nl + KC - 1) / KC), bs);
+  const int bs = 256;
+  const size_t work = (size_t)op->ncol * ((op->nl + KC - 1) / KC);
   Red r = slot >= 0 ? c->red(slot) : Red{nullptr, nullptr, nullptr};
   if (op->kind == LFG_R_DOUBLE) {
     using T = double;
     if (slot >= 0 && dot_with)
-      k_helm_apply<T, false, true, true><<<grid, bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, nullptr, (T*)y->d, (const T*)dot_with->d, r);
+      k_helm_apply<T, false, true, true><<<occ_grid(c, (const void*)k_helm_apply<T, false, true, true>, bs, work), bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, nullptr, (T*)y->d, (const T*)dot_with->d, r);
     else if (slot >= 0)
-      k_helm_apply<T, false, true, false><<<grid, bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, nullptr, (T*)y->d, nullptr, r);
+      k_helm_apply<T, false, true, false><<<occ_grid(c, (const void*)k_helm_apply<T, false, true, false>, bs, work), bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, nullptr, (T*)y->d, nullptr, r);
     else
-      k_helm_apply<T, false, false><<<grid, bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, nullptr, (T*)y->d, nullptr, r);
+      k_helm_apply<T, false, false><<<occ_grid(c, (const void*)k_helm_apply<T, false, false>, bs, work), bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, nullptr, (T*)y->d, nullptr, r);
   } else {
     using T = float;
     if (slot >= 0 && dot_with)
-      k_helm_apply<T, false, true, true><<<grid, bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, nullptr, (T*)y->d, (const T*)dot_with->d, r);
+      k_helm_apply<T, false, true, true><<<occ_grid(c, (const void*)k_helm_apply<T, false, true, true>, bs, work), bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, nullptr, (T*)y->d, (const T*)dot_with->d, r);
     else if (slot >= 0)
-      k_helm_apply<T, false, true, false><<<grid, bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, nullptr, (T*)y->d, nullptr, r);
+      k_helm_apply<T, false, true, false><<<occ_grid(c, (const void*)k_helm_apply<T, false, true, false>, bs, work), bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, nullptr, (T*)y->d, nullptr, r);
     else
-      k_helm_apply<T, false, false><<<grid, bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, nullptr, (T*)y->d, nullptr, r);
+      k_helm_apply<T, false, false><<<occ_grid(c, (const void*)k_helm_apply<T, false, false>, bs, work), bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, nullptr, (T*)y->d, nullptr, r);
   }
   after_launch(c, "helm_apply");
 }
@@ -673,20 +674,21 @@ void helm_residual(lfg_helm op, lfg_field r_out, lfg_field x, lfg_field b, int s
   check_field(op, x, "helm_residual");
   check_field(op, b, "helm_residual");
   lfg_ctx c = op->ctx;
-  const int bs = 256, grid = c->stream_grid((size_t)op->ncol * ((op->nl + KC - 1) / KC), bs);
+  const int bs = 256;
+  const size_t work = (size_t)op->ncol * ((op->nl + KC - 1) / KC);
   Red r = slot >= 0 ? c->red(slot) : Red{nullptr, nullptr, nullptr};
   if (op->kind == LFG_R_DOUBLE) {
     using T = double;
     if (slot >= 0)
-      k_helm_apply<T, true, true><<<grid, bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, (const T*)b->d, (T*)r_out->d, nullptr, r);
+      k_helm_apply<T, true, true><<<occ_grid(c, (const void*)k_helm_apply<T, true, true>, bs, work), bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, (const T*)b->d, (T*)r_out->d, nullptr, r);
     else
-      k_helm_apply<T, true, false><<<grid, bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, (const T*)b->d, (T*)r_out->d, nullptr, r);
+      k_helm_apply<T, true, false><<<occ_grid(c, (const void*)k_helm_apply<T, true, false>, bs, work), bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, (const T*)b->d, (T*)r_out->d, nullptr, r);
   } else {
     using T = float;
     if (slot >= 0)
-      k_helm_apply<T, true, true><<<grid, bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, (const T*)b->d, (T*)r_out->d, nullptr, r);
+      k_helm_apply<T, true, true><<<occ_grid(c, (const void*)k_helm_apply<T, true, true>, bs, work), bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, (const T*)b->d, (T*)r_out->d, nullptr, r);
     else
-      k_helm_apply<T, true, false><<<grid, bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, (const T*)b->d, (T*)r_out->d, nullptr, r);
+      k_helm_apply<T, true, false><<<occ_grid(c, (const void*)k_helm_apply<T, true, false>, bs, work), bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, (const T*)b->d, (T*)r_out->d, nullptr, r);
   }
   after_launch(c, "helm_residual");
 }
@@ -717,11 +719,12 @@ void helm_residual_restrict(lfg_helm op, lfg_intergrid ig, lfg_field x, lfg_fiel
                   bc->kind == op->kind && ig->nx * ig->ny <= 4,
               "residual_restrict: bad coarse field");
   lfg_ctx c = op->ctx;
-  const int bs = 256, grid = c->stream_grid((size_t)ig->ncoarse * ((op->nl + KR - 1) / KR), bs);
+  const int bs = 256;
+  const size_t work = (size_t)ig->ncoarse * ((op->nl + KR - 1) / KR);
   if (op->kind == LFG_R_DOUBLE)
-    k_helm_resid_restrict<double><<<grid, bs, 0, c->stream>>>(args_of<double>(op), (const double*)x->d, (const double*)b->d, (double*)bc->d, ig->child, ig->ncoarse, ig->nx * ig->ny);
+    k_helm_resid_restrict<double><<<occ_grid(c, (const void*)k_helm_resid_restrict<double>, bs, work), bs, 0, c->stream>>>(args_of<double>(op), (const double*)x->d, (const double*)b->d, (double*)bc->d, ig->child, ig->ncoarse, ig->nx * ig->ny);
   else
-    k_helm_resid_restrict<float><<<grid, bs, 0, c->stream>>>(args_of<float>(op), (const float*)x->d, (const float*)b->d, (float*)bc->d, ig->child, ig->ncoarse, ig->nx * ig->ny);
+    k_helm_resid_restrict<float><<<occ_grid(c, (const void*)k_helm_resid_restrict<float>, bs, work), bs, 0, c->stream>>>(args_of<float>(op), (const float*)x->d, (const float*)b->d, (float*)bc->d, ig->child, ig->ncoarse, ig->nx * ig->ny);
   after_launch(c, "resid_restrict");
 }
 

@@ -9,8 +9,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <mutex>
+#include <unordered_map>
 #include <stdexcept>
 #include <string>
 #include <vector>
@@ -265,6 +268,30 @@ int guard(lfg_ctx ctx, F&& f) {
     if (ctx) ctx->last_error = e.what();
     return LFG_ERR_ARG;
   }
+}
+
+// Grid for a grid-stride kernel: enough blocks for `work` threads, capped
+// at one full wave (the blocks of `kern` that fit on every SM at once, from
+// the occupancy calculator; cached per kernel).  A cap above one wave would
+// leave a partial second wave whose blocks each walk the grid-stride loop
+// on their own.
+inline int occ_grid(lfg_ctx c, const void* kern, int threads, size_t work, size_t smem = 0) {
+  static std::mutex mu;
+  static std::unordered_map<const void*, int> per_sm;
+  int nb;
+  {
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = per_sm.find(kern);
+    if (it == per_sm.end()) {
+      int v = 0;
+      LFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, kern, threads, smem));
+      it = per_sm.emplace(kern, v > 0 ? v : 1).first;
+    }
+    nb = it->second;
+  }
+  const size_t need = (work + threads - 1) / threads;
+  const size_t cap = (size_t)c->num_sms * nb;
+  return (int)std::max<size_t>(1, std::min(need, cap));
 }
 
 // vector algebra launchers (lfg_core.cu)
