@@ -372,10 +372,10 @@ def main():
     R.aypx(-1.0, system.b64)
     true_rel = R.norm() / system.b64.norm()
 
-    # ---- roofline of the dominant kernel: k_helm_subst, the column
-    # substitution sweep (the zero-start smoother sweep is exactly one launch
-    # of it), FP32, on the C192 level; the full sweep from a nonzero guess
-    # (k_helm_rhs + k_helm_subst) is timed beside it
+    # ---- roofline of the dominant kernel family: the column substitution
+    # (the zero-start smoother sweep is exactly one launch of it, k_subst_tma
+    # on FP32 fine meshes), on the C192 level; the full sweep from a nonzero
+    # guess (k_helm_rhs + the substitution) is timed beside it
     op32 = system.levels32[0]
     xs, bs, ys = op32.field(), op32.field(), op32.field()
     xs.copy(system.x64)
@@ -453,12 +453,12 @@ def main():
                     "d2h_bytes_per_step": N * 8},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm",
-                         "kernel": "k_helm_subst<float> zero-start column sweep, C192x70",
+                         "kernel": "k_subst_tma<false> zero-start column sweep (TMA-staged), C192x70",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
                          "traffic": traffic, "algorithmic_bytes": subst_bytes,
                          "ms_per_launch": subst_ms},
-            "smoother_sweep": {"kernels": "k_helm_rhs + k_helm_subst, FP32, C192x70",
+            "smoother_sweep": {"kernels": "k_helm_rhs + k_subst_tma<true>, FP32, C192x70",
                                "ms": sweep_ms, "algorithmic_bytes": sweep_bytes,
                                "GB/s": sweep_bytes / (sweep_ms * 1e-3) / 1e9},
             "batched": batched,

@@ -62,6 +62,8 @@ int lfg_ctx_create(int device, lfg_ctx* ctx);
 int lfg_ctx_destroy(lfg_ctx ctx);
 /* Use an external cudaStream_t (passed as void*); NULL restores the own stream. */
 int lfg_ctx_set_stream(lfg_ctx ctx, void* stream);
+/* Waits for the context's stream; LFG_ERR_STATE when a kernel's bounded
+ * wait ran out since the last check (solver applies check the same). */
 int lfg_ctx_synchronize(lfg_ctx ctx);
 /* Number of kernels this library has launched on the context so far. */
 int lfg_ctx_kernel_launches(lfg_ctx ctx, uint64_t* count);

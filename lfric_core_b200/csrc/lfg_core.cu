@@ -404,6 +404,21 @@ void vec_scale_copy(lfg_field dst, Sc a, lfg_field src) {
 
 }  // namespace lfg
 
+namespace lfg {
+void check_device_error(lfg_ctx c) {
+  if (!c->dev_err) return;
+  unsigned e = 0;
+  LFG_CUDA(cudaMemcpyAsync(&e, c->dev_err, sizeof(e), cudaMemcpyDeviceToHost, c->stream));
+  LFG_CUDA(cudaStreamSynchronize(c->stream));
+  if (e) {
+    LFG_CUDA(cudaMemsetAsync(c->dev_err, 0, sizeof(unsigned), c->stream));
+    char buf[96];
+    snprintf(buf, sizeof(buf), "a kernel's bounded wait ran out (device error 0x%x)", e);
+    throw Error(LFG_ERR_STATE, buf);
+  }
+}
+}  // namespace lfg
+
 // ------------------------------------------------------------ ctx methods
 void* lfg_ctx_s::staging(size_t bytes) {
   if (bytes > stage_bytes) {
@@ -457,6 +472,8 @@ int lfg_ctx_create(int device, lfg_ctx* out) {
     LFG_CUDA(cudaMemset(c->red_counters, 0, sizeof(unsigned) * kRedSlots));
     LFG_CUDA(cudaMemset(c->red_results, 0, sizeof(double) * kRedSlots));
     LFG_CUDA(cudaMallocHost(&c->host_results, sizeof(double) * kRedSlots));
+    c->dev_err = (unsigned*)dmalloc(sizeof(unsigned));
+    LFG_CUDA(cudaMemset(c->dev_err, 0, sizeof(unsigned)));
   });
   if (st != LFG_OK) {
     fprintf(stderr, "lfg_ctx_create: %s\n", c->last_error.c_str());
@@ -475,6 +492,7 @@ int lfg_ctx_destroy(lfg_ctx c) {
   dfree(c->red_results);
   dfree(c->stage);
   dfree(c->scratch_buf);
+  dfree(c->dev_err);
   if (c->host_results) cudaFreeHost(c->host_results);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -489,7 +507,10 @@ int lfg_ctx_set_stream(lfg_ctx c, void* stream) {
 
 int lfg_ctx_synchronize(lfg_ctx c) {
   if (!c) return LFG_ERR_ARG;
-  return guard(c, [&] { LFG_CUDA(cudaStreamSynchronize(c->stream)); });
+  return guard(c, [&] {
+    LFG_CUDA(cudaStreamSynchronize(c->stream));
+    check_device_error(c);
+  });
 }
 
 int lfg_ctx_kernel_launches(lfg_ctx c, uint64_t* count) {

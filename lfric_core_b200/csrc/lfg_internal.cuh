@@ -145,6 +145,9 @@ struct lfg_ctx_s {
   // device scratch of the kernels that need one (grown on demand)
   void* scratch_buf = nullptr;
   size_t scratch_bytes = 0;
+  // device error word: kernels whose bounded waits ran out record a code
+  // here (0 = none); read by check_device_error
+  unsigned* dev_err = nullptr;
 
   lfg::Red red(int slot) {
     return lfg::Red{red_partials + (size_t)slot * lfg::kMaxRedBlocks, red_counters + slot,
@@ -293,6 +296,14 @@ inline int occ_grid(lfg_ctx c, const void* kern, int threads, size_t work, size_
   const size_t cap = (size_t)c->num_sms * nb;
   return (int)std::max<size_t>(1, std::min(need, cap));
 }
+
+// Throws LFG_ERR_STATE when a kernel recorded a device error (synchronises).
+void check_device_error(lfg_ctx c);
+
+// TMA-staged column substitution (lfg_subst_tma.cu), FP32 fine meshes.
+bool subst_tma_applicable(lfg_ctx c, int ncol, int nl, const void* const* ptrs, int nptr);
+void subst_tma(lfg_ctx c, int ncol, int nl, const float* r, const float* sub, const float* inv,
+               const float* cp, const float* xin, float omega, float* xout);
 
 // vector algebra launchers (lfg_core.cu)
 void vec_set(lfg_field x, Sc a);

@@ -1019,6 +1019,7 @@ int lfg_solver_apply(lfg_solver s, lfg_field x, lfg_field b, int* iterations, do
                     b->ncol == s->ncol && b->nlev == s->nlev && b->kind == s->kind,
                 "solver_apply: fields do not match the solver");
     status = s->solve(x, b, iterations, err);
+    check_device_error(s->ctx);
   });
   return st != LFG_OK ? st : status;
 }
@@ -1107,6 +1108,7 @@ int lfg_mixed_apply(lfg_mixed m, lfg_field x, lfg_field b, int* outer, int* inne
     if (outer) *outer = o;
     if (inner_total) *inner_total = inner_steps;
     if (rel) *rel = rr;
+    check_device_error(c);
   });
   return st != LFG_OK ? st : status;
 }

@@ -366,6 +366,28 @@ def test_helmholtz_apply_and_smooth(ctx, helm_small, kind):
     assert rel(Y.export(np.float64), ora.smooth(x, b, 0.8)) < tol
 
 
+@pytest.mark.parametrize("n,kind", [(24, R_SINGLE), (48, R_DOUBLE), (96, R_SINGLE),
+                                    (96, R_DOUBLE)])
+def test_helmholtz_smooth_each_launch_path(ctx, n, kind):
+    """The sweep runs as the segmented one-kernel sweep on meshes with few
+    columns (C24, C48), and as right-hand side + substitution on C96 (the
+    FP32 substitution through TMA-staged tiles): all against the oracle."""
+    p = helmholtz_problem(n, 70, seed=11, mg_levels=1)
+    dt = np.float64 if kind == R_DOUBLE else np.float32
+    ora = OraHelm(p)
+    H = api.Helmholtz(ctx, kind, api.Mesh(ctx, p.links), p.nlayers, p.cm, p.hf)
+    rng = np.random.default_rng(13)
+    x = rng.standard_normal(p.ndof).astype(dt)
+    b = rng.standard_normal(p.ndof).astype(dt)
+    X, B, Y = H.field(x), H.field(b), H.field()
+    tol = TOL64 if kind == R_DOUBLE else 2e-6
+    H.smooth(0.8, None, B, Y)
+    assert rel(Y.export(np.float64), ora.smooth(None, b, 0.8)) < tol
+    H.smooth(0.8, X, B, Y)
+    assert rel(Y.export(np.float64), ora.smooth(x, b, 0.8)) < tol
+    ctx.synchronize()   # no bounded wait ran out
+
+
 def test_galerkin_coarse_operator(ctx, helm_small):
     p = helm_small
     ora = OraHelm(p)
