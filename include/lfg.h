@@ -132,6 +132,26 @@ int lfg_prolong_scalar(lfg_intergrid ig, lfg_field fine, lfg_field coarse, lfg_f
 int lfg_restrict_w0(lfg_intergrid ig, lfg_field coarse, lfg_field fine);
 int lfg_prolong_w0(lfg_intergrid ig, lfg_field fine, lfg_field coarse);
 
+/* W2 intergrid transfers (components/science/source/kernel/inter_mesh/) on
+ * flat W2 fields (ncol = undf, nlev = 1) in the reference's dof order.
+ * map_coarse[C*ndf + df] / map_fine[c*ndf + df]: 0-based dof of level 0 of
+ * cell dof df (W, S, E, N, B, T for ndf 6 and W, S, E, N for ndf 4; B, T for
+ * ndf 2); face selectors (1 or 2 per coarse cell) say how many of the E-W
+ * and N-S faces the cell writes, as the reference's face_selector fields. */
+typedef struct lfg_w2map_s* lfg_w2map;
+int lfg_w2map_create(lfg_intergrid ig, int nlayers, int ndf, const int* map_coarse,
+                     int undf_coarse, const int* map_fine, int undf_fine,
+                     const int* face_selector_ew, const int* face_selector_ns, lfg_w2map* map);
+int lfg_w2map_destroy(lfg_w2map map);
+#define LFG_W2_FULL 0   /* restrict_w2  (sci_restrict_w2_kernel_mod.F90)  */
+#define LFG_W2_H 1      /* restrict_w2h (sci_restrict_w2h_kernel_mod.F90) */
+#define LFG_W2_V 2      /* restrict_w2v (sci_restrict_w2v_kernel_mod.F90) */
+int lfg_w2_restrict(lfg_w2map map, int mode, lfg_field coarse, lfg_field fine);
+/* weights_prolong_w2_kernel_code (sci_weights_prolong_w2_kernel_mod.F90) */
+int lfg_w2_prolong_weights(lfg_w2map map, lfg_field weights);
+/* prolong_w2_kernel_code (sci_prolong_w2_kernel_mod.F90) */
+int lfg_w2_prolong(lfg_w2map map, lfg_field fine, lfg_field coarse, lfg_field weights);
+
 /* ------------------------------------------------------------ CMA operators
  * columnwise_operator_type (infrastructure/source/operator/
  * columnwise_operator_mod.f90:42-114): banded column matrices

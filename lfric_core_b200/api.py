@@ -256,6 +256,41 @@ class Intergrid(_Handle):
         self.ctx.check(self.ctx.lib.lfg_prolong_w0(self.h, fine.h, coarse.h), "prolong_w0")
 
 
+W2_FULL, W2_H, W2_V = 0, 1, 2
+
+
+class W2Map(_Handle):
+    """W2 intergrid maps for lfg_w2_*: 0-based dofmaps (ncell, ndf) of the
+    coarse and fine W2 spaces on an Intergrid's meshes, face selectors per
+    coarse cell.  Fields are flat (undf x 1) in the reference's dof order."""
+
+    _destroy = "lfg_w2map_destroy"
+
+    def __init__(self, ig: "Intergrid", nlayers: int, map_coarse, undf_coarse: int, map_fine,
+                 undf_fine: int, sel_ew=None, sel_ns=None):
+        mc = np.ascontiguousarray(map_coarse, dtype=np.int32)
+        mf = np.ascontiguousarray(map_fine, dtype=np.int32)
+        ew = None if sel_ew is None else np.ascontiguousarray(sel_ew, dtype=np.int32)
+        ns = None if sel_ns is None else np.ascontiguousarray(sel_ns, dtype=np.int32)
+        h = C.c_void_p()
+        ig.ctx.check(ig.ctx.lib.lfg_w2map_create(
+            ig.h, nlayers, mc.shape[1], _iptr(mc), undf_coarse, _iptr(mf), undf_fine,
+            None if ew is None else _iptr(ew), None if ns is None else _iptr(ns), C.byref(h)),
+            "w2map_create")
+        super().__init__(ig.ctx, h, [ig])
+        self.undf_coarse, self.undf_fine = undf_coarse, undf_fine
+
+    def restrict(self, mode: int, coarse: "Field", fine: "Field"):
+        self.ctx.check(self.ctx.lib.lfg_w2_restrict(self.h, mode, coarse.h, fine.h), "w2_restrict")
+
+    def prolong_weights(self, weights: "Field"):
+        self.ctx.check(self.ctx.lib.lfg_w2_prolong_weights(self.h, weights.h), "w2_weights")
+
+    def prolong(self, fine: "Field", coarse: "Field", weights: "Field"):
+        self.ctx.check(self.ctx.lib.lfg_w2_prolong(self.h, fine.h, coarse.h, weights.h),
+                       "w2_prolong")
+
+
 class ColumnwiseOperator(_Handle):
     """columnwise_operator_type: columnwise_matrix(bw, nrow, ncol) Fortran order."""
 

@@ -106,6 +106,32 @@ void ora_prolong_w0_code(int nlayers, const int* cell_map, int nx, int ny, int n
  * number in use (1 without OpenMP). */
 int ora_threads(int n);
 
+/* W2 intergrid transfers (components/science/source/kernel/inter_mesh/),
+ * per coarse cell, 1-based maps; work holds nlayers+1 values. */
+void ora_restrict_w2_code_r_double(int nlayers, const int* cell_map, int nx, int ny,
+                                   int ncell_fine, double* coarse, const double* fine,
+                                   const int* sel_ew, const int* sel_ns, const int* map_coarse,
+                                   int ndf, const int* map_fine, const int* map_w3_2d,
+                                   int with_b, double* work);
+void ora_restrict_w2_code_r_single(int nlayers, const int* cell_map, int nx, int ny,
+                                   int ncell_fine, float* coarse, const float* fine,
+                                   const int* sel_ew, const int* sel_ns, const int* map_coarse,
+                                   int ndf, const int* map_fine, const int* map_w3_2d,
+                                   int with_b, float* work);
+void ora_restrict_w2v_code_r_double(int nlayers, const int* cell_map, int nx, int ny,
+                                    int ncell_fine, double* coarse, const double* fine,
+                                    const int* map_coarse, int ndf, const int* map_fine,
+                                    double* work);
+void ora_restrict_w2v_code_r_single(int nlayers, const int* cell_map, int nx, int ny,
+                                    int ncell_fine, float* coarse, const float* fine,
+                                    const int* map_coarse, int ndf, const int* map_fine,
+                                    float* work);
+void ora_weights_prolong_w2_code(int nlayers, const int* cell_map, int nx, int ny,
+                                 int ncell_fine, double* w, int ndf, const int* map_fine);
+void ora_prolong_w2_code(int nlayers, const int* cell_map, int nx, int ny, int ncell_fine,
+                         double* fine, const double* coarse, const double* w, int ndf,
+                         const int* map_fine, const int* map_coarse);
+
 void ora_cma_params(int nlayers, int nint_to, int nface_to, int nint_from, int nface_from,
                     const int* offsets_to, const int* offsets_from, int* out7,
                     int* indirection_to, int* indirection_from);

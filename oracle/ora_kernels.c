@@ -596,3 +596,133 @@ void ora_cma_params(int nlayers, int nint_to, int nface_to, int nint_from, int n
     }
   }
 }
+
+/* ------------------------------------------------- W2 intergrid transfers
+ * components/science/source/kernel/inter_mesh/: per coarse cell, with the
+ * reference's W2 dof numbering W=1, S=2, E=3, N=4, B=5, T=6, cell_map(x, y)
+ * (x W->E, y N->S) and 1-based maps. */
+enum { ORA_W = 1, ORA_S = 2, ORA_E = 3, ORA_N = 4, ORA_B = 5 };
+
+/* fine-cell ranges of each horizontal face of the coarse cell */
+static void ora_w2_face_ranges(int nx, int ny, int xs[5], int xe[5], int ys[5], int ye[5]) {
+  xs[ORA_N] = 1; xe[ORA_N] = nx; ys[ORA_N] = 1; ye[ORA_N] = 1;
+  xs[ORA_S] = 1; xe[ORA_S] = nx; ys[ORA_S] = ny; ye[ORA_S] = ny;
+  xs[ORA_W] = 1; xe[ORA_W] = 1; ys[ORA_W] = 1; ye[ORA_W] = ny;
+  xs[ORA_E] = nx; xe[ORA_E] = nx; ys[ORA_E] = 1; ye[ORA_E] = ny;
+}
+
+/* sci_restrict_w2_kernel_mod.F90 restrict_w2_code_r_double (with_b = 1) and
+ * sci_restrict_w2h_kernel_mod.F90 restrict_w2h_code_r_double (with_b = 0) */
+#define DEF_RESTRICT_W2(T, SFX)                                                       \
+  void ora_restrict_w2_code_##SFX(int nlayers, const int* cell_map, int nx, int ny,   \
+                                  int ncell_fine, T* coarse, const T* fine,           \
+                                  const int* sel_ew, const int* sel_ns,               \
+                                  const int* map_coarse, int ndf,                     \
+                                  const int* map_fine, const int* map_w3_2d,          \
+                                  int with_b, T* work) {                              \
+    (void)ncell_fine;                                                                 \
+    int xs[5], xe[5], ys[5], ye[5];                                                   \
+    ora_w2_face_ranges(nx, ny, xs, xe, ys, ye);                                       \
+    const int ew = V(sel_ew, V(map_w3_2d, 1)), ns = V(sel_ns, V(map_w3_2d, 1));       \
+    for (int face = 1; face <= ew + ns; ++face) {                                     \
+      int df = face;                                                                  \
+      if (face == 3 && ns == 2 && ew == 1) df = ORA_N;                                \
+      for (int k = 0; k < nlayers; ++k) work[k] = (T)0;                               \
+      for (int y = ys[df]; y <= ye[df]; ++y)                                          \
+        for (int x = xs[df]; x <= xe[df]; ++x)                                        \
+          for (int k = 0; k < nlayers; ++k)                                           \
+            work[k] = work[k] +                                                       \
+                V(fine, A2(map_fine, df, A2(cell_map, x, y, nx), ndf) + k);           \
+      for (int k = 0; k < nlayers; ++k) V(coarse, V(map_coarse, df) + k) = work[k];   \
+    }                                                                                 \
+    if (!with_b) return;                                                              \
+    for (int k = 0; k <= nlayers; ++k) work[k] = (T)0;                                \
+    for (int y = 1; y <= ny; ++y)                                                     \
+      for (int x = 1; x <= nx; ++x)                                                   \
+        for (int k = 0; k <= nlayers; ++k)                                            \
+          work[k] = work[k] + V(fine, A2(map_fine, ORA_B, A2(cell_map, x, y, nx), ndf) + k); \
+    for (int k = 0; k <= nlayers; ++k) V(coarse, V(map_coarse, ORA_B) + k) = work[k]; \
+  }
+DEF_RESTRICT_W2(double, r_double)
+DEF_RESTRICT_W2(float, r_single)
+
+/* sci_restrict_w2v_kernel_mod.F90 restrict_w2v_code_r_double: the B column (df 1) */
+#define DEF_RESTRICT_W2V(T, SFX)                                                      \
+  void ora_restrict_w2v_code_##SFX(int nlayers, const int* cell_map, int nx, int ny,  \
+                                   int ncell_fine, T* coarse, const T* fine,          \
+                                   const int* map_coarse, int ndf,                    \
+                                   const int* map_fine, T* work) {                    \
+    (void)ncell_fine;                                                                 \
+    for (int k = 0; k <= nlayers; ++k) work[k] = (T)0;                                \
+    for (int y = 1; y <= ny; ++y)                                                     \
+      for (int x = 1; x <= nx; ++x)                                                   \
+        for (int k = 0; k <= nlayers; ++k)                                            \
+          work[k] = work[k] + V(fine, A2(map_fine, 1, A2(cell_map, x, y, nx), ndf) + k); \
+    for (int k = 0; k <= nlayers; ++k) V(coarse, V(map_coarse, 1) + k) = work[k];     \
+  }
+DEF_RESTRICT_W2V(double, r_double)
+DEF_RESTRICT_W2V(float, r_single)
+
+/* sci_weights_prolong_w2_kernel_mod.F90 weights_prolong_w2_kernel_code */
+void ora_weights_prolong_w2_code(int nlayers, const int* cell_map, int nx, int ny,
+                                 int ncell_fine, double* w, int ndf, const int* map_fine) {
+  (void)ncell_fine;
+#define WF(df, x, y, k) V(w, A2(map_fine, df, A2(cell_map, x, y, nx), ndf) + (k))
+  for (int k = 0; k < nlayers; ++k) {
+    for (int x = 1; x <= nx; ++x) {
+      WF(ORA_N, x, 1, k) = 1.0 / (double)nx;
+      WF(ORA_S, x, ny, k) = 1.0 / (double)nx;
+    }
+    for (int y = 1; y <= ny; ++y) {
+      WF(ORA_W, 1, y, k) = 1.0 / (double)ny;
+      WF(ORA_E, nx, y, k) = 1.0 / (double)ny;
+    }
+    for (int y = 1; y <= ny; ++y)
+      for (int x = 2; x <= nx; ++x) WF(ORA_W, x, y, k) = (double)(nx + 1 - x) / (double)nx;
+    for (int x = 1; x <= nx; ++x)
+      for (int y = 2; y <= ny; ++y) WF(ORA_N, x, y, k) = (double)(ny + 1 - y) / (double)ny;
+  }
+  for (int k = 0; k <= nlayers; ++k)
+    for (int y = 1; y <= ny; ++y)
+      for (int x = 1; x <= nx; ++x) WF(ORA_B, x, y, k) = 1.0 / (double)(nx * ny);
+#undef WF
+}
+
+/* sci_prolong_w2_kernel_mod.F90 prolong_w2_kernel_code */
+void ora_prolong_w2_code(int nlayers, const int* cell_map, int nx, int ny, int ncell_fine,
+                         double* fine, const double* coarse, const double* w, int ndf,
+                         const int* map_fine, const int* map_coarse) {
+  (void)ncell_fine;
+#define FI(df, x, y, k) (A2(map_fine, df, A2(cell_map, x, y, nx), ndf) + (k))
+#define CO(df, k) V(coarse, V(map_coarse, df) + (k))
+  for (int k = 0; k < nlayers; ++k) {
+    for (int x = 1; x <= nx; ++x) {
+      V(fine, FI(ORA_N, x, 1, k)) = V(w, FI(ORA_N, x, 1, k)) * CO(ORA_N, k);
+      V(fine, FI(ORA_S, x, ny, k)) = V(w, FI(ORA_S, x, ny, k)) * CO(ORA_S, k);
+    }
+    for (int y = 1; y <= ny; ++y) {
+      V(fine, FI(ORA_W, 1, y, k)) = V(w, FI(ORA_W, 1, y, k)) * CO(ORA_W, k);
+      V(fine, FI(ORA_E, nx, y, k)) = V(w, FI(ORA_E, nx, y, k)) * CO(ORA_E, k);
+    }
+    for (int y = 1; y <= ny; ++y) {
+      const double ew = V(w, FI(ORA_W, 1, y, k));
+      for (int x = 2; x <= nx; ++x) {
+        const double iw = V(w, FI(ORA_W, x, y, k));
+        V(fine, FI(ORA_W, x, y, k)) = ew * (iw * CO(ORA_W, k) + (1.0 - iw) * CO(ORA_E, k));
+      }
+    }
+    for (int x = 1; x <= nx; ++x) {
+      const double ew = V(w, FI(ORA_N, x, 1, k));
+      for (int y = 2; y <= ny; ++y) {
+        const double iw = V(w, FI(ORA_N, x, y, k));
+        V(fine, FI(ORA_N, x, y, k)) = ew * (iw * CO(ORA_N, k) + (1.0 - iw) * CO(ORA_S, k));
+      }
+    }
+  }
+  for (int y = 1; y <= ny; ++y)
+    for (int x = 1; x <= nx; ++x)
+      for (int k = 0; k <= nlayers; ++k)
+        V(fine, FI(ORA_B, x, y, k)) = V(w, FI(ORA_B, x, y, k)) * CO(ORA_B, k);
+#undef FI
+#undef CO
+}

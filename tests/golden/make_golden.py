@@ -226,6 +226,135 @@ def main(ref: Path) -> None:
         "tol": tol_literal(asm),
     })
 
+    # ------------------------------------------------ W2 intergrid KATs
+    im2 = ref / UT / "inter_mesh"
+
+    def int_list(text, lhs):
+        m = re.search(lhs + r"\s*=\s*(?:reshape\(\s*)?\(/(.*?)/\)", text, re.S)
+        return [int(v) for v in m.group(1).replace("&", " ").split(",")]
+
+    def fields_w2(t, nl, nx, ny, map_f, undf_f, with_b, with_t):
+        # the fine-field loop of restrict_w2{,h}_kernel_mod_test.pf: W of the
+        # first column, E of the last, N of the first row, S of the last,
+        # B (and T on the top layer) everywhere; -100 on faces not read
+        f = np.zeros(undf_f)
+        for k in range(nl):
+            for x in range(1, nx + 1):
+                for y in range(1, ny + 1):
+                    c = x + nx * (y - 1)
+                    m = map_f[c - 1]
+                    if x == 1:
+                        f[m[0] + k - 1] = y + k
+                    elif x == nx:
+                        f[m[2] + k - 1] = y + k + 1
+                    else:
+                        f[m[0] + k - 1] = f[m[2] + k - 1] = -100.0
+                    if y == 1:
+                        f[m[3] + k - 1] = x + k
+                    elif y == ny:
+                        f[m[1] + k - 1] = x + k + 1
+                    else:
+                        f[m[3] + k - 1] = f[m[1] + k - 1] = -100.0
+                    if with_b:
+                        f[m[4] + k - 1] = y + k
+                        if with_t and k == nl - 1:
+                            f[m[5] + k - 1] = x + k
+        return f
+
+    kat = {}
+    for name, ndf, with_b in (("restrict_w2", 6, True), ("restrict_w2h", 4, False)):
+        t = _source(im2 / f"{name}_kernel_mod_test.pf")
+        nl, nx, ny = int(scalar(t, "nlayers")), int(scalar(t, "ncell_f_per_c_x")), \
+            int(scalar(t, "ncell_f_per_c_y"))
+        mf = np.array(int_list(t, "map_f")).reshape(nx * ny, ndf)
+        mc = int_list(t, "map_c")
+        undf_f, undf_c = int(scalar(t, "undf_f")), int(scalar(t, "undf_c"))
+        fine = fields_w2(t, nl, nx, ny, mf, undf_f, with_b, with_b)
+        ans = np.zeros(undf_c)
+        for k in range(nl):   # the test's answer loop
+            ans[mc[0] + k - 1] = 6 + 3 * k
+            ans[mc[1] + k - 1] = 5 + 2 * k
+            ans[mc[2] + k - 1] = 9 + 3 * k
+            ans[mc[3] + k - 1] = 3 + 2 * k
+            if with_b:
+                ans[mc[4] + k - 1] = 12 + 6 * k
+                if k == nl - 1:
+                    ans[mc[5] + k - 1] = 9 + 6 * k
+        kat[name] = dict(nlayers=nl, nx=nx, ny=ny, ndf=ndf, map_f=mf.tolist(), map_c=mc,
+                         face_selector=2, fine=fine.tolist(), answer=ans.tolist())
+    t = _source(im2 / "restrict_w2v_kernel_mod_test.pf")
+    nl, nx, ny = 3, int(scalar(t, "ncell_f_per_c_x")), int(scalar(t, "ncell_f_per_c_y"))
+    mf = np.array(int_list(t, "map_f")).reshape(nx * ny, 2)
+    mc = int_list(t, "map_c")
+    fine = np.zeros(nx * ny * (nl + 1))
+    for k in range(nl):
+        for x in range(1, nx + 1):
+            for y in range(1, ny + 1):
+                c = x + nx * (y - 1)
+                fine[mf[c - 1][0] + k - 1] = y + k
+                if k == nl - 1:
+                    fine[mf[c - 1][1] + k - 1] = x + k
+    ans = np.zeros(nl + 1)
+    for k in range(nl):
+        ans[mc[0] + k - 1] = 12 + 6 * k
+        if k == nl - 1:
+            ans[mc[1] + k - 1] = 9 + 6 * k
+    kat["restrict_w2v"] = dict(nlayers=nl, nx=nx, ny=ny, ndf=2, map_f=mf.tolist(), map_c=mc,
+                               fine=fine.tolist(), answer=ans.tolist())
+    for name in ("prolong_w2", "weights_prolong_w2"):
+        t = _source(im2 / f"{name}_kernel_mod_test.pf")
+        nl, nx, ny = 3, int(scalar(t, "ncell_f_per_c_x")), int(scalar(t, "ncell_f_per_c_y"))
+        mf = np.array(int_list(t, "map_f")).reshape(nx * ny, 6)
+        mc = int_list(t, "map_c")
+        undf_f, undf_c = int(scalar(t, "undf_f")), int(scalar(t, "undf_c"))
+        coarse = np.zeros(undf_c)
+        w = np.zeros(undf_f)
+        ans = np.zeros(undf_f)
+        for k in range(nl):   # the tests' coarse field, weights and answers
+            coarse[mc[0] + k - 1] = 6 + 3 * k
+            coarse[mc[1] + k - 1] = 5 + 2 * k
+            coarse[mc[2] + k - 1] = 9 + 3 * k
+            coarse[mc[3] + k - 1] = 3 + 2 * k
+            coarse[mc[4] + k - 1] = 12 + 6 * k
+            if k == nl - 1:
+                coarse[mc[5] + k - 1] = 9 + 6 * k
+            for x in range(1, nx + 1):
+                for y in range(1, ny + 1):
+                    m = mf[x + nx * (y - 1) - 1]
+                    P = name == "prolong_w2"
+                    if x == 1:
+                        ans[m[0] + k - 1] = (2 + k) if P else 1.0 / ny
+                        w[m[0] + k - 1] = 1.0 / ny
+                        ans[m[2] + k - 1] = (2.5 + k) if P else 0.5
+                        w[m[2] + k - 1] = 0.5
+                    elif x == nx:
+                        ans[m[2] + k - 1] = (3 + k) if P else 1.0 / ny
+                        w[m[2] + k - 1] = 1.0 / ny
+                    if y == 1:
+                        ans[m[3] + k - 1] = (1.5 + k) if P else 1.0 / nx
+                        w[m[3] + k - 1] = 1.0 / nx
+                    elif y == ny:
+                        ans[m[1] + k - 1] = (2.5 + k) if P else 1.0 / nx
+                        w[m[1] + k - 1] = 1.0 / nx
+                    else:
+                        ans[m[1] + k - 1] = (13.0 / 6.0 + k) if P else 1.0 / 3.0
+                        ans[m[3] + k - 1] = (11.0 / 6.0 + k) if P else 2.0 / 3.0
+                        w[m[3] + k - 1] = 2.0 / 3.0
+                        w[m[1] + k - 1] = 1.0 / 3.0
+                    ans[m[4] + k - 1] = (2 + k) if P else 1.0 / (nx * ny)
+                    w[m[4] + k - 1] = 1.0 / (nx * ny)
+                    if k == nl - 1:
+                        ans[m[5] + k - 1] = 3.5 if P else 1.0 / (nx * ny)
+                        w[m[5] + k - 1] = 1.0 / (nx * ny)
+        kat[name] = dict(nlayers=nl, nx=nx, ny=ny, ndf=6, map_f=mf.tolist(), map_c=mc,
+                         coarse=coarse.tolist(), weights=w.tolist(), answer=ans.tolist())
+    t = _source(im2 / "restrict_w2_kernel_mod_test.pf")
+    write("w2_intergrid_kat.json", {
+        "source": [f"{UT}/inter_mesh/{n}_kernel_mod_test.pf" for n in
+                   ("restrict_w2", "restrict_w2h", "restrict_w2v", "prolong_w2",
+                    "weights_prolong_w2")],
+        "tol": tol_literal(t), **kat})
+
     # ------------------------------------------------------- intergrid KATs
     im = ref / UT / "inter_mesh"
     kats = {}

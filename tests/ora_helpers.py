@@ -321,3 +321,60 @@ def cma_dense(cm, p, cell=0):
         for j in range(max(1, jm), min(p["ncol"], jp) + 1):
             D[i - 1, j - 1] = cm[j - jm, i - 1, cell]
     return D
+
+
+# ------------------------------------------------------- W2 intergrid drivers
+def _cellmap(nx, ny):
+    """cell_map(x, y) = x + (y-1) nx of the reference tests, Fortran order."""
+    return np.asfortranarray(np.array([[x + (y - 1) * nx for y in range(1, ny + 1)]
+                                       for x in range(1, nx + 1)], dtype=np.int32))
+
+
+def w2_restrict(kind, nl, nx, ny, map_f, map_c, fine, undf_c, sel_ew=2, sel_ns=2,
+                dtype=np.float64, cell_map=None):
+    """restrict_w2 / restrict_w2h / restrict_w2v over one coarse cell; maps
+    1-based, map_f (ncell_f, ndf) and map_c (ndf,)."""
+    L = lib()
+    cm = _cellmap(nx, ny) if cell_map is None else np.asfortranarray(cell_map, np.int32)
+    mf = np.ascontiguousarray(map_f, dtype=np.int32)      # (ncell, ndf) == Fortran (ndf, ncell)
+    mc = np.ascontiguousarray(map_c, dtype=np.int32)
+    fine = np.ascontiguousarray(fine, dtype=dtype)
+    coarse = np.zeros(undf_c, dtype=dtype)
+    work = np.zeros(nl + 1, dtype=dtype)
+    sfx = _sfx(dtype)
+    ip = lambda a: a.ctypes.data_as(_ip)
+    if kind == "w2v":
+        getattr(L, f"ora_restrict_w2v_code_{sfx}")(nl, ip(cm), nx, ny, nx * ny, ptr(coarse),
+                                                   ptr(fine), ip(mc), mf.shape[1], ip(mf),
+                                                   ptr(work))
+    else:
+        ew, ns = np.array([sel_ew], np.int32), np.array([sel_ns], np.int32)
+        one = np.array([1], np.int32)
+        getattr(L, f"ora_restrict_w2_code_{sfx}")(nl, ip(cm), nx, ny, nx * ny, ptr(coarse),
+                                                  ptr(fine), ip(ew), ip(ns), ip(mc),
+                                                  mf.shape[1], ip(mf), ip(one),
+                                                  1 if kind == "w2" else 0, ptr(work))
+    return coarse
+
+
+def w2_weights(nl, nx, ny, map_f, undf_f, w0=None, cell_map=None):
+    L = lib()
+    cm = _cellmap(nx, ny) if cell_map is None else np.asfortranarray(cell_map, np.int32)
+    mf = np.ascontiguousarray(map_f, dtype=np.int32)
+    w = np.zeros(undf_f) if w0 is None else np.array(w0, dtype=np.float64)
+    L.ora_weights_prolong_w2_code(nl, cm.ctypes.data_as(_ip), nx, ny, nx * ny, ptr(w),
+                                  mf.shape[1], mf.ctypes.data_as(_ip))
+    return w
+
+
+def w2_prolong(nl, nx, ny, map_f, map_c, coarse, weights, fine0, cell_map=None):
+    L = lib()
+    cm = _cellmap(nx, ny) if cell_map is None else np.asfortranarray(cell_map, np.int32)
+    mf = np.ascontiguousarray(map_f, dtype=np.int32)
+    mc = np.ascontiguousarray(map_c, dtype=np.int32)
+    fine = np.array(fine0, dtype=np.float64)
+    L.ora_prolong_w2_code(nl, cm.ctypes.data_as(_ip), nx, ny, nx * ny, ptr(fine),
+                          ptr(np.ascontiguousarray(coarse, np.float64)),
+                          ptr(np.ascontiguousarray(weights, np.float64)), mf.shape[1],
+                          mf.ctypes.data_as(_ip), mc.ctypes.data_as(_ip))
+    return fine

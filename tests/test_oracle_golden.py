@@ -328,3 +328,30 @@ def test_cma_asm_m2v_lumped_inv(dtype):
     tol = 1e-14 if dtype == np.float64 else 1e-6
     assert np.allclose(cm[0, :, 0], want, rtol=tol, atol=0)
     assert not np.any(cm[1:, :, 0])
+
+
+# ------------------------------------------------- W2 intergrid transfers
+@pytest.mark.parametrize("name,dtype", [("restrict_w2", np.float64), ("restrict_w2", np.float32),
+                                        ("restrict_w2h", np.float64), ("restrict_w2v", np.float64),
+                                        ("restrict_w2v", np.float32)])
+def test_w2_restrict_kat(name, dtype):
+    # restrict_w2{,h,v}_kernel_mod_test.pf (one coarse cell of 2 x 3 fine cells)
+    g = load("w2_intergrid_kat.json")
+    k = g[name]
+    kind = {"restrict_w2": "w2", "restrict_w2h": "w2h", "restrict_w2v": "w2v"}[name]
+    got = oh.w2_restrict(kind, k["nlayers"], k["nx"], k["ny"], k["map_f"], k["map_c"],
+                         k["fine"], len(k["answer"]), dtype=dtype)
+    assert np.allclose(got, k["answer"], rtol=0, atol=g["tol"])
+
+
+def test_w2_weights_and_prolong_kat():
+    # weights_prolong_w2_kernel_mod_test.pf and prolong_w2_kernel_mod_test.pf
+    g = load("w2_intergrid_kat.json")
+    k = g["weights_prolong_w2"]
+    w = oh.w2_weights(k["nlayers"], k["nx"], k["ny"], k["map_f"], len(k["answer"]))
+    assert np.allclose(w, k["answer"], rtol=0, atol=g["tol"])
+    k = g["prolong_w2"]
+    assert np.allclose(w, k["weights"], rtol=0, atol=g["tol"])
+    fine = oh.w2_prolong(k["nlayers"], k["nx"], k["ny"], k["map_f"], k["map_c"], k["coarse"],
+                         k["weights"], np.zeros(len(k["answer"])))
+    assert np.allclose(fine, k["answer"], rtol=0, atol=g["tol"])
