@@ -247,6 +247,29 @@ def _true_residual(ctx, S, x64):
     return R.norm() / S.b64.norm()
 
 
+def test_mixed_parity_c96(ctx):
+    """The mixed solve on C96 x 70 (multigrid C96/48/24/12): the fine level
+    runs the TMA-staged substitutions (zero start and from x_in; the
+    prolongation-corrected post-smoother per column), the coarse levels the
+    segmented sweep; against the oracle's mixed solve."""
+    p = helmholtz_problem(96, 70, seed=3, mg_levels=4)
+    ora = OraHelm(p)
+    x_ref, st_ref, mi = ora.mixed_solve(p.rhs, tol=1e-8, inner_tol=1e-4, inner_max_iter=2)
+    S = api.HelmholtzSystem(ctx, p, fp64=True)
+    res = S.solve_mixed(p.rhs)
+    assert res.status == st_ref == 0
+    assert res.outer_iterations == mi.outer_iterations
+    assert rel(S.solution(), x_ref) < 1e-7
+    r = p.rhs - ora.apply(S.solution())
+    assert np.linalg.norm(r) / np.linalg.norm(p.rhs) <= 1e-8
+    # FP64 GCR + MG at the same size against the oracle (per-column FP64 kernels)
+    x64, st64, info = ora.gcr_mg_solve(p.rhs, gcrk=10, r_tol=1e-8, max_iter=20)
+    r64 = S.solve_fp64(p.rhs)
+    assert r64.status == st64 == 0 and r64.iterations == info.iterations
+    assert rel(S.solution(), x64) < 1e-12
+    ctx.synchronize()
+
+
 def test_full_size_fp64_and_mixed(ctx, helm192):
     """C192 x 70: both solves reach 1e-8 in the true FP64 residual; repeated
     solves are bit-identical (deterministic reductions); mixed agrees with
