@@ -46,6 +46,7 @@ def parse():
     ap.add_argument("--n", type=int, default=N_FINE, help=argparse.SUPPRESS)
     # profiling aids: only the batched workload, at a chosen size and launch shape
     ap.add_argument("--batched-only", action="store_true", help=argparse.SUPPRESS)
+    ap.add_argument("--kernels", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--batch-rhs", type=int, default=64, help=argparse.SUPPRESS)
     ap.add_argument("--batch-uneven", type=int, default=32, help=argparse.SUPPRESS)
     ap.add_argument("--batch-shape", type=int, nargs=2, default=(0, 0), help=argparse.SUPPRESS)
@@ -274,6 +275,99 @@ def measure_batched(ctx, stream, steps: int, warmup: int, n_rhs: int = 64, n_une
     }
 
 
+def measure_kernels(ctx, stream, peak: float) -> list:
+    """Every hot-path kernel timed alone (CUDA events on the library's
+    stream, 3 warm-up + 20 timed launches, inputs larger than L2 where the
+    workload allows) against its algorithmic bytes: each array read once
+    and written once at its stored precision."""
+    import torch
+    from lfric_core_b200 import api
+    from lfric_core_b200.api import R_DOUBLE, R_SINGLE, Field
+    from lfric_core_b200.problems import helmholtz_problem, w0_problem
+    rows = []
+
+    def time(fn, n=20):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    def add(name, workload, nbytes, ms):
+        gbs = nbytes / (ms * 1e-3) / 1e9
+        rows.append({"kernel": name, "workload": workload, "algorithmic_bytes": nbytes,
+                     "us": ms * 1e3, "GB/s": gbs, "frac_of_measured_hbm": gbs / peak})
+
+    prob = helmholtz_problem(N_FINE, NLAYERS, seed=SEED, mg_levels=2)
+    N = prob.ndof
+    mesh = api.Mesh(ctx, prob.links)
+    for kind, w, tag in ((R_SINGLE, 4, "FP32"), (R_DOUBLE, 8, "FP64")):
+        H = api.Helmholtz(ctx, kind, mesh, NLAYERS, prob.cm, prob.hf)
+        x, b, y = H.field(), H.field(), H.field()
+        x.import_(prob.rhs)
+        b.import_(prob.rhs)
+        wl = f"C{N_FINE}x{NLAYERS} {tag}"
+        add("k_helm_apply (y = A x)", wl, 9 * N * w, time(lambda: H.apply(y, x)))
+        add("substitution from zero (k_subst_tma / k_helm_subst)", wl, 5 * N * w,
+            time(lambda: H.smooth(0.8, None, b, y)))
+        add("smoother sweep (k_helm_rhs + substitution)", wl, 13 * N * w,
+            time(lambda: H.smooth(0.8, x, b, y)))
+        add("k_axpy (y = y + a x)", wl, 3 * N * w, time(lambda: y.axpy(0.5, x)))
+        add("k_axpby (z = a x + b y)", wl, 3 * N * w, time(lambda: y.axpby(0.5, x, 0.25, b)))
+        add("k_dot (<x, y>, FP64 accumulation)", wl, 2 * N * w, time(lambda: x.dot(b)))
+        del H, x, b, y
+    # intergrid C192 -> C96 (FP64): restrict_mass_w3 and prolong_scalar_unweighted
+    ig = api.Intergrid(ctx, prob.mg_child[0], prob.ncol)
+    nc = prob.mg_child[0].shape[0]
+    F = Field(ctx, R_DOUBLE, prob.ncol, NLAYERS)
+    Cc = Field(ctx, R_DOUBLE, nc, NLAYERS)
+    F.set_scalar(1.0)
+    Cc.set_scalar(1.0)
+    add("k_restrict (restrict_mass_w3)", f"C{N_FINE}->C{N_FINE // 2}x{NLAYERS} FP64",
+        (N + nc * NLAYERS) * 8, time(lambda: ig.restrict(api.RESTRICT_MASS_W3, Cc, F)))
+    add("k_prolong (prolong_scalar_unweighted)", f"C{N_FINE // 2}->C{N_FINE}x{NLAYERS} FP64",
+        (2 * N + nc * NLAYERS) * 8, time(lambda: ig.prolong(F, Cc)))
+    # CMA tridiagonal on C96 x 70 (W3 -> W3): app and appinv
+    n96 = 6 * 96 * 96
+    rng = np.random.default_rng(2)
+    sub = -rng.random((n96, NLAYERS))
+    sup = -rng.random((n96, NLAYERS))
+    diag = (np.abs(sub) + np.abs(sup)) * (1.5 + 1.5 * rng.random((n96, NLAYERS)))
+    cm = np.stack([sub, diag, sup], axis=-1).ravel()
+    ind = np.arange(1, NLAYERS + 1)
+    for kind, w, tag in ((R_DOUBLE, 8, "FP64"), (R_SINGLE, 4, "FP32")):
+        A = api.ColumnwiseOperator(ctx, kind, n96, NLAYERS, NLAYERS, 3, 1, 1, 1, 1, ind, ind, cm)
+        X = Field(ctx, kind, n96, NLAYERS)
+        Y = Field(ctx, kind, n96, NLAYERS)
+        X.set_scalar(1.0)
+        Y.set_scalar(0.0)
+        n = n96 * NLAYERS
+        add("k_cma_app (columnwise_op_app)", f"C96x{NLAYERS} {tag}", 6 * n * w,
+            time(lambda: A.apply(Y, X)))
+        add("k_thomas (columnwise_op_appinv)", f"C96x{NLAYERS} {tag}", 5 * n * w,
+            time(lambda: A.apply_inverse(Y, X)))
+        del A, X, Y
+    # LMA W0 apply (matrix_vector, gather form) on the C48 x 30 W0 problem
+    wp = w0_problem(48, 30, seed=4, top=30e3)
+    L = api.LocalOperator(ctx, R_DOUBLE, wp.ncell, wp.nlayers, wp.matrix(), wp.map, wp.nvert,
+                          wp.nlayers + 1)
+    X = Field(ctx, R_DOUBLE, wp.nvert, wp.nlayers + 1)
+    Y = Field(ctx, R_DOUBLE, wp.nvert, wp.nlayers + 1)
+    X.set_scalar(1.0)
+    Y.set_scalar(0.0)
+    ncell3 = wp.ncell * wp.nlayers
+    add("k_lma_apply (matrix_vector, gather)", "C48x30 W0 FP64",
+        (64 * ncell3 + 3 * wp.ndof) * 8, time(lambda: L.apply(api.LMA_INC, Y, X)))
+    add("k_lma_apply_t (transpose_matrix_vector)", "C48x30 W0 FP64",
+        (64 * ncell3 + 3 * wp.ndof) * 8, time(lambda: L.apply(api.LMA_TRANSPOSE, Y, X)))
+    return rows
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -293,6 +387,19 @@ def main():
 
     from lfric_core_b200 import api
     from lfric_core_b200.problems import helmholtz_problem
+
+    if args.kernels:
+        ctx = api.Context(dev)
+        stream = torch.cuda.Stream()
+        torch.cuda.set_stream(stream)
+        ctx.set_stream(stream.cuda_stream)
+        peak, kind = measured_hbm_peak()
+        rows = measure_kernels(ctx, stream, peak)
+        if rank == 0:
+            print(json.dumps({"kernels": rows, "peak_GB/s": peak, "peak_source": kind}),
+                  flush=True)
+        ctx.close()
+        return
 
     if args.batched_only:
         ctx = api.Context(dev)

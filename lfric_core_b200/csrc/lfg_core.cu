@@ -34,13 +34,92 @@ void upload(void* d, const void* h, size_t bytes) {
 }
 
 // ------------------------------------------------------------ kernels
+// The vector algebra streams its arrays in 16-byte packs (4 floats or 2
+// doubles per load) when every pointer is 16-byte aligned, so each load
+// instruction moves four times the bytes of a scalar FP32 load; a scalar
+// tail (and the scalar path for unaligned views) covers the rest.  Each
+// kernel is an element operation applied to W consecutive elements; the
+// scalars (Sc) are evaluated once per thread.
+template <class T, int W>
+struct Pack {
+  T e[W];
+  __device__ __forceinline__ static Pack load(const T* p) {
+    Pack r;
+    if constexpr (W * sizeof(T) == 16) {
+      const uint4 q = *reinterpret_cast<const uint4*>(p);
+      memcpy(r.e, &q, 16);
+    } else {
+#pragma unroll
+      for (int i = 0; i < W; ++i) r.e[i] = p[i];
+    }
+    return r;
+  }
+  __device__ __forceinline__ void store(T* p) const {
+    if constexpr (W * sizeof(T) == 16) {
+      uint4 q;
+      memcpy(&q, e, 16);
+      *reinterpret_cast<uint4*>(p) = q;
+    } else {
+#pragma unroll
+      for (int i = 0; i < W; ++i) p[i] = e[i];
+    }
+  }
+};
+
 template <class T>
-__global__ void k_set(T* __restrict__ x, size_t n, Sc a) {
-  const T v = (T)sc_eval(a);
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x)
-    x[i] = v;
+constexpr int kVec = 16 / (int)sizeof(T);
+
+inline bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15u) == 0; }
+
+// Applies op over [0, n): packs of W = 16 / sizeof(T) elements, then the tail.
+template <class T, class Op>
+__device__ __forceinline__ void for_each_pack(const Op& op, size_t n, bool vec, double& acc) {
+  const size_t tid = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+  const size_t st = (size_t)gridDim.x * blockDim.x;
+  size_t i0 = 0;
+  if (vec) {
+    constexpr int W = kVec<T>;
+    const size_t nv = n / W;
+    for (size_t j = tid; j < nv; j += st) op.template run<W>(j * W, acc);
+    i0 = nv * W;
+  }
+  for (size_t i = i0 + tid; i < n; i += st) op.template run<1>(i, acc);
 }
+
+template <class T, class Op>
+__global__ void k_ew(Op op, size_t n, bool vec) {
+  double acc = 0.0;
+  const auto b = op.bind();
+  for_each_pack<T>(b, n, vec, acc);
+}
+
+template <class T, class Op>
+__global__ void k_ewr(Op op, size_t n, bool vec, Red r) {
+  double acc = 0.0;
+  const auto b = op.bind();
+  for_each_pack<T>(b, n, vec, acc);
+  red_finish(r, acc);
+}
+
+#define LFG_PACK(T, W, name, ptr, i) const Pack<T, W> name = Pack<T, W>::load((ptr) + (i))
+
+// X = c
+template <class T>
+struct SetOp {
+  T* x;
+  Sc a;
+  struct B {
+    T* x;
+    T v;
+    template <int W> __device__ void run(size_t i, double&) const {
+      Pack<T, W> o;
+#pragma unroll
+      for (int q = 0; q < W; ++q) o.e[q] = v;
+      o.store(x + i);
+    }
+  };
+  __device__ B bind() const { return B{x, (T)sc_eval(a)}; }
+};
 
 template <class TO, class TI>
 __global__ void k_copy(TO* __restrict__ y, const TI* __restrict__ x, size_t n) {
@@ -48,6 +127,21 @@ __global__ void k_copy(TO* __restrict__ y, const TI* __restrict__ x, size_t n) {
        i += (size_t)gridDim.x * blockDim.x)
     y[i] = (TO)x[i];
 }
+
+// Y = X, same kind
+template <class T>
+struct CopyOp {
+  T* y;
+  const T* x;
+  struct B {
+    T* y;
+    const T* x;
+    template <int W> __device__ void run(size_t i, double&) const {
+      Pack<T, W>::load(x + i).store(y + i);
+    }
+  };
+  __device__ B bind() const { return B{y, x}; }
+};
 
 // X = X + b Y   (inc_X_plus_bY); Y may be of another kind (r_def += r_solver,
 // sci_psykal_light_mod.f90:218-265), the product is then formed in X's kind.
@@ -59,33 +153,91 @@ __global__ void k_axpy(T* __restrict__ x, const TY* __restrict__ y, size_t n, Sc
     x[i] = x[i] + bv * (T)y[i];
 }
 
+template <class T>
+struct AxpyOp {  // X = X + b Y, same kind
+  T* x;
+  const T* y;
+  Sc b;
+  struct B {
+    T* x;
+    const T* y;
+    T bv;
+    template <int W> __device__ void run(size_t i, double&) const {
+      LFG_PACK(T, W, xv, x, i);
+      LFG_PACK(T, W, yv, y, i);
+      Pack<T, W> o;
+#pragma unroll
+      for (int q = 0; q < W; ++q) o.e[q] = xv.e[q] + bv * yv.e[q];
+      o.store(x + i);
+    }
+  };
+  __device__ B bind() const { return B{x, y, (T)sc_eval(b)}; }
+};
+
 // X = a X + Y   (inc_aX_plus_Y)
 template <class T>
-__global__ void k_aypx(T* __restrict__ x, const T* __restrict__ y, size_t n, Sc a) {
-  const T av = (T)sc_eval(a);
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x)
-    x[i] = av * x[i] + y[i];
-}
+struct AypxOp {
+  T* x;
+  const T* y;
+  Sc a;
+  struct B {
+    T* x;
+    const T* y;
+    T av;
+    template <int W> __device__ void run(size_t i, double&) const {
+      LFG_PACK(T, W, xv, x, i);
+      LFG_PACK(T, W, yv, y, i);
+      Pack<T, W> o;
+#pragma unroll
+      for (int q = 0; q < W; ++q) o.e[q] = av * xv.e[q] + yv.e[q];
+      o.store(x + i);
+    }
+  };
+  __device__ B bind() const { return B{x, y, (T)sc_eval(a)}; }
+};
 
 // Z = a X + b Y   (aX_plus_bY)
 template <class T>
-__global__ void k_axpby(T* __restrict__ z, const T* __restrict__ x, const T* __restrict__ y,
-                        size_t n, Sc a, Sc b) {
-  const T av = (T)sc_eval(a), bv = (T)sc_eval(b);
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x)
-    z[i] = av * x[i] + bv * y[i];
-}
+struct AxpbyOp {
+  T* z;
+  const T* x;
+  const T* y;
+  Sc a, b;
+  struct B {
+    T* z;
+    const T* x;
+    const T* y;
+    T av, bv;
+    template <int W> __device__ void run(size_t i, double&) const {
+      LFG_PACK(T, W, xv, x, i);
+      LFG_PACK(T, W, yv, y, i);
+      Pack<T, W> o;
+#pragma unroll
+      for (int q = 0; q < W; ++q) o.e[q] = av * xv.e[q] + bv * yv.e[q];
+      o.store(z + i);
+    }
+  };
+  __device__ B bind() const { return B{z, x, y, (T)sc_eval(a), (T)sc_eval(b)}; }
+};
 
 // X = a X   (inc_a_times_X)
 template <class T>
-__global__ void k_scale(T* __restrict__ x, size_t n, Sc a) {
-  const T av = (T)sc_eval(a);
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x)
-    x[i] = av * x[i];
-}
+struct ScaleOp {
+  T* x;
+  Sc a;
+  struct B {
+    T* x;
+    T av;
+    template <int W> __device__ void run(size_t i, double&) const {
+      LFG_PACK(T, W, xv, x, i);
+      Pack<T, W> o;
+#pragma unroll
+      for (int q = 0; q < W; ++q) o.e[q] = av * xv.e[q];
+      o.store(x + i);
+    }
+  };
+  __device__ B bind() const { return B{x, (T)sc_eval(a)}; }
+};
 
 // Z = X / Y   (X_divideby_Y)
 template <class T>
@@ -98,106 +250,177 @@ __global__ void k_divide(T* __restrict__ z, const T* __restrict__ x, const T* __
 
 // <X, Y> accumulated in double
 template <class T>
-__global__ void k_dot(const T* __restrict__ x, const T* __restrict__ y, size_t n, Red r) {
-  double acc = 0.0;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x)
-    acc += (double)x[i] * (double)y[i];
-  red_finish(r, acc);
-}
+struct DotOp {
+  const T* x;
+  const T* y;
+  struct B {
+    const T* x;
+    const T* y;
+    template <int W> __device__ void run(size_t i, double& acc) const {
+      LFG_PACK(T, W, xv, x, i);
+      LFG_PACK(T, W, yv, y, i);
+#pragma unroll
+      for (int q = 0; q < W; ++q) acc += (double)xv.e[q] * (double)yv.e[q];
+    }
+  };
+  __device__ B bind() const { return B{x, y}; }
+};
 
 // Modified Gram-Schmidt step of gcr_solve (sci_iterative_solver_mod.f90:1358-1362)
 // fused with the next inner product: v -= a vj; pv -= a pvj; acc <v, next>
 // (next == null: <v, v>, the norm that follows the loop).
 template <class T>
-__global__ void k_mgs(T* __restrict__ v, T* __restrict__ pv, const T* __restrict__ vj,
-                      const T* __restrict__ pvj, const T* __restrict__ next, size_t n, Sc a,
-                      Red r) {
-  const T av = (T)sc_eval(a);
-  double acc = 0.0;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    const T vn = v[i] + av * vj[i];
-    v[i] = vn;
-    pv[i] = pv[i] + av * pvj[i];
-    const T w = next ? next[i] : vn;
-    acc += (double)vn * (double)w;
-  }
-  red_finish(r, acc);
-}
+struct MgsOp {
+  T* v;
+  T* pv;
+  const T* vj;
+  const T* pvj;
+  const T* next;
+  Sc a;
+  struct B {
+    T* v;
+    T* pv;
+    const T* vj;
+    const T* pvj;
+    const T* next;
+    T av;
+    template <int W> __device__ void run(size_t i, double& acc) const {
+      LFG_PACK(T, W, vv, v, i);
+      LFG_PACK(T, W, vjv, vj, i);
+      LFG_PACK(T, W, pvv, pv, i);
+      LFG_PACK(T, W, pvjv, pvj, i);
+      Pack<T, W> nv, np, w;
+#pragma unroll
+      for (int q = 0; q < W; ++q) {
+        nv.e[q] = vv.e[q] + av * vjv.e[q];
+        np.e[q] = pvv.e[q] + av * pvjv.e[q];
+      }
+      if (next) w = Pack<T, W>::load(next + i);
+      else w = nv;
+#pragma unroll
+      for (int q = 0; q < W; ++q) acc += (double)nv.e[q] * (double)w.e[q];
+      nv.store(v + i);
+      np.store(pv + i);
+    }
+  };
+  __device__ B bind() const { return B{v, pv, vj, pvj, next, (T)sc_eval(a)}; }
+};
 
 // v *= b; pv *= b; acc <res, v>   (gcr_solve :1363-1367)
 template <class T>
-__global__ void k_scale2_dot(T* __restrict__ v, T* __restrict__ pv, const T* __restrict__ res,
-                             size_t n, Sc b, Red r) {
-  const T bv = (T)sc_eval(b);
-  double acc = 0.0;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    const T vn = bv * v[i];
-    v[i] = vn;
-    pv[i] = bv * pv[i];
-    acc += (double)res[i] * (double)vn;
-  }
-  red_finish(r, acc);
-}
+struct Scale2DotOp {
+  T* v;
+  T* pv;
+  const T* res;
+  Sc b;
+  struct B {
+    T* v;
+    T* pv;
+    const T* res;
+    T bv;
+    template <int W> __device__ void run(size_t i, double& acc) const {
+      LFG_PACK(T, W, vv, v, i);
+      LFG_PACK(T, W, pvv, pv, i);
+      LFG_PACK(T, W, rv, res, i);
+      Pack<T, W> nv, np;
+#pragma unroll
+      for (int q = 0; q < W; ++q) {
+        nv.e[q] = bv * vv.e[q];
+        np.e[q] = bv * pvv.e[q];
+        acc += (double)rv.e[q] * (double)nv.e[q];
+      }
+      nv.store(v + i);
+      np.store(pv + i);
+    }
+  };
+  __device__ B bind() const { return B{v, pv, res, (T)sc_eval(b)}; }
+};
 
 // dx += a pv; res -= a v; acc <res, res>   (gcr_solve :1368-1374)
 template <class T>
-__global__ void k_update2_norm(T* __restrict__ dx, const T* __restrict__ pv,
-                               T* __restrict__ res, const T* __restrict__ v, size_t n, Sc a,
-                               Red r) {
-  const double ad = sc_eval(a);
-  const T ap = (T)ad, am = (T)(-ad);
-  double acc = 0.0;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    dx[i] = dx[i] + ap * pv[i];
-    const T rn = res[i] + am * v[i];
-    res[i] = rn;
-    acc += (double)rn * (double)rn;
+struct Update2NormOp {
+  T* dx;
+  const T* pv;
+  T* res;
+  const T* v;
+  Sc a;
+  struct B {
+    T* dx;
+    const T* pv;
+    T* res;
+    const T* v;
+    T ap, am;
+    template <int W> __device__ void run(size_t i, double& acc) const {
+      LFG_PACK(T, W, dv, dx, i);
+      LFG_PACK(T, W, pvv, pv, i);
+      LFG_PACK(T, W, rv, res, i);
+      LFG_PACK(T, W, vv, v, i);
+      Pack<T, W> nd, nr;
+#pragma unroll
+      for (int q = 0; q < W; ++q) {
+        nd.e[q] = dv.e[q] + ap * pvv.e[q];
+        nr.e[q] = rv.e[q] + am * vv.e[q];
+        acc += (double)nr.e[q] * (double)nr.e[q];
+      }
+      nd.store(dx + i);
+      nr.store(res + i);
+    }
+  };
+  __device__ B bind() const {
+    const double ad = sc_eval(a);
+    return B{dx, pv, res, v, (T)ad, (T)(-ad)};
   }
-  red_finish(r, acc);
-}
+};
 
-// x += b y; acc <x, x>
+// x += b y; acc <x, next> (next null: <x, x>)  (gmres/fgmres Arnoldi, and
+// the monitored residual update of bicgstab / jacobi)
 template <class T>
-__global__ void k_axpy_norm(T* __restrict__ x, const T* __restrict__ y, size_t n, Sc b,
-                            Red r) {
-  const T bv = (T)sc_eval(b);
-  double acc = 0.0;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    const T xn = x[i] + bv * y[i];
-    x[i] = xn;
-    acc += (double)xn * (double)xn;
-  }
-  red_finish(r, acc);
-}
-
-// x += b y; acc <x, next> (next null: <x, x>)  (gmres/fgmres Arnoldi)
-template <class T>
-__global__ void k_axpy_dot(T* __restrict__ x, const T* __restrict__ y,
-                           const T* __restrict__ next, size_t n, Sc b, Red r) {
-  const T bv = (T)sc_eval(b);
-  double acc = 0.0;
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x) {
-    const T xn = x[i] + bv * y[i];
-    x[i] = xn;
-    acc += (double)xn * (double)(next ? next[i] : xn);
-  }
-  red_finish(r, acc);
-}
+struct AxpyDotOp {
+  T* x;
+  const T* y;
+  const T* next;
+  Sc b;
+  struct B {
+    T* x;
+    const T* y;
+    const T* next;
+    T bv;
+    template <int W> __device__ void run(size_t i, double& acc) const {
+      LFG_PACK(T, W, xv, x, i);
+      LFG_PACK(T, W, yv, y, i);
+      Pack<T, W> o, w;
+#pragma unroll
+      for (int q = 0; q < W; ++q) o.e[q] = xv.e[q] + bv * yv.e[q];
+      if (next) w = Pack<T, W>::load(next + i);
+      else w = o;
+#pragma unroll
+      for (int q = 0; q < W; ++q) acc += (double)o.e[q] * (double)w.e[q];
+      o.store(x + i);
+    }
+  };
+  __device__ B bind() const { return B{x, y, next, (T)sc_eval(b)}; }
+};
 
 // dst = a src   (copy followed by inc_a_times_X)
 template <class T>
-__global__ void k_scale_copy(T* __restrict__ dst, const T* __restrict__ src, size_t n, Sc a) {
-  const T av = (T)sc_eval(a);
-  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
-       i += (size_t)gridDim.x * blockDim.x)
-    dst[i] = av * src[i];
-}
+struct ScaleCopyOp {
+  T* dst;
+  const T* src;
+  Sc a;
+  struct B {
+    T* dst;
+    const T* src;
+    T av;
+    template <int W> __device__ void run(size_t i, double&) const {
+      LFG_PACK(T, W, sv, src, i);
+      Pack<T, W> o;
+#pragma unroll
+      for (int q = 0; q < W; ++q) o.e[q] = av * sv.e[q];
+      o.store(dst + i);
+    }
+  };
+  __device__ B bind() const { return B{dst, src, (T)sc_eval(a)}; }
+};
 
 // Column-contiguous (e*nlev + k) <-> level-major (k*ncol + e) with kind
 // conversion, through 32x32 shared-memory tiles.
@@ -255,40 +478,64 @@ static void same_kind(lfg_field a, lfg_field b, const char* what) {
   LFG_REQUIRE(a->kind == b->kind, std::string(what) + ": fields differ in kind");
 }
 
+template <class T, class Op>
+void launch_ew(lfg_ctx c, const Op& op, size_t n, bool vec, const char* what) {
+  const size_t work = vec ? n / kVec<T> + n % kVec<T> : n;
+  k_ew<T, Op><<<occ_grid(c, (const void*)k_ew<T, Op>, kThreads, work), kThreads, 0, c->stream>>>(
+      op, n, vec);
+  after_launch(c, what);
+}
+
+template <class T, class Op>
+void launch_ewr(lfg_ctx c, const Op& op, size_t n, bool vec, int slot, const char* what) {
+  const size_t work = vec ? n / kVec<T> + n % kVec<T> : n;
+  // the reduction's partials live in kMaxRedBlocks slots per reduction
+  const int g = std::min(occ_grid(c, (const void*)k_ewr<T, Op>, kThreads, work), kMaxRedBlocks);
+  k_ewr<T, Op><<<g, kThreads, 0, c->stream>>>(op, n, vec, c->red(slot));
+  after_launch(c, what);
+}
+
+template <class... P>
+bool all_aligned(const P*... p) {
+  return (... && (p == nullptr || aligned16(p)));
+}
+
 void vec_set(lfg_field x, Sc a) {
   lfg_ctx c = x->ctx;
-  DISPATCH_KIND(x->kind, T,
-                k_set<T><<<c->stream_grid(x->n()), kThreads, 0, c->stream>>>((T*)x->d, x->n(), a));
-  after_launch(c, "set");
+  DISPATCH_KIND(x->kind, T, launch_ew<T>(c, SetOp<T>{(T*)x->d, a}, x->n(), all_aligned(x->d), "set"));
 }
 
 void vec_copy(lfg_field dst, lfg_field src) {
   same_shape(dst, src, "copy");
   lfg_ctx c = dst->ctx;
+  if (dst->kind == src->kind) {
+    DISPATCH_KIND(dst->kind, T,
+                  launch_ew<T>(c, CopyOp<T>{(T*)dst->d, (const T*)src->d}, dst->n(),
+                               all_aligned(dst->d, src->d), "copy"));
+    return;
+  }
   const int g = c->stream_grid(dst->n());
-  if (dst->kind == LFG_R_DOUBLE && src->kind == LFG_R_DOUBLE)
-    k_copy<double, double><<<g, kThreads, 0, c->stream>>>((double*)dst->d, (const double*)src->d, dst->n());
-  else if (dst->kind == LFG_R_DOUBLE)
+  if (dst->kind == LFG_R_DOUBLE)
     k_copy<double, float><<<g, kThreads, 0, c->stream>>>((double*)dst->d, (const float*)src->d, dst->n());
-  else if (src->kind == LFG_R_DOUBLE)
-    k_copy<float, double><<<g, kThreads, 0, c->stream>>>((float*)dst->d, (const double*)src->d, dst->n());
   else
-    k_copy<float, float><<<g, kThreads, 0, c->stream>>>((float*)dst->d, (const float*)src->d, dst->n());
+    k_copy<float, double><<<g, kThreads, 0, c->stream>>>((float*)dst->d, (const double*)src->d, dst->n());
   after_launch(c, "copy");
 }
 
 void vec_axpy(lfg_field x, Sc b, lfg_field y) {
   same_shape(x, y, "inc_X_plus_bY");
   lfg_ctx c = x->ctx;
-  const int g = c->stream_grid(x->n());
   if (x->kind == y->kind) {
     DISPATCH_KIND(x->kind, T,
-                  k_axpy<T, T><<<g, kThreads, 0, c->stream>>>((T*)x->d, (const T*)y->d, x->n(), b));
-  } else if (x->kind == LFG_R_DOUBLE) {
-    k_axpy<double, float><<<g, kThreads, 0, c->stream>>>((double*)x->d, (const float*)y->d, x->n(), b);
-  } else {
-    k_axpy<float, double><<<g, kThreads, 0, c->stream>>>((float*)x->d, (const double*)y->d, x->n(), b);
+                  launch_ew<T>(c, AxpyOp<T>{(T*)x->d, (const T*)y->d, b}, x->n(),
+                               all_aligned(x->d, y->d), "axpy"));
+    return;
   }
+  const int g = c->stream_grid(x->n());
+  if (x->kind == LFG_R_DOUBLE)
+    k_axpy<double, float><<<g, kThreads, 0, c->stream>>>((double*)x->d, (const float*)y->d, x->n(), b);
+  else
+    k_axpy<float, double><<<g, kThreads, 0, c->stream>>>((float*)x->d, (const double*)y->d, x->n(), b);
   after_launch(c, "axpy");
 }
 
@@ -296,8 +543,8 @@ void vec_aypx(lfg_field x, Sc a, lfg_field y) {
   same_kind(x, y, "inc_aX_plus_Y");
   lfg_ctx c = x->ctx;
   DISPATCH_KIND(x->kind, T,
-                k_aypx<T><<<c->stream_grid(x->n()), kThreads, 0, c->stream>>>((T*)x->d, (const T*)y->d, x->n(), a));
-  after_launch(c, "aypx");
+                launch_ew<T>(c, AypxOp<T>{(T*)x->d, (const T*)y->d, a}, x->n(),
+                             all_aligned(x->d, y->d), "aypx"));
 }
 
 void vec_axpby(lfg_field z, Sc a, lfg_field x, Sc b, lfg_field y) {
@@ -305,16 +552,14 @@ void vec_axpby(lfg_field z, Sc a, lfg_field x, Sc b, lfg_field y) {
   same_kind(z, y, "aX_plus_bY");
   lfg_ctx c = z->ctx;
   DISPATCH_KIND(z->kind, T,
-                k_axpby<T><<<c->stream_grid(z->n()), kThreads, 0, c->stream>>>(
-                    (T*)z->d, (const T*)x->d, (const T*)y->d, z->n(), a, b));
-  after_launch(c, "axpby");
+                launch_ew<T>(c, AxpbyOp<T>{(T*)z->d, (const T*)x->d, (const T*)y->d, a, b},
+                             z->n(), all_aligned(z->d, x->d, y->d), "axpby"));
 }
 
 void vec_scale(lfg_field x, Sc a) {
   lfg_ctx c = x->ctx;
   DISPATCH_KIND(x->kind, T,
-                k_scale<T><<<c->stream_grid(x->n()), kThreads, 0, c->stream>>>((T*)x->d, x->n(), a));
-  after_launch(c, "scale");
+                launch_ew<T>(c, ScaleOp<T>{(T*)x->d, a}, x->n(), all_aligned(x->d), "scale"));
 }
 
 void vec_divide(lfg_field z, lfg_field x, lfg_field y) {
@@ -331,9 +576,8 @@ void vec_dot(lfg_field x, lfg_field y, int slot) {
   same_kind(x, y, "X_innerproduct_Y");
   lfg_ctx c = x->ctx;
   DISPATCH_KIND(x->kind, T,
-                k_dot<T><<<c->stream_grid(x->n()), kThreads, 0, c->stream>>>(
-                    (const T*)x->d, (const T*)y->d, x->n(), c->red(slot)));
-  after_launch(c, "dot");
+                launch_ewr<T>(c, DotOp<T>{(const T*)x->d, (const T*)y->d}, x->n(),
+                              all_aligned(x->d, y->d), slot, "dot"));
 }
 
 void vec_mgs_step(lfg_field v, lfg_field pv, lfg_field vj, lfg_field pvj, Sc alpha,
@@ -343,11 +587,12 @@ void vec_mgs_step(lfg_field v, lfg_field pv, lfg_field vj, lfg_field pvj, Sc alp
   same_kind(v, pvj, "mgs");
   if (next) same_kind(v, next, "mgs");
   lfg_ctx c = v->ctx;
+  const void* nx = next ? next->d : nullptr;
   DISPATCH_KIND(v->kind, T,
-                k_mgs<T><<<c->stream_grid(v->n()), kThreads, 0, c->stream>>>(
-                    (T*)v->d, (T*)pv->d, (const T*)vj->d, (const T*)pvj->d,
-                    next ? (const T*)next->d : nullptr, v->n(), alpha, c->red(slot)));
-  after_launch(c, "mgs");
+                launch_ewr<T>(c, MgsOp<T>{(T*)v->d, (T*)pv->d, (const T*)vj->d,
+                                          (const T*)pvj->d, (const T*)nx, alpha},
+                              v->n(), all_aligned(v->d, pv->d, vj->d, pvj->d, nx), slot,
+                              "mgs"));
 }
 
 void vec_scale2_dot(lfg_field v, lfg_field pv, Sc beta, lfg_field res, int slot) {
@@ -355,9 +600,8 @@ void vec_scale2_dot(lfg_field v, lfg_field pv, Sc beta, lfg_field res, int slot)
   same_kind(v, res, "scale2_dot");
   lfg_ctx c = v->ctx;
   DISPATCH_KIND(v->kind, T,
-                k_scale2_dot<T><<<c->stream_grid(v->n()), kThreads, 0, c->stream>>>(
-                    (T*)v->d, (T*)pv->d, (const T*)res->d, v->n(), beta, c->red(slot)));
-  after_launch(c, "scale2_dot");
+                launch_ewr<T>(c, Scale2DotOp<T>{(T*)v->d, (T*)pv->d, (const T*)res->d, beta},
+                              v->n(), all_aligned(v->d, pv->d, res->d), slot, "scale2_dot"));
 }
 
 void vec_update2_norm(lfg_field dx, lfg_field pv, lfg_field res, lfg_field v, Sc alpha,
@@ -367,39 +611,36 @@ void vec_update2_norm(lfg_field dx, lfg_field pv, lfg_field res, lfg_field v, Sc
   same_kind(dx, v, "update2_norm");
   lfg_ctx c = dx->ctx;
   DISPATCH_KIND(dx->kind, T,
-                k_update2_norm<T><<<c->stream_grid(dx->n()), kThreads, 0, c->stream>>>(
-                    (T*)dx->d, (const T*)pv->d, (T*)res->d, (const T*)v->d, dx->n(), alpha,
-                    c->red(slot)));
-  after_launch(c, "update2_norm");
+                launch_ewr<T>(c, Update2NormOp<T>{(T*)dx->d, (const T*)pv->d, (T*)res->d,
+                                                  (const T*)v->d, alpha},
+                              dx->n(), all_aligned(dx->d, pv->d, res->d, v->d), slot,
+                              "update2_norm"));
 }
 
 void vec_axpy_norm(lfg_field x, Sc b, lfg_field y, int slot) {
   same_kind(x, y, "axpy_norm");
   lfg_ctx c = x->ctx;
   DISPATCH_KIND(x->kind, T,
-                k_axpy_norm<T><<<c->stream_grid(x->n()), kThreads, 0, c->stream>>>(
-                    (T*)x->d, (const T*)y->d, x->n(), b, c->red(slot)));
-  after_launch(c, "axpy_norm");
+                launch_ewr<T>(c, AxpyDotOp<T>{(T*)x->d, (const T*)y->d, nullptr, b}, x->n(),
+                              all_aligned(x->d, y->d), slot, "axpy_norm"));
 }
 
 void vec_axpy_dot(lfg_field x, Sc b, lfg_field y, lfg_field next, int slot) {
   same_kind(x, y, "axpy_dot");
   if (next) same_kind(x, next, "axpy_dot");
   lfg_ctx c = x->ctx;
+  const void* nx = next ? next->d : nullptr;
   DISPATCH_KIND(x->kind, T,
-                k_axpy_dot<T><<<c->stream_grid(x->n()), kThreads, 0, c->stream>>>(
-                    (T*)x->d, (const T*)y->d, next ? (const T*)next->d : nullptr, x->n(), b,
-                    c->red(slot)));
-  after_launch(c, "axpy_dot");
+                launch_ewr<T>(c, AxpyDotOp<T>{(T*)x->d, (const T*)y->d, (const T*)nx, b},
+                              x->n(), all_aligned(x->d, y->d, nx), slot, "axpy_dot"));
 }
 
 void vec_scale_copy(lfg_field dst, Sc a, lfg_field src) {
   same_kind(dst, src, "scale_copy");
   lfg_ctx c = dst->ctx;
   DISPATCH_KIND(dst->kind, T,
-                k_scale_copy<T><<<c->stream_grid(dst->n()), kThreads, 0, c->stream>>>(
-                    (T*)dst->d, (const T*)src->d, dst->n(), a));
-  after_launch(c, "scale_copy");
+                launch_ew<T>(c, ScaleCopyOp<T>{(T*)dst->d, (const T*)src->d, a}, dst->n(),
+                             all_aligned(dst->d, src->d), "scale_copy"));
 }
 
 }  // namespace lfg
