@@ -150,6 +150,105 @@ __global__ void k_thomas_scratch(TriSrc<T> s, const T* __restrict__ x, T* __rest
   }
 }
 
+// Thomas factors of a CMA tridiagonal, one thread per column, in the
+// reference's arithmetic (sci_columnwise_op_appinv_kernel_mod.F90:77-145):
+// inv_1 = 1/a2, inv_i = 1/(a2 - a1 c'_{i-1}); c'_i = inv_i a3 (not on the
+// last row).  They depend on the matrix alone.
+template <class T>
+__global__ void k_cma_factor(const T* __restrict__ bands, int ncol, int nrow, T* __restrict__ finv,
+                             T* __restrict__ fcp) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncol) return;
+  const size_t N = ncol, plane = (size_t)nrow * N;
+  T cprev = (T)0;
+  for (int k = 0; k < nrow; ++k) {
+    const size_t i = (size_t)k * N + c;
+    const T a1 = bands[i], a2 = bands[plane + i], a3 = bands[2 * plane + i];
+    const T inv = k == 0 ? (T)1 / a2 : (T)1 / (a2 - a1 * cprev);
+    const T cp = (k == 0 || k < nrow - 1) ? inv * a3 : (T)0;
+    finv[i] = inv;
+    fcp[i] = cp;
+    cprev = cp;
+  }
+}
+
+// lhs = A^{-1} x on the precomputed factors: d'_k = inv_k (x_k - a1_k d'_{k-1}),
+// z_k = d'_k - c'_k z_{k+1}, x and lhs at the rows' dof offsets.  One
+// thread per column, d' in shared memory; each sweep walks the column in
+// blocks of CSP levels and loads block b+1 before it computes block b.
+constexpr int CSP = 8;
+template <class T>
+__global__ void __launch_bounds__(128) k_cma_subst(const T* __restrict__ bands,
+                                                   const T* __restrict__ finv,
+                                                   const T* __restrict__ fcp,
+                                                   const int* __restrict__ ind, int ncol,
+                                                   int nrow, const T* __restrict__ x,
+                                                   T* __restrict__ lhs) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sd = reinterpret_cast<T*>(smem_raw);  // [nrow][blockDim]
+  const int t = threadIdx.x, bs = blockDim.x;
+  const int c = blockIdx.x * bs + t;
+  if (c >= ncol) return;
+  const size_t N = ncol;
+  const int nb = (nrow + CSP - 1) / CSP;
+  auto lv = [&](int k) { return min(max(k, 0), nrow - 1); };
+  T ax[CSP], ai[CSP], as[CSP], bx[CSP], bi[CSP], bsb[CSP];
+#pragma unroll
+  for (int p = 0; p < CSP; ++p) {
+    const int k = lv(p);
+    ax[p] = x[(size_t)ind[k] * N + c];
+    ai[p] = finv[(size_t)k * N + c];
+    as[p] = bands[(size_t)k * N + c];
+  }
+  T d = (T)0;
+  for (int blk = 0; blk < nb; ++blk) {
+    const int k0 = blk * CSP;
+#pragma unroll
+    for (int p = 0; p < CSP; ++p) {
+      const int k = lv(k0 + CSP + p);
+      bx[p] = x[(size_t)ind[k] * N + c];
+      bi[p] = finv[(size_t)k * N + c];
+      bsb[p] = bands[(size_t)k * N + c];
+    }
+#pragma unroll
+    for (int p = 0; p < CSP; ++p) {
+      const int k = k0 + p;
+      const T dn = k == 0 ? ai[p] * ax[p] : ai[p] * (ax[p] - as[p] * d);
+      if (k < nrow) {
+        d = dn;
+        sd[k * bs + t] = d;
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < CSP; ++p) {
+      ax[p] = bx[p];
+      ai[p] = bi[p];
+      as[p] = bsb[p];
+    }
+  }
+  T ac[CSP], bc[CSP];
+  const int ktop = nrow - 1;
+#pragma unroll
+  for (int p = 0; p < CSP; ++p) ac[p] = fcp[(size_t)lv(ktop - p) * N + c];
+  T z = (T)0;
+  for (int blk = 0; blk < nb; ++blk) {
+    const int k0 = ktop - blk * CSP;
+#pragma unroll
+    for (int p = 0; p < CSP; ++p) bc[p] = fcp[(size_t)lv(k0 - CSP - p) * N + c];
+#pragma unroll
+    for (int p = 0; p < CSP; ++p) {
+      const int k = k0 - p;
+      if (k >= 0) {
+        const T dk = sd[k * bs + t];
+        z = k == ktop ? dk : dk - ac[p] * z;
+        lhs[(size_t)ind[k] * N + c] = z;
+      }
+    }
+#pragma unroll
+    for (int p = 0; p < CSP; ++p) ac[p] = bc[p];
+  }
+}
+
 int col_block(int ncol, int nsm) {
   int per = (ncol + nsm - 1) / nsm;
   int bs = ((per + 31) / 32) * 32;
@@ -442,6 +541,8 @@ int lfg_cma_destroy(lfg_cma m) {
   dfree(m->jplus);
   dfree(m->tptr);
   dfree(m->trow);
+  dfree(m->finv);
+  dfree(m->fcp);
   delete m;
   return LFG_OK;
 }
@@ -494,11 +595,44 @@ int lfg_cma_apply_inverse(lfg_cma m, lfg_field lhs, lfg_field x) {
                     lhs->nlev >= m->max_ind_to && x->nlev >= m->max_ind_to &&
                     lhs->kind == m->kind && x->kind == m->kind,
                 "cma_apply_inverse: fields do not match the operator");
+    const size_t n = (size_t)m->nrow * m->ncol;
+    const size_t smem_col = (size_t)m->nrow * m->kind;
+    if (smem_col * 32 > 200 * 1024) {  // columns too tall for shared memory
+      dispatch(m->kind, [&](auto tag) {
+        using T = decltype(tag);
+        TriSrc<T> s{m->ncol, m->nrow, (const T*)m->bands, nullptr, nullptr, nullptr, m->ind_to, 0};
+        launch_thomas<T, SRC_CMA>(c, s, (const T*)x->d, (T*)lhs->d);
+      });
+      return;
+    }
+    if (!m->fvalid) {
+      if (!m->finv) {
+        m->finv = dmalloc(n * m->kind);
+        m->fcp = dmalloc(n * m->kind);
+      }
+      dispatch(m->kind, [&](auto tag) {
+        using T = decltype(tag);
+        k_cma_factor<T><<<(m->ncol + 127) / 128, 128, 0, c->stream>>>(
+            (const T*)m->bands, m->ncol, m->nrow, (T*)m->finv, (T*)m->fcp);
+      });
+      after_launch(c, "cma_factor");
+      m->fvalid = true;
+    }
+    int bs = 128;
+    while (bs > 32 && (m->ncol + bs - 1) / bs < 2 * c->num_sms) bs /= 2;
+    while (smem_col * bs > 200 * 1024) bs /= 2;
     dispatch(m->kind, [&](auto tag) {
       using T = decltype(tag);
-      TriSrc<T> s{m->ncol, m->nrow, (const T*)m->bands, nullptr, nullptr, nullptr, m->ind_to, 0};
-      launch_thomas<T, SRC_CMA>(c, s, (const T*)x->d, (T*)lhs->d);
+      static std::once_flag attr;
+      std::call_once(attr, [] {
+        LFG_CUDA(cudaFuncSetAttribute(k_cma_subst<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      200 * 1024));
+      });
+      k_cma_subst<T><<<(m->ncol + bs - 1) / bs, bs, smem_col * bs, c->stream>>>(
+          (const T*)m->bands, (const T*)m->finv, (const T*)m->fcp, m->ind_to, m->ncol, m->nrow,
+          (const T*)x->d, (T*)lhs->d);
     });
+    after_launch(c, "cma_subst");
   });
 }
 

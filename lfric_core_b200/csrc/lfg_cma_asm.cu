@@ -250,6 +250,7 @@ int lfg_cma_assemble(lfg_cma m, lfg_lma a, const int* cb_to, const int* cb_from)
       });
     });
     after_launch(c, "cma_asm");
+    m->fvalid = false;  // the bands changed
     LFG_CUDA(cudaStreamSynchronize(c->stream));  // the dofmap copies are freed on return
   });
 }
@@ -285,6 +286,7 @@ int lfg_cma_multiply(lfg_cma C, lfg_cma A, lfg_cma B) {
           C->ncol);
     });
     after_launch(c, "cma_mul");
+    C->fvalid = false;  // the bands changed
   });
 }
 
@@ -319,6 +321,7 @@ int lfg_cma_scaled_add(lfg_cma C, lfg_cma A, lfg_cma B, double alpha, double bet
           (T)alpha, (T)beta);
     });
     after_launch(c, "cma_scaledadd");
+    C->fvalid = false;  // the bands changed
   });
 }
 
@@ -346,6 +349,7 @@ int lfg_cma_assemble_diag_hmht(lfg_cma m, lfg_lma dh, lfg_lma m2h, const int* cb
       });
     });
     after_launch(c, "cma_asm_diag_hmht");
+    m->fvalid = false;  // the bands changed
     LFG_CUDA(cudaStreamSynchronize(c->stream));
   });
 }
@@ -369,6 +373,7 @@ int lfg_cma_assemble_m2v_lumped_inv(lfg_cma m, lfg_lma mm, const int* cbm) {
       });
     });
     after_launch(c, "cma_asm_m2v_lumped_inv");
+    m->fvalid = false;  // the bands changed
     LFG_CUDA(cudaStreamSynchronize(c->stream));
   });
 }

@@ -206,6 +206,12 @@ struct lfg_cma_s {
   int max_ind_to = 0, max_ind_from = 0;  // largest 1-based column offsets
   int* tptr = nullptr;        // [ncolumn+1] rows reaching each column (transpose)
   int* trow = nullptr;
+  // Thomas factors of a square tridiagonal operator (columnwise_op_appinv's
+  // inverse denominators and c'), [nrow][ncol]; computed on the first
+  // lfg_cma_apply_inverse after the bands change
+  void* finv = nullptr;
+  void* fcp = nullptr;
+  bool fvalid = false;
 };
 
 struct lfg_lma_s {
