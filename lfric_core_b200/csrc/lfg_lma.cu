@@ -118,6 +118,88 @@ __global__ void k_lma_apply_t(LmaArgs<T> L, const int* __restrict__ ptr,
   y[o] = acc;
 }
 
+// Two-phase applies.  Phase 1, one thread per (cell, layer) with cells
+// fastest, reads the element matrix once, coalesced, and writes the cell's
+// local products: forward loc(df, layer, cell) = sum_df2 A(df,df2) x(df2),
+// transposed loc(df2, layer, cell) = sum_df A(df,df2) x(df).  Phase 2 is
+// the gather: every output dof adds the local products of its incidences
+// in the incidence order.  The dense matrix traffic of phase 1 replaces the
+// scattered per-incidence matrix reads of a one-pass gather.
+constexpr int kLocDf = 16;  // largest ndf handled by the two-phase form
+
+template <class T, bool TR>
+__global__ void k_lma_local(LmaArgs<T> L, const T* __restrict__ x, T* __restrict__ loc) {
+  const size_t n = (size_t)L.ncell * L.nl;
+  const int nin = TR ? L.ndf_to : L.ndf_from, nout = TR ? L.ndf_from : L.ndf_to;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int cell = (int)(t % L.ncell), layer = (int)(t / L.ncell);
+    T xv[kLocDf];
+#pragma unroll
+    for (int d = 0; d < kLocDf; ++d)
+      if (d < nin) {
+        const size_t ti = (size_t)d * L.ncell + cell;
+        xv[d] = TR ? x[(size_t)(layer + L.off_to[ti]) * L.nent_to + L.ent_to[ti]]
+                   : x[(size_t)(layer + L.off_from[ti]) * L.nent_from + L.ent_from[ti]];
+      }
+    for (int o = 0; o < nout; ++o) {
+      T acc = (T)0;
+#pragma unroll
+      for (int d = 0; d < kLocDf; ++d)
+        if (d < nin) acc = acc + (TR ? amat(L, d, o, layer, cell) : amat(L, o, d, layer, cell)) * xv[d];
+      loc[((size_t)o * L.nl + layer) * L.ncell + cell] = acc;
+    }
+  }
+}
+
+// forward gather: y(e,k) (+)= sum over the incidences (cell, df) of e, in
+// order, of loc(df, k - off_to(df, cell), cell)
+template <class T, bool INC>
+__global__ void k_lma_gather(LmaArgs<T> L, const int* __restrict__ ptr,
+                             const int* __restrict__ inc, const T* __restrict__ loc,
+                             T* __restrict__ y) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y;
+  if (e >= L.nent_to) return;
+  const size_t o = (size_t)k * L.nent_to + e;
+  T acc = INC ? y[o] : (T)0;
+  for (int g = ptr[e]; g < ptr[e + 1]; ++g) {
+    const int cell = inc[g] / L.ndf_to, df = inc[g] - cell * L.ndf_to;
+    const int layer = k - L.off_to[(size_t)df * L.ncell + cell];
+    if (layer < 0 || layer >= L.nl) continue;
+    acc = acc + loc[((size_t)df * L.nl + layer) * L.ncell + cell];
+  }
+  y[o] = acc;
+}
+
+// transposed gather: the incidences of each from-space dof, a cell's
+// local dofs in decreasing order (increasing layer) as k_lma_apply_t
+template <class T>
+__global__ void k_lma_gather_t(LmaArgs<T> L, const int* __restrict__ ptr,
+                               const int* __restrict__ inc, const T* __restrict__ loc,
+                               T* __restrict__ y) {
+  const int e = blockIdx.x * blockDim.x + threadIdx.x;
+  const int k = blockIdx.y;
+  if (e >= L.nent_from) return;
+  const size_t o = (size_t)k * L.nent_from + e;
+  T acc = y[o];
+  const int j0 = ptr[e], j1 = ptr[e + 1];
+  int j = j0;
+  while (j < j1) {
+    const int cell = inc[j] / L.ndf_from;
+    int jend = j + 1;
+    while (jend < j1 && inc[jend] / L.ndf_from == cell) ++jend;
+    for (int g = jend - 1; g >= j; --g) {
+      const int df2 = inc[g] - cell * L.ndf_from;
+      const int layer = k - L.off_from[(size_t)df2 * L.ncell + cell];
+      if (layer < 0 || layer >= L.nl) continue;
+      acc = acc + loc[((size_t)df2 * L.nl + layer) * L.ncell + cell];
+    }
+    j = jend;
+  }
+  y[o] = acc;
+}
+
 // diag(e,k) += A(df, df, layer, cell) over incidences, increasing layer
 template <class T>
 __global__ void k_lma_diag(LmaArgs<T> L, const int* __restrict__ ptr,
@@ -317,6 +399,38 @@ int lfg_lma_apply(lfg_lma m, int mode, lfg_field lhs, lfg_field x) {
       LFG_REQUIRE(lhs->ncol == m->nent_to && lhs->nlev == m->nlev_to &&
                       x->ncol == m->nent_from && x->nlev == m->nlev_from,
                   "lma_apply: fields do not match the operator's spaces");
+    }
+    // two-phase form for the forward applies (the one-pass transposed gather
+    // measured faster than its two-phase form on the W0 operator)
+    if (mode != LFG_LMA_TRANSPOSE && m->ndf_to <= kLocDf && m->ndf_from <= kLocDf) {
+      const size_t ncl = (size_t)m->ncell * m->nl;
+      dispatch(m->kind, [&](auto tag) {
+        using T = decltype(tag);
+        const bool tr = mode == LFG_LMA_TRANSPOSE;
+        T* loc = (T*)c->scratch(ncl * (tr ? m->ndf_from : m->ndf_to) * sizeof(T));
+        if (tr)
+          k_lma_local<T, true><<<occ_grid(c, (const void*)k_lma_local<T, true>, 256, ncl), 256, 0,
+                                 c->stream>>>(args_of<T>(m), (const T*)x->d, loc);
+        else
+          k_lma_local<T, false><<<occ_grid(c, (const void*)k_lma_local<T, false>, 256, ncl), 256,
+                                  0, c->stream>>>(args_of<T>(m), (const T*)x->d, loc);
+        after_launch(c, "lma_local");
+        if (tr) {
+          dim3 grid((m->nent_from + 127) / 128, m->nlev_from);
+          k_lma_gather_t<T><<<grid, 128, 0, c->stream>>>(args_of<T>(m), m->inc_from_ptr,
+                                                         m->inc_from, loc, (T*)lhs->d);
+        } else {
+          dim3 grid((m->nent_to + 127) / 128, m->nlev_to);
+          if (mode == LFG_LMA_INC)
+            k_lma_gather<T, true><<<grid, 128, 0, c->stream>>>(args_of<T>(m), m->inc_to_ptr,
+                                                               m->inc_to, loc, (T*)lhs->d);
+          else
+            k_lma_gather<T, false><<<grid, 128, 0, c->stream>>>(args_of<T>(m), m->inc_to_ptr,
+                                                                m->inc_to, loc, (T*)lhs->d);
+        }
+      });
+      after_launch(c, "lma_gather");
+      return;
     }
     dispatch(m->kind, [&](auto tag) {
       using T = decltype(tag);
