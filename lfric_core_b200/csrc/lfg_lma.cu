@@ -118,13 +118,14 @@ __global__ void k_lma_apply_t(LmaArgs<T> L, const int* __restrict__ ptr,
   y[o] = acc;
 }
 
-// Two-phase applies.  Phase 1, one thread per (cell, layer) with cells
-// fastest, reads the element matrix once, coalesced, and writes the cell's
-// local products: forward loc(df, layer, cell) = sum_df2 A(df,df2) x(df2),
-// transposed loc(df2, layer, cell) = sum_df A(df,df2) x(df).  Phase 2 is
-// the gather: every output dof adds the local products of its incidences
-// in the incidence order.  The dense matrix traffic of phase 1 replaces the
-// scattered per-incidence matrix reads of a one-pass gather.
+// Two-phase forward apply.  Phase 1, one thread per (cell, layer) with
+// cells fastest, reads the element matrix once, coalesced, and writes the
+// cell's local products loc(df, layer, cell) = sum_df2 A(df,df2) x(df2)
+// (TR: the transposed products sum_df A(df,df2) x(df), kept for the
+// transposed apply's measurements).  Phase 2 is the gather: every output
+// dof adds the local products of its incidences in the incidence order.
+// The dense matrix traffic of phase 1 replaces the scattered per-incidence
+// matrix reads of a one-pass gather.
 constexpr int kLocDf = 16;  // largest ndf handled by the two-phase form
 
 template <class T, bool TR>
@@ -168,34 +169,6 @@ __global__ void k_lma_gather(LmaArgs<T> L, const int* __restrict__ ptr,
     const int layer = k - L.off_to[(size_t)df * L.ncell + cell];
     if (layer < 0 || layer >= L.nl) continue;
     acc = acc + loc[((size_t)df * L.nl + layer) * L.ncell + cell];
-  }
-  y[o] = acc;
-}
-
-// transposed gather: the incidences of each from-space dof, a cell's
-// local dofs in decreasing order (increasing layer) as k_lma_apply_t
-template <class T>
-__global__ void k_lma_gather_t(LmaArgs<T> L, const int* __restrict__ ptr,
-                               const int* __restrict__ inc, const T* __restrict__ loc,
-                               T* __restrict__ y) {
-  const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k = blockIdx.y;
-  if (e >= L.nent_from) return;
-  const size_t o = (size_t)k * L.nent_from + e;
-  T acc = y[o];
-  const int j0 = ptr[e], j1 = ptr[e + 1];
-  int j = j0;
-  while (j < j1) {
-    const int cell = inc[j] / L.ndf_from;
-    int jend = j + 1;
-    while (jend < j1 && inc[jend] / L.ndf_from == cell) ++jend;
-    for (int g = jend - 1; g >= j; --g) {
-      const int df2 = inc[g] - cell * L.ndf_from;
-      const int layer = k - L.off_from[(size_t)df2 * L.ncell + cell];
-      if (layer < 0 || layer >= L.nl) continue;
-      acc = acc + loc[((size_t)df2 * L.nl + layer) * L.ncell + cell];
-    }
-    j = jend;
   }
   y[o] = acc;
 }
@@ -406,28 +379,17 @@ int lfg_lma_apply(lfg_lma m, int mode, lfg_field lhs, lfg_field x) {
       const size_t ncl = (size_t)m->ncell * m->nl;
       dispatch(m->kind, [&](auto tag) {
         using T = decltype(tag);
-        const bool tr = mode == LFG_LMA_TRANSPOSE;
-        T* loc = (T*)c->scratch(ncl * (tr ? m->ndf_from : m->ndf_to) * sizeof(T));
-        if (tr)
-          k_lma_local<T, true><<<occ_grid(c, (const void*)k_lma_local<T, true>, 256, ncl), 256, 0,
-                                 c->stream>>>(args_of<T>(m), (const T*)x->d, loc);
-        else
-          k_lma_local<T, false><<<occ_grid(c, (const void*)k_lma_local<T, false>, 256, ncl), 256,
-                                  0, c->stream>>>(args_of<T>(m), (const T*)x->d, loc);
+        T* loc = (T*)c->scratch(ncl * m->ndf_to * sizeof(T));
+        k_lma_local<T, false><<<occ_grid(c, (const void*)k_lma_local<T, false>, 256, ncl), 256, 0,
+                                c->stream>>>(args_of<T>(m), (const T*)x->d, loc);
         after_launch(c, "lma_local");
-        if (tr) {
-          dim3 grid((m->nent_from + 127) / 128, m->nlev_from);
-          k_lma_gather_t<T><<<grid, 128, 0, c->stream>>>(args_of<T>(m), m->inc_from_ptr,
-                                                         m->inc_from, loc, (T*)lhs->d);
-        } else {
-          dim3 grid((m->nent_to + 127) / 128, m->nlev_to);
-          if (mode == LFG_LMA_INC)
-            k_lma_gather<T, true><<<grid, 128, 0, c->stream>>>(args_of<T>(m), m->inc_to_ptr,
-                                                               m->inc_to, loc, (T*)lhs->d);
-          else
-            k_lma_gather<T, false><<<grid, 128, 0, c->stream>>>(args_of<T>(m), m->inc_to_ptr,
-                                                                m->inc_to, loc, (T*)lhs->d);
-        }
+        dim3 grid((m->nent_to + 127) / 128, m->nlev_to);
+        if (mode == LFG_LMA_INC)
+          k_lma_gather<T, true><<<grid, 128, 0, c->stream>>>(args_of<T>(m), m->inc_to_ptr,
+                                                             m->inc_to, loc, (T*)lhs->d);
+        else
+          k_lma_gather<T, false><<<grid, 128, 0, c->stream>>>(args_of<T>(m), m->inc_to_ptr,
+                                                              m->inc_to, loc, (T*)lhs->d);
       });
       after_launch(c, "lma_gather");
       return;
