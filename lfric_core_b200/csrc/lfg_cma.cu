@@ -249,6 +249,89 @@ __global__ void __launch_bounds__(128) k_cma_subst(const T* __restrict__ bands,
   }
 }
 
+// The same substitutions with S warps per 32 columns: warp j of a block
+// owns rows [j*L, j*L + L), L = ceil(nrow/S) <= kCmaSeg, of the block's 32
+// columns (one column per lane, so every row is one coalesced 32-column
+// load) and loads them all at once.  Each thread composes its rows' affine
+// maps (forward d_out = D + M d_in, backward z_in = E + Nn z_out); through
+// shared memory every segment then applies the maps of the segments before
+// it (after it, backward) to find its incoming value, and computes its rows
+// with the per-row formulas of k_cma_subst.  Only the value that enters a
+// segment is formed through the maps, a rounding-level difference.
+constexpr int kCmaSeg = 12;
+template <class T, int S>
+__global__ void __launch_bounds__(32 * S) k_cma_subst_seg(const T* __restrict__ bands,
+                                                          const T* __restrict__ finv,
+                                                          const T* __restrict__ fcp,
+                                                          const int* __restrict__ ind, int ncol,
+                                                          int nrow, const T* __restrict__ x,
+                                                          T* __restrict__ lhs) {
+  __shared__ T sa[S][32], sm[S][32];
+  const int lane = threadIdx.x & 31, j = threadIdx.x >> 5;
+  const unsigned c = blockIdx.x * 32u + lane;
+  const size_t N = ncol;
+  const int L = (nrow + S - 1) / S, k0 = j * L;
+  const int nmy = c < N ? max(0, min(L, nrow - k0)) : 0;
+  T d[kCmaSeg], iv[kCmaSeg], sb[kCmaSeg], cc[kCmaSeg];
+#pragma unroll
+  for (int u = 0; u < kCmaSeg; ++u)
+    if (u < nmy) {
+      const size_t i = (size_t)(k0 + u) * N + c;
+      d[u] = x[(size_t)ind[k0 + u] * N + c];
+      iv[u] = finv[i];
+      sb[u] = bands[i];
+      cc[u] = fcp[i];
+    }
+  T D = (T)0, M = (T)1;
+#pragma unroll
+  for (int u = 0; u < kCmaSeg; ++u)
+    if (u < nmy) {
+      D = (d[u] - sb[u] * D) * iv[u];
+      M = M * (-sb[u] * iv[u]);
+    }
+  sa[j][lane] = D;
+  sm[j][lane] = M;
+  __syncthreads();
+  T dv = (T)0;
+  for (int q = 0; q < j; ++q) dv = sa[q][lane] + sm[q][lane] * dv;
+#pragma unroll
+  for (int u = 0; u < kCmaSeg; ++u)
+    if (u < nmy) {
+      dv = k0 + u == 0 ? iv[u] * d[u] : iv[u] * (d[u] - sb[u] * dv);
+      d[u] = dv;
+    }
+  T E = (T)0, Nn = (T)1;
+#pragma unroll
+  for (int u = kCmaSeg - 1; u >= 0; --u)
+    if (u < nmy) {
+      E = d[u] - cc[u] * E;
+      Nn = Nn * (-cc[u]);
+    }
+  __syncthreads();
+  sa[j][lane] = E;
+  sm[j][lane] = Nn;
+  __syncthreads();
+  T z = (T)0;
+  for (int q = S - 1; q > j; --q) z = sa[q][lane] + sm[q][lane] * z;
+#pragma unroll
+  for (int u = kCmaSeg - 1; u >= 0; --u)
+    if (u < nmy) {
+      const int k = k0 + u;
+      z = k == nrow - 1 ? d[u] : d[u] - cc[u] * z;
+      lhs[(size_t)ind[k] * N + c] = z;
+    }
+}
+
+// warps per 32 columns for k_cma_subst_seg: the fewest (2, 4 or 8) that
+// cut the column into segments of at most kCmaSeg rows; 0 for columns of
+// at most kCmaSeg rows (one thread holds them) or taller than 8 * kCmaSeg
+int cma_seg_lanes(int nrow) {
+  if (nrow <= kCmaSeg) return 0;
+  for (int S = 2; S <= 8; S *= 2)
+    if ((nrow + S - 1) / S <= kCmaSeg) return S;
+  return 0;
+}
+
 int col_block(int ncol, int nsm) {
   int per = (ncol + nsm - 1) / nsm;
   int bs = ((per + 31) / 32) * 32;
@@ -346,16 +429,34 @@ __global__ void k_restrict(T* __restrict__ coarse, const T* __restrict__ fine,
   coarse[(size_t)k * ncoarse + C] = acc;
 }
 
+// fine(c,k) (+)= [w(c,k)] coarse(parent(c),k): one thread per (column,
+// block of KI levels), columns fastest, grid-stride; the parent index is
+// read once per block and the block's loads all issue before its stores.
+constexpr int KI = 4;
+
 template <class T, bool WEIGHTED>
 __global__ void k_prolong(T* __restrict__ fine, const T* __restrict__ coarse,
                           const T* __restrict__ w, const int* __restrict__ parent, int nfine,
                           int ncoarse, int nlev) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k = blockIdx.y;
-  if (c >= nfine || k >= nlev) return;
-  const size_t i = (size_t)k * nfine + c;
-  const T cv = coarse[(size_t)k * ncoarse + parent[c]];
-  fine[i] = WEIGHTED ? fine[i] + w[i] * cv : fine[i] + cv;
+  const size_t nblk = (size_t)nfine * ((nlev + KI - 1) / KI);
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < nblk;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(t % nfine), k0 = (int)(t / nfine) * KI;
+    const int p = parent[c];
+    T cv[KI], fv[KI], wv[KI];
+#pragma unroll
+    for (int kk = 0; kk < KI; ++kk)
+      if (k0 + kk < nlev) {
+        const size_t i = (size_t)(k0 + kk) * nfine + c;
+        cv[kk] = coarse[(size_t)(k0 + kk) * ncoarse + p];
+        fv[kk] = fine[i];
+        if (WEIGHTED) wv[kk] = w[i];
+      }
+#pragma unroll
+    for (int kk = 0; kk < KI; ++kk)
+      if (k0 + kk < nlev)
+        fine[(size_t)(k0 + kk) * nfine + c] = WEIGHTED ? fv[kk] + wv[kk] * cv[kk] : fv[kk] + cv[kk];
+  }
 }
 
 // W0 injection: coarse vertex v takes the value of the coinciding fine vertex.
@@ -618,6 +719,24 @@ int lfg_cma_apply_inverse(lfg_cma m, lfg_field lhs, lfg_field x) {
       after_launch(c, "cma_factor");
       m->fvalid = true;
     }
+    // FP64: segmented form; FP32 columns (half the bytes per row) measured
+    // faster one thread per column
+    if (const int S = m->kind == LFG_R_DOUBLE ? cma_seg_lanes(m->nrow) : 0) {
+      const unsigned grid = (unsigned)((m->ncol + 31) / 32);
+      dispatch(m->kind, [&](auto tag) {
+        using T = decltype(tag);
+        auto go = [&](void (*k)(const T*, const T*, const T*, const int*, int, int, const T*, T*)) {
+          k<<<grid, 32 * S, 0, c->stream>>>((const T*)m->bands, (const T*)m->finv,
+                                            (const T*)m->fcp, m->ind_to, m->ncol, m->nrow,
+                                            (const T*)x->d, (T*)lhs->d);
+        };
+        if (S == 2) go(k_cma_subst_seg<T, 2>);
+        else if (S == 4) go(k_cma_subst_seg<T, 4>);
+        else go(k_cma_subst_seg<T, 8>);
+      });
+      after_launch(c, "cma_subst_seg");
+      return;
+    }
     int bs = 128;
     while (bs > 32 && (m->ncol + bs - 1) / bs < 2 * c->num_sms) bs /= 2;
     while (smem_col * bs > 200 * 1024) bs /= 2;
@@ -822,13 +941,16 @@ int lfg_prolong_scalar(lfg_intergrid g, lfg_field fine, lfg_field coarse, lfg_fi
     if (w)
       LFG_REQUIRE(w->ncol == fine->ncol && w->nlev == fine->nlev && w->kind == fine->kind,
                   "prolong_scalar: weights must be a fine field");
-    dim3 grid((g->nfine + 127) / 128, fine->nlev);
+    const size_t nblk = (size_t)g->nfine * ((fine->nlev + KI - 1) / KI);
     dispatch(fine->kind, [&](auto tag) {
       using T = decltype(tag);
-      if (w)
-        k_prolong<T, true><<<grid, 128, 0, c->stream>>>((T*)fine->d, (const T*)coarse->d, (const T*)w->d, g->parent, g->nfine, g->ncoarse, fine->nlev);
-      else
-        k_prolong<T, false><<<grid, 128, 0, c->stream>>>((T*)fine->d, (const T*)coarse->d, nullptr, g->parent, g->nfine, g->ncoarse, fine->nlev);
+      auto go = [&](void (*k)(T*, const T*, const T*, const int*, int, int, int)) {
+        k<<<occ_grid(c, (const void*)k, 256, nblk), 256, 0, c->stream>>>(
+            (T*)fine->d, (const T*)coarse->d, w ? (const T*)w->d : nullptr, g->parent, g->nfine,
+            g->ncoarse, fine->nlev);
+      };
+      if (w) go(k_prolong<T, true>);
+      else go(k_prolong<T, false>);
     });
     after_launch(c, "prolong_scalar");
   });

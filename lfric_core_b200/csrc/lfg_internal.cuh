@@ -230,6 +230,12 @@ struct lfg_lma_s {
   int* inc_from_ptr = nullptr;
   int* inc_from = nullptr;
   int max_inc_to = 0, max_inc_from = 0;
+  // the same lists padded to a fixed width, [slot][entity], each slot the
+  // pair (loc offset of layer 0, level offset); empty slots never match a
+  // level.  tab_to keeps the forward order, tab_from the transposed one.
+  int2* tab_to = nullptr;
+  int2* tab_from = nullptr;
+  int tab_to_w = 0, tab_from_w = 0;  // 0: no padded table (wider lists)
 };
 
 struct lfg_helm_s {

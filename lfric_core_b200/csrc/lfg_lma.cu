@@ -118,59 +118,100 @@ __global__ void k_lma_apply_t(LmaArgs<T> L, const int* __restrict__ ptr,
   y[o] = acc;
 }
 
-// Two-phase forward apply.  Phase 1, one thread per (cell, layer) with
-// cells fastest, reads the element matrix once, coalesced, and writes the
-// cell's local products loc(df, layer, cell) = sum_df2 A(df,df2) x(df2)
-// (TR: the transposed products sum_df A(df,df2) x(df), kept for the
-// transposed apply's measurements).  Phase 2 is the gather: every output
-// dof adds the local products of its incidences in the incidence order.
-// The dense matrix traffic of phase 1 replaces the scattered per-incidence
-// matrix reads of a one-pass gather.
+// Two-phase applies.  Phase 1, one thread per (cell, layer) with cells
+// fastest, streams the element matrix once (coalesced, evict-first loads so
+// that the local products stay in L2) and writes the cell's local products
+//   forward    (TR false): loc(df,  layer, cell) = sum_df2 A(df,df2) x(df2)
+//   transposed (TR true):  loc(df2, layer, cell) = sum_df  A(df,df2) x(df)
+// each summed from zero in ascending order.  Phase 2 is the gather: every
+// output dof adds the local products of its incidences in the one-pass
+// kernels' order.  The transposed form thus equals k_lma_apply_t bit for
+// bit; the forward form adds one local product per incidence where the
+// reference (and k_lma_apply) adds the ndf_from products one at a time, a
+// rounding-level difference.
+// NT/NF > 0 fix ndf_to/ndf_from at compile time (loops fully unrolled);
+// 0 takes them at run time, up to kLocDf.
 constexpr int kLocDf = 16;  // largest ndf handled by the two-phase form
 
-template <class T, bool TR>
+template <class T, bool TR, int NT, int NF>
 __global__ void k_lma_local(LmaArgs<T> L, const T* __restrict__ x, T* __restrict__ loc) {
-  const size_t n = (size_t)L.ncell * L.nl;
-  const int nin = TR ? L.ndf_to : L.ndf_from, nout = TR ? L.ndf_from : L.ndf_to;
-  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n;
+  constexpr int CIN = TR ? NT : NF, COUT = TR ? NF : NT;
+  constexpr int MAXIN = CIN > 0 ? CIN : kLocDf;
+  const int nin = CIN > 0 ? CIN : (TR ? L.ndf_to : L.ndf_from);
+  const int nout = COUT > 0 ? COUT : (TR ? L.ndf_from : L.ndf_to);
+  const int ndf_from = NF > 0 ? NF : L.ndf_from;
+  const size_t plane = (size_t)L.ncell * L.nl;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < plane;
        t += (size_t)gridDim.x * blockDim.x) {
     const int cell = (int)(t % L.ncell), layer = (int)(t / L.ncell);
-    T xv[kLocDf];
+    T xv[MAXIN];
 #pragma unroll
-    for (int d = 0; d < kLocDf; ++d)
+    for (int d = 0; d < MAXIN; ++d)
       if (d < nin) {
         const size_t ti = (size_t)d * L.ncell + cell;
         xv[d] = TR ? x[(size_t)(layer + L.off_to[ti]) * L.nent_to + L.ent_to[ti]]
                    : x[(size_t)(layer + L.off_from[ti]) * L.nent_from + L.ent_from[ti]];
       }
-    for (int o = 0; o < nout; ++o) {
-      T acc = (T)0;
+    if constexpr (COUT == 0) {  // run-time sizes: one output at a time
+      for (int o = 0; o < nout; ++o) {
+        T acc = (T)0;
 #pragma unroll
-      for (int d = 0; d < kLocDf; ++d)
-        if (d < nin) acc = acc + (TR ? amat(L, d, o, layer, cell) : amat(L, o, d, layer, cell)) * xv[d];
-      loc[((size_t)o * L.nl + layer) * L.ncell + cell] = acc;
+        for (int d = 0; d < MAXIN; ++d)
+          if (d < nin) {
+            const int df = TR ? d : o, df2 = TR ? o : d;
+            acc = acc + __ldcs(L.a + (size_t)(df * ndf_from + df2) * plane + t) * xv[d];
+          }
+        loc[(size_t)o * plane + t] = acc;
+      }
+    } else {
+      // fixed sizes: every output summed in registers before any store, so
+      // that the stores do not hold back the matrix loads
+      T acc[COUT];
+#pragma unroll
+      for (int o = 0; o < COUT; ++o) acc[o] = (T)0;
+#pragma unroll
+      for (int d = 0; d < MAXIN; ++d)
+#pragma unroll
+        for (int o = 0; o < COUT; ++o) {
+          const int df = TR ? d : o, df2 = TR ? o : d;
+          acc[o] = acc[o] + __ldcs(L.a + (size_t)(df * ndf_from + df2) * plane + t) * xv[d];
+        }
+#pragma unroll
+      for (int o = 0; o < COUT; ++o) loc[(size_t)o * plane + t] = acc[o];
     }
   }
 }
 
-// forward gather: y(e,k) (+)= sum over the incidences (cell, df) of e, in
-// order, of loc(df, k - off_to(df, cell), cell)
-template <class T, bool INC>
-__global__ void k_lma_gather(LmaArgs<T> L, const int* __restrict__ ptr,
-                             const int* __restrict__ inc, const T* __restrict__ loc,
-                             T* __restrict__ y) {
+// Padded incidence table: slot m of entity e, [m][e], holds its m-th
+// incidence as (cell, o << 8 | df), o the level offset of local dof df in
+// the cell; level k of e takes layer k - o of the cell when 0 <= k - o < nl.
+// Empty slots carry an offset no level reaches.
+__device__ __forceinline__ int slot_df(int2 s) { return s.y & 255; }
+__device__ __forceinline__ int slot_off(int2 s) { return s.y >> 8; }
+
+// gather through the padded table: y(e,k) (+)= sum over the slots of e
+// whose layer is in range of loc(df, layer, cell); a thread covers KC
+// levels of one entity and keeps its W slots in registers
+template <class T, bool INC, int W, int KC>
+__global__ void k_lma_gather_tab(const int2* __restrict__ tab, int nent, int nlev, int nl,
+                                 int ncell, const T* __restrict__ loc, T* __restrict__ y) {
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
-  const int k = blockIdx.y;
-  if (e >= L.nent_to) return;
-  const size_t o = (size_t)k * L.nent_to + e;
-  T acc = INC ? y[o] : (T)0;
-  for (int g = ptr[e]; g < ptr[e + 1]; ++g) {
-    const int cell = inc[g] / L.ndf_to, df = inc[g] - cell * L.ndf_to;
-    const int layer = k - L.off_to[(size_t)df * L.ncell + cell];
-    if (layer < 0 || layer >= L.nl) continue;
-    acc = acc + loc[((size_t)df * L.nl + layer) * L.ncell + cell];
+  if (e >= nent) return;
+  int2 s[W];
+#pragma unroll
+  for (int m = 0; m < W; ++m) s[m] = tab[(size_t)m * nent + e];
+  const int k0 = blockIdx.y * KC, k1 = min(k0 + KC, nlev);
+  for (int k = k0; k < k1; ++k) {
+    const size_t o = (size_t)k * nent + e;
+    T acc = INC ? y[o] : (T)0;
+#pragma unroll
+    for (int m = 0; m < W; ++m) {
+      const int layer = k - slot_off(s[m]);
+      if (layer >= 0 && layer < nl)
+        acc = acc + loc[((size_t)slot_df(s[m]) * nl + layer) * ncell + s[m].x];
+    }
+    y[o] = acc;
   }
-  y[o] = acc;
 }
 
 // diag(e,k) += A(df, df, layer, cell) over incidences, increasing layer
@@ -268,6 +309,68 @@ int* dcopy(const std::vector<int>& v) {
   return p;
 }
 
+// padded incidence table of one space (format at slot_df): incidences keep
+// the lists' order (cells ascending); REV takes each cell's dfs in
+// descending order (the transposed apply's).  Returns the width (a power
+// of two), or 0 when the lists are wider than 16, ndf > 255 or the level
+// offsets reach 2^22.
+int build_tab(const std::vector<int>& off, const std::vector<int>& ptr,
+              const std::vector<int>& inc, int ndf, int ncell, int nlev, int maxinc, bool rev,
+              int2** out) {
+  int w = 1;
+  while (w < maxinc) w <<= 1;
+  if (w > 16 || ndf > 255 || nlev >= (1 << 22)) return 0;
+  const int nent = (int)ptr.size() - 1;
+  std::vector<int2> tab((size_t)w * nent, make_int2(0, 1 << 30));
+  for (int e = 0; e < nent; ++e) {
+    int m = 0;
+    for (int j = ptr[e]; j < ptr[e + 1];) {
+      const int cell = inc[j] / ndf;
+      int jend = j + 1;
+      while (jend < ptr[e + 1] && inc[jend] / ndf == cell) ++jend;
+      for (int q = 0; q < jend - j; ++q) {
+        const int df = inc[rev ? jend - 1 - q : j + q] - cell * ndf;
+        const int o = off[(size_t)df * ncell + cell];
+        tab[(size_t)m++ * nent + e] = make_int2(cell, o << 8 | df);
+      }
+      j = jend;
+    }
+  }
+  *out = (int2*)dmalloc(tab.size() * sizeof(int2));
+  upload(*out, tab.data(), tab.size() * sizeof(int2));
+  return w;
+}
+
+template <class T, bool TR>
+void launch_local(lfg_ctx c, lfg_lma m, const T* x, T* loc) {
+  const size_t ncl = (size_t)m->ncell * m->nl;
+  auto go = [&](void (*k)(LmaArgs<T>, const T*, T*)) {
+    k<<<occ_grid(c, (const void*)k, 256, ncl), 256, 0, c->stream>>>(args_of<T>(m), x, loc);
+  };
+  if (m->ndf_to == 8 && m->ndf_from == 8) go(k_lma_local<T, TR, 8, 8>);
+  else if (m->ndf_to == 1 && m->ndf_from == 1) go(k_lma_local<T, TR, 1, 1>);
+  else go(k_lma_local<T, TR, 0, 0>);
+  after_launch(c, "lma_local");
+}
+
+template <class T, bool INC>
+void launch_gather_tab(lfg_ctx c, const int2* tab, int w, int nent, int nlev, int nl, int ncell,
+                       const T* loc, T* y) {
+  constexpr int KC = 4;
+  const dim3 grid((nent + 127) / 128, (nlev + KC - 1) / KC);
+  auto go = [&](void (*k)(const int2*, int, int, int, int, const T*, T*)) {
+    k<<<grid, 128, 0, c->stream>>>(tab, nent, nlev, nl, ncell, loc, y);
+  };
+  switch (w) {
+    case 1: go(k_lma_gather_tab<T, INC, 1, KC>); break;
+    case 2: go(k_lma_gather_tab<T, INC, 2, KC>); break;
+    case 4: go(k_lma_gather_tab<T, INC, 4, KC>); break;
+    case 8: go(k_lma_gather_tab<T, INC, 8, KC>); break;
+    default: go(k_lma_gather_tab<T, INC, 16, KC>); break;
+  }
+  after_launch(c, "lma_gather");
+}
+
 void upload_matrix(lfg_lma m, const double* ls) {
   const size_t n3 = (size_t)m->ncell * m->nl;
   const size_t n = n3 * m->ndf_to * m->ndf_from;
@@ -326,12 +429,18 @@ int lfg_lma_create(lfg_ctx c, int kind, int ncell, int nl, int ndf_to, int ndf_f
       m->off_to = dcopy(off);
       m->inc_to_ptr = dcopy(ptr);
       m->inc_to = dcopy(inc);
+      if (ndf_to <= kLocDf && ndf_from <= kLocDf)
+        m->tab_to_w = build_tab(off, ptr, inc, ndf_to, ncell, nlev_to, m->max_inc_to, false,
+                                &m->tab_to);
       build_space(map_from, ndf_from, ncell, nl, nent_from, nlev_from, ent, off, ptr, inc,
                   m->max_inc_from);
       m->ent_from = dcopy(ent);
       m->off_from = dcopy(off);
       m->inc_from_ptr = dcopy(ptr);
       m->inc_from = dcopy(inc);
+      if (ndf_to <= kLocDf && ndf_from <= kLocDf)
+        m->tab_from_w = build_tab(off, ptr, inc, ndf_from, ncell, nlev_from, m->max_inc_from,
+                                  true, &m->tab_from);
       m->a = dmalloc((size_t)ncell * nl * ndf_to * ndf_from * kind);
       upload_matrix(m, ls);
     } catch (...) {
@@ -346,7 +455,8 @@ int lfg_lma_destroy(lfg_lma m) {
   if (!m) return LFG_OK;
   for (void* p : {(void*)m->a, (void*)m->ent_to, (void*)m->off_to, (void*)m->ent_from,
                   (void*)m->off_from, (void*)m->inc_to_ptr, (void*)m->inc_to,
-                  (void*)m->inc_from_ptr, (void*)m->inc_from})
+                  (void*)m->inc_from_ptr, (void*)m->inc_from, (void*)m->tab_to,
+                  (void*)m->tab_from})
     dfree(p);
   delete m;
   return LFG_OK;
@@ -373,25 +483,27 @@ int lfg_lma_apply(lfg_lma m, int mode, lfg_field lhs, lfg_field x) {
                       x->ncol == m->nent_from && x->nlev == m->nlev_from,
                   "lma_apply: fields do not match the operator's spaces");
     }
-    // two-phase form for the forward applies (the one-pass transposed gather
-    // measured faster than its two-phase form on the W0 operator)
-    if (mode != LFG_LMA_TRANSPOSE && m->ndf_to <= kLocDf && m->ndf_from <= kLocDf) {
+    const bool tr = mode == LFG_LMA_TRANSPOSE;
+    // two-phase form: local products, then the padded-table gather
+    if (tr ? m->tab_from_w > 0 : m->tab_to_w > 0) {
       const size_t ncl = (size_t)m->ncell * m->nl;
       dispatch(m->kind, [&](auto tag) {
         using T = decltype(tag);
-        T* loc = (T*)c->scratch(ncl * m->ndf_to * sizeof(T));
-        k_lma_local<T, false><<<occ_grid(c, (const void*)k_lma_local<T, false>, 256, ncl), 256, 0,
-                                c->stream>>>(args_of<T>(m), (const T*)x->d, loc);
-        after_launch(c, "lma_local");
-        dim3 grid((m->nent_to + 127) / 128, m->nlev_to);
-        if (mode == LFG_LMA_INC)
-          k_lma_gather<T, true><<<grid, 128, 0, c->stream>>>(args_of<T>(m), m->inc_to_ptr,
-                                                             m->inc_to, loc, (T*)lhs->d);
-        else
-          k_lma_gather<T, false><<<grid, 128, 0, c->stream>>>(args_of<T>(m), m->inc_to_ptr,
-                                                              m->inc_to, loc, (T*)lhs->d);
+        T* loc = (T*)c->scratch(ncl * (tr ? m->ndf_from : m->ndf_to) * sizeof(T));
+        if (tr) {
+          launch_local<T, true>(c, m, (const T*)x->d, loc);
+          launch_gather_tab<T, true>(c, m->tab_from, m->tab_from_w, m->nent_from, m->nlev_from,
+                                     m->nl, m->ncell, loc, (T*)lhs->d);
+        } else {
+          launch_local<T, false>(c, m, (const T*)x->d, loc);
+          if (mode == LFG_LMA_INC)
+            launch_gather_tab<T, true>(c, m->tab_to, m->tab_to_w, m->nent_to, m->nlev_to, m->nl,
+                                       m->ncell, loc, (T*)lhs->d);
+          else
+            launch_gather_tab<T, false>(c, m->tab_to, m->tab_to_w, m->nent_to, m->nlev_to, m->nl,
+                                        m->ncell, loc, (T*)lhs->d);
+        }
       });
-      after_launch(c, "lma_gather");
       return;
     }
     dispatch(m->kind, [&](auto tag) {

@@ -44,10 +44,13 @@ def test_helmholtz_column_heights(ctx, n, nl, kind):
     ctx.synchronize()
 
 
-@pytest.mark.parametrize("nl,kind", [(1, R_DOUBLE), (2, R_SINGLE), (100, R_DOUBLE)])
+@pytest.mark.parametrize("nl,kind", [(1, R_DOUBLE), (2, R_SINGLE), (13, R_DOUBLE), (33, R_DOUBLE),
+                                     (33, R_SINGLE), (70, R_DOUBLE), (100, R_DOUBLE)])
 def test_cma_appinv_column_heights(ctx, nl, kind):
-    """columnwise_op_appinv for 1, 2 and 100 rows (the cached-factor
-    substitution keeps d' in shared memory up to 800 FP64 rows)."""
+    """columnwise_op_appinv for 1 to 100 rows: in FP64 one thread per
+    column up to 12 rows, then 2, 4 or 8 segments per column (13 rows leave
+    a short last segment), and one thread per column again above 96 rows
+    (d' in shared memory up to 800 FP64 rows); FP32 one thread per column."""
     ncol = 333
     dt = np.float64 if kind == R_DOUBLE else np.float32
     rng = np.random.default_rng(23)
