@@ -30,6 +30,7 @@
 #include <map>
 #include <mutex>
 #include <tuple>
+#include <type_traits>
 
 #include "lfg_internal.cuh"
 
@@ -188,6 +189,115 @@ __global__ void __launch_bounds__(TC) k_subst_tma(const __grid_constant__ TmaMap
   }
 }
 
+// The same sweep with d' in registers: NCH = ceil(nl / KCH) is fixed at
+// compile time, so each thread keeps its column's NCH*KCH values of d' in
+// a fully unrolled register array instead of shared memory.  The stages
+// are then all the shared memory a block needs, 3 blocks fit on an SM
+// instead of 2, and half as many bytes again are in flight.  The job
+// sequence, ring and bounded waits are those of k_subst_tma.
+constexpr int kRegChunks = 5;  // register form up to kRegChunks * KCH levels
+template <bool XIN, int NCH>
+__global__ void __launch_bounds__(TC, 3) k_subst_tma_reg(const __grid_constant__ TmaMaps maps,
+                                                         int ncol, int nl, float omega,
+                                                         float* __restrict__ xout,
+                                                         unsigned* err) {
+  extern __shared__ __align__(128) unsigned char smem[];
+  float* stage = reinterpret_cast<float*>(smem);  // [NST][NARR][KCH][TC]
+  __shared__ __align__(8) unsigned long long full[NST];
+  __shared__ int s_abort;
+  const int t = threadIdx.x;
+  constexpr int nch = NCH;
+  const int ntile = (ncol + TC - 1) / TC;
+  const int my_tiles = blockIdx.x < ntile ? (ntile - 1 - blockIdx.x) / gridDim.x + 1 : 0;
+  const int njobs = my_tiles * 2 * nch;
+  if (t == 0) {
+    for (int s = 0; s < NST; ++s) mbar_init(&full[s], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    s_abort = 0;
+  }
+  __syncthreads();
+  auto issue = [&](int j) {
+    const int s = j % NST;
+    const int tile = blockIdx.x + (j / (2 * nch)) * gridDim.x;
+    const int q = j % (2 * nch);
+    const bool fwd = q < nch;
+    const int chunk = fwd ? q : 2 * nch - 1 - q;
+    const int c0 = tile * TC, k0 = chunk * KCH;
+    float* dst = stage + (size_t)s * NARR * KCH * TC;
+    const int narr = fwd ? 3 : (XIN ? 2 : 1);
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    mbar_expect_tx(&full[s], (unsigned)(narr * KCH * TC * sizeof(float)));
+    if (fwd) {
+      tma_load_2d(dst, &maps.r, c0, k0, &full[s]);
+      tma_load_2d(dst + KCH * TC, &maps.inv, c0, k0, &full[s]);
+      tma_load_2d(dst + 2 * KCH * TC, &maps.sub, c0, k0, &full[s]);
+    } else {
+      tma_load_2d(dst, &maps.cp, c0, k0, &full[s]);
+      if (XIN) tma_load_2d(dst + KCH * TC, &maps.xin, c0, k0, &full[s]);
+    }
+  };
+  // wait for job j's stage; false (for the whole block) when a wait ran out
+  auto acquire = [&](int j) {
+    if (!mbar_wait_bounded(&full[j % NST], (unsigned)((j / NST) & 1))) {
+      atomicCAS(err, 0u, kErrTmaWait);
+      s_abort = 1;
+    }
+    __syncthreads();
+    return s_abort == 0;
+  };
+  auto release = [&](int j) {
+    __syncthreads();  // the stage has been read by every thread
+    if (t == 0 && j + NST < njobs) issue(j + NST);
+  };
+  if (t == 0)
+    for (int j = 0; j < NST && j < njobs; ++j) issue(j);
+  const float om1 = 1.f - omega;
+  int j = 0;
+  bool ok = true;
+  for (int it = 0; it < my_tiles && ok; ++it) {
+    const int c = (blockIdx.x + it * gridDim.x) * TC + t;
+    float dreg[NCH * KCH];
+    float d = 0.f;
+#pragma unroll
+    for (int q = 0; q < NCH; ++q) {
+      if (!(ok = acquire(j))) break;
+      const float* st = stage + (size_t)(j % NST) * NARR * KCH * TC;
+#pragma unroll
+      for (int u = 0; u < KCH; ++u) {
+        const int k = q * KCH + u;
+        const float rv = st[u * TC + t], iv = st[(KCH + u) * TC + t],
+                    sb = st[(2 * KCH + u) * TC + t];
+        if (k < nl) d = k == 0 ? iv * rv : iv * (rv - sb * d);
+        dreg[k] = d;
+      }
+      release(j++);
+    }
+    if (!ok) break;
+    float z = 0.f;
+#pragma unroll
+    for (int q = NCH - 1; q >= 0; --q) {
+      if (!(ok = acquire(j))) break;
+      const float* st = stage + (size_t)(j % NST) * NARR * KCH * TC;
+#pragma unroll
+      for (int u = KCH - 1; u >= 0; --u) {
+        const int k = q * KCH + u;
+        if (k < nl) {
+          z = (k == nl - 1) ? dreg[k] : dreg[k] - st[u * TC + t] * z;
+          float v = omega * z;
+          if (XIN) v = v + om1 * st[(KCH + u) * TC + t];
+          if (c < ncol) xout[(size_t)k * ncol + c] = v;
+        }
+      }
+      release(j++);
+    }
+  }
+  if (!ok && t == 0) {
+    // drain the loads this block has issued (bounded) before leaving
+    for (int i = j; i < njobs && i < j + NST; ++i)
+      mbar_wait_bounded(&full[i % NST], (unsigned)((i / NST) & 1));
+  }
+}
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
   static std::once_flag once;
@@ -241,6 +351,43 @@ void subst_tma(lfg_ctx c, int ncol, int nl, const float* r, const float* sub, co
   maps.sub = make_map(sub, ncol, nl);
   maps.cp = make_map(cp, ncol, nl);
   maps.xin = make_map(xin ? xin : cp, ncol, nl);
+  const int nch = (nl + KCH - 1) / KCH;
+  if (nch <= kRegChunks) {
+    const size_t smem = sizeof(float) * (size_t)NST * NARR * KCH * TC;
+    static std::once_flag attr_reg;
+    std::call_once(attr_reg, [&] {
+      const void* all[] = {
+          (const void*)k_subst_tma_reg<false, 1>, (const void*)k_subst_tma_reg<false, 2>,
+          (const void*)k_subst_tma_reg<false, 3>, (const void*)k_subst_tma_reg<false, 4>,
+          (const void*)k_subst_tma_reg<false, 5>, (const void*)k_subst_tma_reg<true, 1>,
+          (const void*)k_subst_tma_reg<true, 2>,  (const void*)k_subst_tma_reg<true, 3>,
+          (const void*)k_subst_tma_reg<true, 4>,  (const void*)k_subst_tma_reg<true, 5>};
+      for (const void* k : all)
+        LFG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem));
+    });
+    auto go = [&](auto kern) {
+      int per_sm = 0;
+      LFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TC, smem));
+      const int ntile = (ncol + TC - 1) / TC;
+      const int grid = std::max(1, std::min(ntile, c->num_sms * std::max(per_sm, 1)));
+      kern<<<grid, TC, smem, c->stream>>>(maps, ncol, nl, omega, xout, c->dev_err);
+    };
+    auto by_nch = [&](auto xtag) {
+      constexpr bool X = decltype(xtag)::value;
+      switch (nch) {
+        case 1: go(k_subst_tma_reg<X, 1>); break;
+        case 2: go(k_subst_tma_reg<X, 2>); break;
+        case 3: go(k_subst_tma_reg<X, 3>); break;
+        case 4: go(k_subst_tma_reg<X, 4>); break;
+        default: go(k_subst_tma_reg<X, 5>); break;
+      }
+    };
+    if (xin) by_nch(std::true_type{});
+    else by_nch(std::false_type{});
+    after_launch(c, "helm_subst_tma");
+    return;
+  }
   const size_t smem = smem_bytes(nl);
   const void* kern = xin ? (const void*)k_subst_tma<true> : (const void*)k_subst_tma<false>;
   static std::once_flag attr;
