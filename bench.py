@@ -313,7 +313,7 @@ def measure_kernels(ctx, stream, peak: float) -> list:
         b.import_(prob.rhs)
         wl = f"C{N_FINE}x{NLAYERS} {tag}"
         add("k_helm_apply (y = A x)", wl, 9 * N * w, time(lambda: H.apply(y, x)))
-        add("substitution from zero (k_subst_tma / k_helm_subst)", wl, 5 * N * w,
+        add("substitution from zero (k_subst_tma_reg FP32 / k_helm_subst FP64)", wl, 5 * N * w,
             time(lambda: H.smooth(0.8, None, b, y)))
         add("smoother sweep (k_helm_rhs + substitution)", wl, 13 * N * w,
             time(lambda: H.smooth(0.8, x, b, y)))
@@ -349,7 +349,7 @@ def measure_kernels(ctx, stream, peak: float) -> list:
         n = n96 * NLAYERS
         add("k_cma_app (columnwise_op_app)", f"C96x{NLAYERS} {tag}", 6 * n * w,
             time(lambda: A.apply(Y, X)))
-        add("k_thomas (columnwise_op_appinv)", f"C96x{NLAYERS} {tag}", 5 * n * w,
+        add("k_cma_subst_seg FP64 / k_cma_subst FP32 (columnwise_op_appinv)", f"C96x{NLAYERS} {tag}", 5 * n * w,
             time(lambda: A.apply_inverse(Y, X)))
         del A, X, Y
     # LMA W0 apply (matrix_vector, gather form) on the C48 x 30 W0 problem
@@ -361,9 +361,9 @@ def measure_kernels(ctx, stream, peak: float) -> list:
     X.set_scalar(1.0)
     Y.set_scalar(0.0)
     ncell3 = wp.ncell * wp.nlayers
-    add("k_lma_apply (matrix_vector, gather)", "C48x30 W0 FP64",
+    add("k_lma_local + k_lma_gather_tab (matrix_vector)", "C48x30 W0 FP64",
         (64 * ncell3 + 3 * wp.ndof) * 8, time(lambda: L.apply(api.LMA_INC, Y, X)))
-    add("k_lma_apply_t (transpose_matrix_vector)", "C48x30 W0 FP64",
+    add("k_lma_local + k_lma_gather_tab (transpose_matrix_vector)", "C48x30 W0 FP64",
         (64 * ncell3 + 3 * wp.ndof) * 8, time(lambda: L.apply(api.LMA_TRANSPOSE, Y, X)))
     return rows
 
@@ -480,8 +480,8 @@ def main():
     true_rel = R.norm() / system.b64.norm()
 
     # ---- roofline of the dominant kernel family: the column substitution
-    # (the zero-start smoother sweep is exactly one launch of it, k_subst_tma
-    # on FP32 fine meshes), on the C192 level; the full sweep from a nonzero
+    # (the zero-start smoother sweep is exactly one launch of it,
+    # k_subst_tma_reg on FP32 fine meshes), on the C192 level; the full sweep from a nonzero
     # guess (k_helm_rhs + the substitution) is timed beside it
     op32 = system.levels32[0]
     xs, bs, ys = op32.field(), op32.field(), op32.field()
@@ -560,12 +560,12 @@ def main():
                     "d2h_bytes_per_step": N * 8},
             "gpu_launches": launches,
             "roofline": {"bound": "hbm",
-                         "kernel": "k_subst_tma<false> zero-start column sweep (TMA-staged), C192x70",
+                         "kernel": "k_subst_tma_reg<false,5> zero-start column sweep (TMA-staged, d' in registers), C192x70",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "peak_source": peak_kind,
                          "traffic": traffic, "algorithmic_bytes": subst_bytes,
                          "ms_per_launch": subst_ms},
-            "smoother_sweep": {"kernels": "k_helm_rhs + k_subst_tma<true>, FP32, C192x70",
+            "smoother_sweep": {"kernels": "k_helm_rhs + k_subst_tma_reg<true,5>, FP32, C192x70",
                                "ms": sweep_ms, "algorithmic_bytes": sweep_bytes,
                                "GB/s": sweep_bytes / (sweep_ms * 1e-3) / 1e9},
             "batched": batched,
