@@ -191,9 +191,9 @@ __global__ void __launch_bounds__(256) k_helm_rhs(HelmArgs<T> A, const T* __rest
       for (int f = 0; f < 4; ++f) {
         T xn = xin[(size_t)k * N + nb[f]];
         if (PRO) xn = xn + xc[(size_t)k * ncoarse + pn[f]];
-        hs = hs + A.h[f * plane + i] * xn;
+        hs = hs + __ldcs(A.h + f * plane + i) * xn;
       }
-      out[kk] = b[i] + hs;
+      out[kk] = __ldcs(b + i) + hs;
     }
 #pragma unroll
     for (int kk = 0; kk < KC; ++kk)
