@@ -576,11 +576,10 @@ void launch_subst(lfg_ctx c, int ncol, int nl, const T* r, const T* sub, const T
   if ((size_t)nl * 32 * sizeof(T) > cap)
     throw Error(LFG_ERR_ARG, "helm_smooth: column too tall for shared memory");
   while ((size_t)nl * bs * sizeof(T) > cap) bs /= 2;
-  if constexpr (sizeof(T) == 4 && !PRO) {
+  if constexpr (!PRO) {
     const void* ptrs[5] = {r, sub, inv, cp, xin};
-    if (subst_tma_applicable(c, ncol, nl, ptrs, 5)) {
-      subst_tma(c, ncol, nl, (const float*)r, (const float*)sub, (const float*)inv,
-                (const float*)cp, XIN ? (const float*)xin : nullptr, (float)omega, (float*)xout);
+    if (subst_tma_applicable(c, ncol, nl, ptrs, 5, (int)sizeof(T))) {
+      subst_tma(c, ncol, nl, r, sub, inv, cp, XIN ? xin : nullptr, omega, xout);
       return;
     }
   }

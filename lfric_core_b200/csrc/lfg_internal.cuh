@@ -312,10 +312,15 @@ inline int occ_grid(lfg_ctx c, const void* kern, int threads, size_t work, size_
 // Throws LFG_ERR_STATE when a kernel recorded a device error (synchronises).
 void check_device_error(lfg_ctx c);
 
-// TMA-staged column substitution (lfg_subst_tma.cu), FP32 fine meshes.
-bool subst_tma_applicable(lfg_ctx c, int ncol, int nl, const void* const* ptrs, int nptr);
+// TMA-staged column substitution (lfg_subst_tma.cu), fine meshes; FP64
+// for columns of at most 80 levels.
+bool subst_tma_applicable(lfg_ctx c, int ncol, int nl, const void* const* ptrs, int nptr,
+                          int elem_bytes);
 void subst_tma(lfg_ctx c, int ncol, int nl, const float* r, const float* sub, const float* inv,
                const float* cp, const float* xin, float omega, float* xout);
+void subst_tma(lfg_ctx c, int ncol, int nl, const double* r, const double* sub,
+               const double* inv, const double* cp, const double* xin, double omega,
+               double* xout);
 
 // vector algebra launchers (lfg_core.cu)
 void vec_set(lfg_field x, Sc a);

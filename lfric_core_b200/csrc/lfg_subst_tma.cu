@@ -194,20 +194,25 @@ __global__ void __launch_bounds__(TC) k_subst_tma(const __grid_constant__ TmaMap
 // a fully unrolled register array instead of shared memory.  The stages
 // are then all the shared memory a block needs, 3 blocks fit on an SM
 // instead of 2, and half as many bytes again are in flight.  The job
-// sequence, ring and bounded waits are those of k_subst_tma.
+// sequence, ring and bounded waits are those of k_subst_tma.  T is float
+// (tiles of 128 columns) or double (tiles of 64): a box row is 512 bytes
+// and a stage 24 KB either way.
 constexpr int kRegChunks = 5;  // register form up to kRegChunks * KCH levels
-template <bool XIN, int NCH>
-__global__ void __launch_bounds__(TC, 3) k_subst_tma_reg(const __grid_constant__ TmaMaps maps,
-                                                         int ncol, int nl, float omega,
-                                                         float* __restrict__ xout,
-                                                         unsigned* err) {
+template <class T>
+__host__ __device__ constexpr int tile_cols() { return 512 / (int)sizeof(T); }
+
+template <class T, bool XIN, int NCH>
+__global__ void __launch_bounds__(tile_cols<T>(), 3)
+    k_subst_tma_reg(const __grid_constant__ TmaMaps maps, int ncol, int nl, T omega,
+                    T* __restrict__ xout, unsigned* err) {
+  constexpr int TCT = tile_cols<T>();
   extern __shared__ __align__(128) unsigned char smem[];
-  float* stage = reinterpret_cast<float*>(smem);  // [NST][NARR][KCH][TC]
+  T* stage = reinterpret_cast<T*>(smem);  // [NST][NARR][KCH][TCT]
   __shared__ __align__(8) unsigned long long full[NST];
   __shared__ int s_abort;
   const int t = threadIdx.x;
   constexpr int nch = NCH;
-  const int ntile = (ncol + TC - 1) / TC;
+  const int ntile = (ncol + TCT - 1) / TCT;
   const int my_tiles = blockIdx.x < ntile ? (ntile - 1 - blockIdx.x) / gridDim.x + 1 : 0;
   const int njobs = my_tiles * 2 * nch;
   if (t == 0) {
@@ -222,18 +227,18 @@ __global__ void __launch_bounds__(TC, 3) k_subst_tma_reg(const __grid_constant__
     const int q = j % (2 * nch);
     const bool fwd = q < nch;
     const int chunk = fwd ? q : 2 * nch - 1 - q;
-    const int c0 = tile * TC, k0 = chunk * KCH;
-    float* dst = stage + (size_t)s * NARR * KCH * TC;
+    const int c0 = tile * TCT, k0 = chunk * KCH;
+    T* dst = stage + (size_t)s * NARR * KCH * TCT;
     const int narr = fwd ? 3 : (XIN ? 2 : 1);
     asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    mbar_expect_tx(&full[s], (unsigned)(narr * KCH * TC * sizeof(float)));
+    mbar_expect_tx(&full[s], (unsigned)(narr * KCH * TCT * sizeof(T)));
     if (fwd) {
       tma_load_2d(dst, &maps.r, c0, k0, &full[s]);
-      tma_load_2d(dst + KCH * TC, &maps.inv, c0, k0, &full[s]);
-      tma_load_2d(dst + 2 * KCH * TC, &maps.sub, c0, k0, &full[s]);
+      tma_load_2d(dst + KCH * TCT, &maps.inv, c0, k0, &full[s]);
+      tma_load_2d(dst + 2 * KCH * TCT, &maps.sub, c0, k0, &full[s]);
     } else {
       tma_load_2d(dst, &maps.cp, c0, k0, &full[s]);
-      if (XIN) tma_load_2d(dst + KCH * TC, &maps.xin, c0, k0, &full[s]);
+      if (XIN) tma_load_2d(dst + KCH * TCT, &maps.xin, c0, k0, &full[s]);
     }
   };
   // wait for job j's stage; false (for the whole block) when a wait ran out
@@ -251,40 +256,40 @@ __global__ void __launch_bounds__(TC, 3) k_subst_tma_reg(const __grid_constant__
   };
   if (t == 0)
     for (int j = 0; j < NST && j < njobs; ++j) issue(j);
-  const float om1 = 1.f - omega;
+  const T om1 = (T)1 - omega;
   int j = 0;
   bool ok = true;
   for (int it = 0; it < my_tiles && ok; ++it) {
-    const int c = (blockIdx.x + it * gridDim.x) * TC + t;
-    float dreg[NCH * KCH];
-    float d = 0.f;
+    const int c = (blockIdx.x + it * gridDim.x) * TCT + t;
+    T dreg[NCH * KCH];
+    T d = (T)0;
 #pragma unroll
     for (int q = 0; q < NCH; ++q) {
       if (!(ok = acquire(j))) break;
-      const float* st = stage + (size_t)(j % NST) * NARR * KCH * TC;
+      const T* st = stage + (size_t)(j % NST) * NARR * KCH * TCT;
 #pragma unroll
       for (int u = 0; u < KCH; ++u) {
         const int k = q * KCH + u;
-        const float rv = st[u * TC + t], iv = st[(KCH + u) * TC + t],
-                    sb = st[(2 * KCH + u) * TC + t];
+        const T rv = st[u * TCT + t], iv = st[(KCH + u) * TCT + t],
+                sb = st[(2 * KCH + u) * TCT + t];
         if (k < nl) d = k == 0 ? iv * rv : iv * (rv - sb * d);
         dreg[k] = d;
       }
       release(j++);
     }
     if (!ok) break;
-    float z = 0.f;
+    T z = (T)0;
 #pragma unroll
     for (int q = NCH - 1; q >= 0; --q) {
       if (!(ok = acquire(j))) break;
-      const float* st = stage + (size_t)(j % NST) * NARR * KCH * TC;
+      const T* st = stage + (size_t)(j % NST) * NARR * KCH * TCT;
 #pragma unroll
       for (int u = KCH - 1; u >= 0; --u) {
         const int k = q * KCH + u;
         if (k < nl) {
-          z = (k == nl - 1) ? dreg[k] : dreg[k] - st[u * TC + t] * z;
-          float v = omega * z;
-          if (XIN) v = v + om1 * st[(KCH + u) * TC + t];
+          z = (k == nl - 1) ? dreg[k] : dreg[k] - st[u * TCT + t] * z;
+          T v = omega * z;
+          if (XIN) v = v + om1 * st[(KCH + u) * TCT + t];
           if (c < ncol) xout[(size_t)k * ncol + c] = v;
         }
       }
@@ -312,15 +317,19 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
   return fn;
 }
 
-// 2-D tensor map over a level-major FP32 array [nl][ncol], box KCH x TC.
-CUtensorMap make_map(const float* base, int ncol, int nl) {
+// 2-D tensor map over a level-major array [nl][ncol] of T, box KCH levels
+// x tile_cols<T>() columns (512 bytes).
+template <class T>
+CUtensorMap make_map(const T* base, int ncol, int nl) {
   CUtensorMap m;
   std::memset(&m, 0, sizeof(m));
   const cuuint64_t dims[2] = {(cuuint64_t)ncol, (cuuint64_t)nl};
-  const cuuint64_t strides[1] = {(cuuint64_t)ncol * sizeof(float)};
-  const cuuint32_t box[2] = {(cuuint32_t)TC, (cuuint32_t)KCH};
+  const cuuint64_t strides[1] = {(cuuint64_t)ncol * sizeof(T)};
+  const cuuint32_t box[2] = {(cuuint32_t)tile_cols<T>(), (cuuint32_t)KCH};
   const cuuint32_t estr[2] = {1, 1};
-  const CUresult r = encode_fn()(&m, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void*)base, dims,
+  const CUtensorMapDataType dt =
+      sizeof(T) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  const CUresult r = encode_fn()(&m, dt, 2, (void*)base, dims,
                                  strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
                                  CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                                  CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
@@ -334,58 +343,82 @@ size_t smem_bytes(int nl) {
 
 }  // namespace
 
-bool subst_tma_applicable(lfg_ctx c, int ncol, int nl, const void* const* ptrs, int nptr) {
-  if (!c->dev_err || ncol % 4 != 0 || ncol < 2 * TC || nl < 1 || nl > kMaxLevels) return false;
+bool subst_tma_applicable(lfg_ctx c, int ncol, int nl, const void* const* ptrs, int nptr,
+                          int elem_bytes) {
+  if (!c->dev_err || nl < 1 || nl > kMaxLevels) return false;
+  if (elem_bytes == 4) {
+    if (ncol % 4 != 0 || ncol < 2 * TC) return false;
+  } else {  // FP64: the register form only
+    if (elem_bytes != 8 || ncol % 2 != 0 || ncol < 2 * tile_cols<double>() ||
+        nl > kRegChunks * KCH)
+      return false;
+  }
   for (int i = 0; i < nptr; ++i)
     if (ptrs[i] && reinterpret_cast<uintptr_t>(ptrs[i]) % 16 != 0) return false;
   return encode_fn() != nullptr;
 }
 
-// Launches the TMA substitution; xin may be null (zero start).  The caller
-// checked subst_tma_applicable.
-void subst_tma(lfg_ctx c, int ncol, int nl, const float* r, const float* sub, const float* inv,
-               const float* cp, const float* xin, float omega, float* xout) {
+namespace {
+
+template <class T>
+void launch_reg(lfg_ctx c, const TmaMaps& maps, int ncol, int nl, bool xin, T omega, T* xout) {
+  constexpr int TCT = tile_cols<T>();
+  const int nch = (nl + KCH - 1) / KCH;
+  const size_t smem = sizeof(T) * (size_t)NST * NARR * KCH * TCT;
+  static std::once_flag attr_reg;
+  std::call_once(attr_reg, [&] {
+    const void* all[] = {
+        (const void*)k_subst_tma_reg<T, false, 1>, (const void*)k_subst_tma_reg<T, false, 2>,
+        (const void*)k_subst_tma_reg<T, false, 3>, (const void*)k_subst_tma_reg<T, false, 4>,
+        (const void*)k_subst_tma_reg<T, false, 5>, (const void*)k_subst_tma_reg<T, true, 1>,
+        (const void*)k_subst_tma_reg<T, true, 2>,  (const void*)k_subst_tma_reg<T, true, 3>,
+        (const void*)k_subst_tma_reg<T, true, 4>,  (const void*)k_subst_tma_reg<T, true, 5>};
+    for (const void* k : all)
+      LFG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  });
+  auto go = [&](auto kern) {
+    int per_sm = 0;
+    LFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TCT, smem));
+    const int ntile = (ncol + TCT - 1) / TCT;
+    const int grid = std::max(1, std::min(ntile, c->num_sms * std::max(per_sm, 1)));
+    kern<<<grid, TCT, smem, c->stream>>>(maps, ncol, nl, omega, xout, c->dev_err);
+  };
+  auto by_nch = [&](auto xtag) {
+    constexpr bool X = decltype(xtag)::value;
+    switch (nch) {
+      case 1: go(k_subst_tma_reg<T, X, 1>); break;
+      case 2: go(k_subst_tma_reg<T, X, 2>); break;
+      case 3: go(k_subst_tma_reg<T, X, 3>); break;
+      case 4: go(k_subst_tma_reg<T, X, 4>); break;
+      default: go(k_subst_tma_reg<T, X, 5>); break;
+    }
+  };
+  if (xin) by_nch(std::true_type{});
+  else by_nch(std::false_type{});
+  after_launch(c, "helm_subst_tma");
+}
+
+template <class T>
+TmaMaps maps_of(int ncol, int nl, const T* r, const T* sub, const T* inv, const T* cp,
+                const T* xin) {
   TmaMaps maps;
   maps.r = make_map(r, ncol, nl);
   maps.inv = make_map(inv, ncol, nl);
   maps.sub = make_map(sub, ncol, nl);
   maps.cp = make_map(cp, ncol, nl);
   maps.xin = make_map(xin ? xin : cp, ncol, nl);
-  const int nch = (nl + KCH - 1) / KCH;
-  if (nch <= kRegChunks) {
-    const size_t smem = sizeof(float) * (size_t)NST * NARR * KCH * TC;
-    static std::once_flag attr_reg;
-    std::call_once(attr_reg, [&] {
-      const void* all[] = {
-          (const void*)k_subst_tma_reg<false, 1>, (const void*)k_subst_tma_reg<false, 2>,
-          (const void*)k_subst_tma_reg<false, 3>, (const void*)k_subst_tma_reg<false, 4>,
-          (const void*)k_subst_tma_reg<false, 5>, (const void*)k_subst_tma_reg<true, 1>,
-          (const void*)k_subst_tma_reg<true, 2>,  (const void*)k_subst_tma_reg<true, 3>,
-          (const void*)k_subst_tma_reg<true, 4>,  (const void*)k_subst_tma_reg<true, 5>};
-      for (const void* k : all)
-        LFG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      (int)smem));
-    });
-    auto go = [&](auto kern) {
-      int per_sm = 0;
-      LFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TC, smem));
-      const int ntile = (ncol + TC - 1) / TC;
-      const int grid = std::max(1, std::min(ntile, c->num_sms * std::max(per_sm, 1)));
-      kern<<<grid, TC, smem, c->stream>>>(maps, ncol, nl, omega, xout, c->dev_err);
-    };
-    auto by_nch = [&](auto xtag) {
-      constexpr bool X = decltype(xtag)::value;
-      switch (nch) {
-        case 1: go(k_subst_tma_reg<X, 1>); break;
-        case 2: go(k_subst_tma_reg<X, 2>); break;
-        case 3: go(k_subst_tma_reg<X, 3>); break;
-        case 4: go(k_subst_tma_reg<X, 4>); break;
-        default: go(k_subst_tma_reg<X, 5>); break;
-      }
-    };
-    if (xin) by_nch(std::true_type{});
-    else by_nch(std::false_type{});
-    after_launch(c, "helm_subst_tma");
+  return maps;
+}
+
+}  // namespace
+
+// Launches the TMA substitution; xin may be null (zero start).  The caller
+// checked subst_tma_applicable.
+void subst_tma(lfg_ctx c, int ncol, int nl, const float* r, const float* sub, const float* inv,
+               const float* cp, const float* xin, float omega, float* xout) {
+  const TmaMaps maps = maps_of(ncol, nl, r, sub, inv, cp, xin);
+  if ((nl + KCH - 1) / KCH <= kRegChunks) {
+    launch_reg<float>(c, maps, ncol, nl, xin != nullptr, omega, xout);
     return;
   }
   const size_t smem = smem_bytes(nl);
@@ -405,6 +438,13 @@ void subst_tma(lfg_ctx c, int ncol, int nl, const float* r, const float* sub, co
   else
     k_subst_tma<false><<<grid, TC, smem, c->stream>>>(maps, ncol, nl, omega, xout, c->dev_err);
   after_launch(c, "helm_subst_tma");
+}
+
+void subst_tma(lfg_ctx c, int ncol, int nl, const double* r, const double* sub,
+               const double* inv, const double* cp, const double* xin, double omega,
+               double* xout) {
+  launch_reg<double>(c, maps_of(ncol, nl, r, sub, inv, cp, xin), ncol, nl, xin != nullptr,
+                     omega, xout);
 }
 
 }  // namespace lfg
