@@ -225,7 +225,8 @@ __device__ void finish_problem(const BArgs& a, int pi, const BProb& P, int mode)
 // forward-substitution values, stride TC.  Levels go in chunks of U whose
 // loads are all issued before any arithmetic (indices clamped into the
 // column, so no load waits behind a branch).
-constexpr int kU = 4;    // FP32 phases
+constexpr int kU = 8;    // FP32 phases (6 loads a level)
+constexpr int kUB = 16;  // the backward substitutions (2 loads a level)
 constexpr int kUA = 2;   // the apply phase (17 loads a level)
 constexpr int kU64 = 2;  // the FP64 residual phase
 
@@ -296,16 +297,16 @@ __device__ __forceinline__ void column_step(const BProb& P, const BState* st, in
         }
       }
       float zn = 0.f;
-      for (int k1 = nl - 1; k1 >= 0; k1 -= kU) {
-        float vc[kU], vr[kU];
+      for (int k1 = nl - 1; k1 >= 0; k1 -= kUB) {
+        float vc[kUB], vr[kUB];
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
+        for (int u = 0; u < kUB; ++u) {
           const size_t i = (size_t)max(k1 - u, 0) * N + c;
           vc[u] = __ldg(cp + i);
           vr[u] = r[i];
         }
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
+        for (int u = 0; u < kUB; ++u) {
           const int k = k1 - u;
           if (k >= 0) {
             const size_t i = (size_t)k * N + c;
@@ -404,16 +405,16 @@ __device__ __forceinline__ void column_step(const BProb& P, const BState* st, in
         }
       }
       float zn = 0.f;
-      for (int k1 = nl - 1; k1 >= 0; k1 -= kU) {
-        float vc[kU], vr[kU];
+      for (int k1 = nl - 1; k1 >= 0; k1 -= kUB) {
+        float vc[kUB], vr[kUB];
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
+        for (int u = 0; u < kUB; ++u) {
           const size_t i = (size_t)max(k1 - u, 0) * N + c;
           vc[u] = __ldg(cp + i);
           vr[u] = r[i];
         }
 #pragma unroll
-        for (int u = 0; u < kU; ++u) {
+        for (int u = 0; u < kUB; ++u) {
           const int k = k1 - u;
           if (k >= 0) {
             const float zv = dps[k * TC] - vc[u] * zn;
