@@ -432,7 +432,7 @@ def main():
     def timed(fn, steps):
         barrier()
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        n0 = ctx.kernel_launches()
+        n0, b0 = ctx.kernel_launches(), ctx.algorithmic_bytes()
         e0.record(stream)
         last = None
         for _ in range(steps):
@@ -440,6 +440,7 @@ def main():
         e1.record(stream)
         barrier()
         ms = max_over_ranks(e0.elapsed_time(e1), world)
+        timed.bytes = (ctx.algorithmic_bytes() - b0) / steps
         return ms, ctx.kernel_launches() - n0, last
 
     # ---- warm-up (both forms)
@@ -451,10 +452,12 @@ def main():
     with ClockSampler(dev) as clk:
         torch.cuda.nvtx.range_push("timed_mixed")
         ms_mixed, launches, res_m = timed(system.solve_mixed, args.steps)
+        bytes_mixed = timed.bytes
         torch.cuda.nvtx.range_pop()
     # ---- plain FP64 drop-in
     torch.cuda.nvtx.range_push("timed_fp64")
     ms_fp64, launches64, res_64 = timed(system.solve_fp64, args.steps)
+    bytes_fp64 = timed.bytes
     torch.cuda.nvtx.range_pop()
 
     # ---- e2e through the ABI with host buffers (pinned)
@@ -559,6 +562,13 @@ def main():
             "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": N * 8,
                     "d2h_bytes_per_step": N * 8},
             "gpu_launches": launches,
+            # every kernel of a solve: the algorithmic bytes the library
+            # counts per launch (each array read once, written once) over
+            # the solve's time, against the measured copy bandwidth
+            "solve_level": {
+                form: {"algorithmic_bytes_per_solve": nb, "GB/s": nb / (ms * 1e-3 / args.steps) / 1e9,
+                       "frac": nb / (ms * 1e-3 / args.steps) / 1e9 / peak}
+                for form, nb, ms in (("mixed", bytes_mixed, ms_mixed), ("fp64", bytes_fp64, ms_fp64))},
             "roofline": {"bound": "hbm",
                          "kernel": "k_subst_tma_reg<false,5> zero-start column sweep (TMA-staged, d' in registers), C192x70",
                          "achieved": achieved, "peak": peak, "unit": "GB/s",

@@ -67,6 +67,13 @@ int lfg_ctx_set_stream(lfg_ctx ctx, void* stream);
 int lfg_ctx_synchronize(lfg_ctx ctx);
 /* Number of kernels this library has launched on the context so far. */
 int lfg_ctx_kernel_launches(lfg_ctx ctx, uint64_t* count);
+/* Algorithmic bytes of those kernels: every array a kernel reads counted
+ * once and every array it writes counted once, at its stored precision
+ * (index maps not counted); kernels replayed from a solver's CUDA graphs
+ * count each replay.  Divided by a solve's time it gives the solve-level
+ * bandwidth.  A diagnostic of this library, with no counterpart in the
+ * reference. */
+int lfg_ctx_algorithmic_bytes(lfg_ctx ctx, uint64_t* bytes);
 /* Message of the last failed call on this context (never NULL). */
 const char* lfg_last_error(lfg_ctx ctx);
 /* Library version string and the compute capability it was built for. */

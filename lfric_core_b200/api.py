@@ -90,6 +90,13 @@ class Context:
         self.check(self.lib.lfg_ctx_kernel_launches(self.h, C.byref(n)))
         return n.value
 
+    def algorithmic_bytes(self) -> int:
+        """Bytes the launched kernels must move at least: each array a kernel
+        reads or writes counted once, at its stored precision."""
+        n = C.c_uint64()
+        self.check(self.lib.lfg_ctx_algorithmic_bytes(self.h, C.byref(n)))
+        return n.value
+
     def close(self):
         if getattr(self, "h", None):
             self.lib.lfg_ctx_destroy(self.h)

@@ -350,7 +350,8 @@ void launch_thomas_t(lfg_ctx c, const TriSrc<T>& s, const T* x, T* lhs) {
     attr = true;
   }
   kern<<<(s.ncol + bs - 1) / bs, bs, smem, c->stream>>>(s, x, lhs);
-  after_launch(c, "thomas");
+  // three bands and x read, the solution written
+  after_launch(c, "thomas", sizeof(T) * 5 * (uint64_t)s.nrow * s.ncol);
 }
 
 template <class T, int SRC>
@@ -362,7 +363,7 @@ void launch_thomas(lfg_ctx c, const TriSrc<T>& s, const T* x, T* lhs) {
     T* scratch = (T*)c->scratch(2 * (size_t)s.nrow * s.ncol * sizeof(T));
     const int bs = 128;
     k_thomas_scratch<T, SRC><<<(s.ncol + bs - 1) / bs, bs, 0, c->stream>>>(s, x, lhs, scratch);
-    after_launch(c, "thomas_scratch");
+    after_launch(c, "thomas_scratch", sizeof(T) * 5 * (uint64_t)s.nrow * s.ncol);
   }
 }
 
@@ -663,7 +664,7 @@ int lfg_cma_apply(lfg_cma m, lfg_field lhs, lfg_field x) {
                                                 m->jminus, m->jplus, m->ncol, m->nrow,
                                                 m->ncolumn, (const T*)x->d, (T*)lhs->d);
     });
-    after_launch(c, "cma_app");
+    after_launch(c, "cma_app", (uint64_t)m->kind * m->ncol * ((uint64_t)(m->bw + 2) * m->nrow + m->ncolumn));
   });
 }
 
@@ -682,7 +683,7 @@ int lfg_cma_apply_transpose(lfg_cma m, lfg_field lhs, lfg_field x) {
                                                   m->jminus, m->tptr, m->trow, m->ncol, m->nrow,
                                                   (const T*)x->d, (T*)lhs->d);
     });
-    after_launch(c, "cma_app_t");
+    after_launch(c, "cma_app_t", (uint64_t)m->kind * m->ncol * ((uint64_t)(m->bw + 1) * m->nrow + 2 * (uint64_t)m->ncolumn));
   });
 }
 
@@ -716,7 +717,7 @@ int lfg_cma_apply_inverse(lfg_cma m, lfg_field lhs, lfg_field x) {
         k_cma_factor<T><<<(m->ncol + 127) / 128, 128, 0, c->stream>>>(
             (const T*)m->bands, m->ncol, m->nrow, (T*)m->finv, (T*)m->fcp);
       });
-      after_launch(c, "cma_factor");
+      after_launch(c, "cma_factor", (uint64_t)m->kind * 5 * m->ncol * m->nrow);
       m->fvalid = true;
     }
     // FP64: segmented form; FP32 columns (half the bytes per row) measured
@@ -734,7 +735,7 @@ int lfg_cma_apply_inverse(lfg_cma m, lfg_field lhs, lfg_field x) {
         else if (S == 4) go(k_cma_subst_seg<T, 4>);
         else go(k_cma_subst_seg<T, 8>);
       });
-      after_launch(c, "cma_subst_seg");
+      after_launch(c, "cma_subst_seg", (uint64_t)m->kind * 5 * m->ncol * m->nrow);
       return;
     }
     int bs = 128;
@@ -751,7 +752,7 @@ int lfg_cma_apply_inverse(lfg_cma m, lfg_field lhs, lfg_field x) {
           (const T*)m->bands, (const T*)m->finv, (const T*)m->fcp, m->ind_to, m->ncol, m->nrow,
           (const T*)x->d, (T*)lhs->d);
     });
-    after_launch(c, "cma_subst");
+    after_launch(c, "cma_subst", (uint64_t)m->kind * 5 * m->ncol * m->nrow);
   });
 }
 
@@ -927,7 +928,10 @@ int lfg_restrict_scalar(lfg_intergrid g, int mode, lfg_field coarse, lfg_field f
       else
         k_restrict<T, LFG_RESTRICT_MASS_W3><<<grid, 128, 0, c->stream>>>((T*)coarse->d, (const T*)fine->d, wp, g->child, g->ncoarse, g->nfine, nq, fine->nlev);
     });
-    after_launch(c, "restrict_scalar");
+    // fine read (and its weights), coarse written
+    after_launch(c, "restrict_scalar",
+                 (uint64_t)fine->kind * fine->nlev *
+                     ((uint64_t)g->nfine * (mode == LFG_RESTRICT_WEIGHTED ? 2 : 1) + g->ncoarse));
   });
 }
 
@@ -952,7 +956,10 @@ int lfg_prolong_scalar(lfg_intergrid g, lfg_field fine, lfg_field coarse, lfg_fi
       if (w) go(k_prolong<T, true>);
       else go(k_prolong<T, false>);
     });
-    after_launch(c, "prolong_scalar");
+    // fine read and written (weights read), coarse read
+    after_launch(c, "prolong_scalar",
+                 (uint64_t)fine->kind * fine->nlev *
+                     ((uint64_t)g->nfine * (w ? 3 : 2) + g->ncoarse));
   });
 }
 
@@ -971,7 +978,7 @@ int lfg_restrict_w0(lfg_intergrid g, lfg_field coarse, lfg_field fine) {
       k_restrict_w0<T><<<grid, 128, 0, c->stream>>>((T*)coarse->d, (const T*)fine->d, g->w0_inj,
                                                     g->nvert_coarse, g->nvert_fine, fine->nlev);
     });
-    after_launch(c, "restrict_w0");
+    after_launch(c, "restrict_w0", (uint64_t)fine->kind * fine->nlev * 2 * g->nvert_coarse);
   });
 }
 
@@ -991,7 +998,8 @@ int lfg_prolong_w0(lfg_intergrid g, lfg_field fine, lfg_field coarse) {
                                                    g->w0_w, g->ccorner, g->nvert_fine,
                                                    g->nvert_coarse, g->ncoarse, fine->nlev);
     });
-    after_launch(c, "prolong_w0");
+    after_launch(c, "prolong_w0",
+                 (uint64_t)fine->kind * fine->nlev * ((uint64_t)g->nvert_fine + g->nvert_coarse));
   });
 }
 

@@ -478,21 +478,23 @@ static void same_kind(lfg_field a, lfg_field b, const char* what) {
   LFG_REQUIRE(a->kind == b->kind, std::string(what) + ": fields differ in kind");
 }
 
+// words: arrays the operation reads plus arrays it writes (n values each)
 template <class T, class Op>
-void launch_ew(lfg_ctx c, const Op& op, size_t n, bool vec, const char* what) {
+void launch_ew(lfg_ctx c, const Op& op, size_t n, bool vec, const char* what, int words) {
   const size_t work = vec ? n / kVec<T> + n % kVec<T> : n;
   k_ew<T, Op><<<occ_grid(c, (const void*)k_ew<T, Op>, kThreads, work), kThreads, 0, c->stream>>>(
       op, n, vec);
-  after_launch(c, what);
+  after_launch(c, what, (uint64_t)words * n * sizeof(T));
 }
 
 template <class T, class Op>
-void launch_ewr(lfg_ctx c, const Op& op, size_t n, bool vec, int slot, const char* what) {
+void launch_ewr(lfg_ctx c, const Op& op, size_t n, bool vec, int slot, const char* what,
+                int words) {
   const size_t work = vec ? n / kVec<T> + n % kVec<T> : n;
   // the reduction's partials live in kMaxRedBlocks slots per reduction
   const int g = std::min(occ_grid(c, (const void*)k_ewr<T, Op>, kThreads, work), kMaxRedBlocks);
   k_ewr<T, Op><<<g, kThreads, 0, c->stream>>>(op, n, vec, c->red(slot));
-  after_launch(c, what);
+  after_launch(c, what, (uint64_t)words * n * sizeof(T));
 }
 
 template <class... P>
@@ -502,7 +504,7 @@ bool all_aligned(const P*... p) {
 
 void vec_set(lfg_field x, Sc a) {
   lfg_ctx c = x->ctx;
-  DISPATCH_KIND(x->kind, T, launch_ew<T>(c, SetOp<T>{(T*)x->d, a}, x->n(), all_aligned(x->d), "set"));
+  DISPATCH_KIND(x->kind, T, launch_ew<T>(c, SetOp<T>{(T*)x->d, a}, x->n(), all_aligned(x->d), "set", 1));
 }
 
 void vec_copy(lfg_field dst, lfg_field src) {
@@ -511,7 +513,7 @@ void vec_copy(lfg_field dst, lfg_field src) {
   if (dst->kind == src->kind) {
     DISPATCH_KIND(dst->kind, T,
                   launch_ew<T>(c, CopyOp<T>{(T*)dst->d, (const T*)src->d}, dst->n(),
-                               all_aligned(dst->d, src->d), "copy"));
+                               all_aligned(dst->d, src->d), "copy", 2));
     return;
   }
   const int g = c->stream_grid(dst->n());
@@ -519,7 +521,7 @@ void vec_copy(lfg_field dst, lfg_field src) {
     k_copy<double, float><<<g, kThreads, 0, c->stream>>>((double*)dst->d, (const float*)src->d, dst->n());
   else
     k_copy<float, double><<<g, kThreads, 0, c->stream>>>((float*)dst->d, (const double*)src->d, dst->n());
-  after_launch(c, "copy");
+  after_launch(c, "copy", (uint64_t)dst->n() * (dst->kind + src->kind));
 }
 
 void vec_axpy(lfg_field x, Sc b, lfg_field y) {
@@ -528,7 +530,7 @@ void vec_axpy(lfg_field x, Sc b, lfg_field y) {
   if (x->kind == y->kind) {
     DISPATCH_KIND(x->kind, T,
                   launch_ew<T>(c, AxpyOp<T>{(T*)x->d, (const T*)y->d, b}, x->n(),
-                               all_aligned(x->d, y->d), "axpy"));
+                               all_aligned(x->d, y->d), "axpy", 3));
     return;
   }
   const int g = c->stream_grid(x->n());
@@ -536,7 +538,7 @@ void vec_axpy(lfg_field x, Sc b, lfg_field y) {
     k_axpy<double, float><<<g, kThreads, 0, c->stream>>>((double*)x->d, (const float*)y->d, x->n(), b);
   else
     k_axpy<float, double><<<g, kThreads, 0, c->stream>>>((float*)x->d, (const double*)y->d, x->n(), b);
-  after_launch(c, "axpy");
+  after_launch(c, "axpy", (uint64_t)x->n() * (2 * x->kind + y->kind));
 }
 
 void vec_aypx(lfg_field x, Sc a, lfg_field y) {
@@ -544,7 +546,7 @@ void vec_aypx(lfg_field x, Sc a, lfg_field y) {
   lfg_ctx c = x->ctx;
   DISPATCH_KIND(x->kind, T,
                 launch_ew<T>(c, AypxOp<T>{(T*)x->d, (const T*)y->d, a}, x->n(),
-                             all_aligned(x->d, y->d), "aypx"));
+                             all_aligned(x->d, y->d), "aypx", 3));
 }
 
 void vec_axpby(lfg_field z, Sc a, lfg_field x, Sc b, lfg_field y) {
@@ -553,13 +555,13 @@ void vec_axpby(lfg_field z, Sc a, lfg_field x, Sc b, lfg_field y) {
   lfg_ctx c = z->ctx;
   DISPATCH_KIND(z->kind, T,
                 launch_ew<T>(c, AxpbyOp<T>{(T*)z->d, (const T*)x->d, (const T*)y->d, a, b},
-                             z->n(), all_aligned(z->d, x->d, y->d), "axpby"));
+                             z->n(), all_aligned(z->d, x->d, y->d), "axpby", 3));
 }
 
 void vec_scale(lfg_field x, Sc a) {
   lfg_ctx c = x->ctx;
   DISPATCH_KIND(x->kind, T,
-                launch_ew<T>(c, ScaleOp<T>{(T*)x->d, a}, x->n(), all_aligned(x->d), "scale"));
+                launch_ew<T>(c, ScaleOp<T>{(T*)x->d, a}, x->n(), all_aligned(x->d), "scale", 2));
 }
 
 void vec_divide(lfg_field z, lfg_field x, lfg_field y) {
@@ -569,7 +571,7 @@ void vec_divide(lfg_field z, lfg_field x, lfg_field y) {
   DISPATCH_KIND(z->kind, T,
                 k_divide<T><<<c->stream_grid(z->n()), kThreads, 0, c->stream>>>(
                     (T*)z->d, (const T*)x->d, (const T*)y->d, z->n()));
-  after_launch(c, "divide");
+  after_launch(c, "divide", (uint64_t)3 * z->n() * z->kind);
 }
 
 void vec_dot(lfg_field x, lfg_field y, int slot) {
@@ -577,7 +579,7 @@ void vec_dot(lfg_field x, lfg_field y, int slot) {
   lfg_ctx c = x->ctx;
   DISPATCH_KIND(x->kind, T,
                 launch_ewr<T>(c, DotOp<T>{(const T*)x->d, (const T*)y->d}, x->n(),
-                              all_aligned(x->d, y->d), slot, "dot"));
+                              all_aligned(x->d, y->d), slot, "dot", 2));
 }
 
 void vec_mgs_step(lfg_field v, lfg_field pv, lfg_field vj, lfg_field pvj, Sc alpha,
@@ -592,7 +594,7 @@ void vec_mgs_step(lfg_field v, lfg_field pv, lfg_field vj, lfg_field pvj, Sc alp
                 launch_ewr<T>(c, MgsOp<T>{(T*)v->d, (T*)pv->d, (const T*)vj->d,
                                           (const T*)pvj->d, (const T*)nx, alpha},
                               v->n(), all_aligned(v->d, pv->d, vj->d, pvj->d, nx), slot,
-                              "mgs"));
+                              "mgs", nx ? 7 : 6));
 }
 
 void vec_scale2_dot(lfg_field v, lfg_field pv, Sc beta, lfg_field res, int slot) {
@@ -601,7 +603,7 @@ void vec_scale2_dot(lfg_field v, lfg_field pv, Sc beta, lfg_field res, int slot)
   lfg_ctx c = v->ctx;
   DISPATCH_KIND(v->kind, T,
                 launch_ewr<T>(c, Scale2DotOp<T>{(T*)v->d, (T*)pv->d, (const T*)res->d, beta},
-                              v->n(), all_aligned(v->d, pv->d, res->d), slot, "scale2_dot"));
+                              v->n(), all_aligned(v->d, pv->d, res->d), slot, "scale2_dot", 5));
 }
 
 void vec_update2_norm(lfg_field dx, lfg_field pv, lfg_field res, lfg_field v, Sc alpha,
@@ -614,7 +616,7 @@ void vec_update2_norm(lfg_field dx, lfg_field pv, lfg_field res, lfg_field v, Sc
                 launch_ewr<T>(c, Update2NormOp<T>{(T*)dx->d, (const T*)pv->d, (T*)res->d,
                                                   (const T*)v->d, alpha},
                               dx->n(), all_aligned(dx->d, pv->d, res->d, v->d), slot,
-                              "update2_norm"));
+                              "update2_norm", 6));
 }
 
 void vec_axpy_norm(lfg_field x, Sc b, lfg_field y, int slot) {
@@ -622,7 +624,7 @@ void vec_axpy_norm(lfg_field x, Sc b, lfg_field y, int slot) {
   lfg_ctx c = x->ctx;
   DISPATCH_KIND(x->kind, T,
                 launch_ewr<T>(c, AxpyDotOp<T>{(T*)x->d, (const T*)y->d, nullptr, b}, x->n(),
-                              all_aligned(x->d, y->d), slot, "axpy_norm"));
+                              all_aligned(x->d, y->d), slot, "axpy_norm", 3));
 }
 
 void vec_axpy_dot(lfg_field x, Sc b, lfg_field y, lfg_field next, int slot) {
@@ -632,7 +634,7 @@ void vec_axpy_dot(lfg_field x, Sc b, lfg_field y, lfg_field next, int slot) {
   const void* nx = next ? next->d : nullptr;
   DISPATCH_KIND(x->kind, T,
                 launch_ewr<T>(c, AxpyDotOp<T>{(T*)x->d, (const T*)y->d, (const T*)nx, b},
-                              x->n(), all_aligned(x->d, y->d, nx), slot, "axpy_dot"));
+                              x->n(), all_aligned(x->d, y->d, nx), slot, "axpy_dot", nx ? 4 : 3));
 }
 
 void vec_scale_copy(lfg_field dst, Sc a, lfg_field src) {
@@ -640,7 +642,7 @@ void vec_scale_copy(lfg_field dst, Sc a, lfg_field src) {
   lfg_ctx c = dst->ctx;
   DISPATCH_KIND(dst->kind, T,
                 launch_ew<T>(c, ScaleCopyOp<T>{(T*)dst->d, (const T*)src->d, a}, dst->n(),
-                             all_aligned(dst->d, src->d), "scale_copy"));
+                             all_aligned(dst->d, src->d), "scale_copy", 2));
 }
 
 }  // namespace lfg
@@ -760,6 +762,12 @@ int lfg_ctx_kernel_launches(lfg_ctx c, uint64_t* count) {
   return LFG_OK;
 }
 
+int lfg_ctx_algorithmic_bytes(lfg_ctx c, uint64_t* bytes) {
+  if (!c || !bytes) return LFG_ERR_ARG;
+  *bytes = c->bytes;
+  return LFG_OK;
+}
+
 const char* lfg_last_error(lfg_ctx c) {
   if (!c) return "null context";
   return c->last_error.c_str();
@@ -836,7 +844,7 @@ int lfg_field_import(lfg_field f, const void* host, int host_kind) {
       k_to_level_major<float, double><<<grid, block, 0, c->stream>>>((float*)f->d, (const double*)st, f->ncol, f->nlev);
     else
       k_to_level_major<float, float><<<grid, block, 0, c->stream>>>((float*)f->d, (const float*)st, f->ncol, f->nlev);
-    after_launch(c, "to_level_major");
+    after_launch(c, "to_level_major", (uint64_t)bytes + f->bytes());
     LFG_CUDA(cudaStreamSynchronize(c->stream));
   });
 }
@@ -859,7 +867,7 @@ int lfg_field_export(lfg_field f, void* host, int host_kind) {
       k_to_column<double, float><<<grid, block, 0, c->stream>>>((double*)st, (const float*)f->d, f->ncol, f->nlev);
     else
       k_to_column<float, float><<<grid, block, 0, c->stream>>>((float*)st, (const float*)f->d, f->ncol, f->nlev);
-    after_launch(c, "to_column");
+    after_launch(c, "to_column", (uint64_t)bytes + f->bytes());
     LFG_CUDA(cudaMemcpyAsync(host, st, bytes, cudaMemcpyDeviceToHost, c->stream));
     LFG_CUDA(cudaStreamSynchronize(c->stream));
   });

@@ -561,7 +561,11 @@ void launch_sweep_seg(lfg_ctx c, int S, HelmArgs<T> A, const T* b, const T* xin,
     case 16: k_helm_sweep_seg<T, XIN, PRO, 16><<<grid, 128, 0, c->stream>>>(A, b, xin, parent, xc, ncoarse, omega, xout); break;
     default: k_helm_sweep_seg<T, XIN, PRO, 32><<<grid, 128, 0, c->stream>>>(A, b, xin, parent, xc, ncoarse, omega, xout); break;
   }
-  after_launch(c, "helm_sweep_seg");
+  // b, inv, sub, c' read and x written; x_in and the four couplings with
+  // XIN; the coarse field with PRO
+  const uint64_t n = (uint64_t)A.ncol * A.nl;
+  after_launch(c, "helm_sweep_seg",
+               sizeof(T) * ((XIN ? 10 : 5) * n + (PRO ? (uint64_t)ncoarse * A.nl : 0)));
 }
 
 template <class T, bool XIN, bool PRO>
@@ -592,7 +596,10 @@ void launch_subst(lfg_ctx c, int ncol, int nl, const T* r, const T* sub, const T
   kern<<<(ncol + bs - 1) / bs, bs, (size_t)nl * bs * sizeof(T), c->stream>>>(
       ncol, nl, r, sub, inv, cp, xin, parent, xc, ncoarse, omega, xout);
   (void)smem;
-  after_launch(c, "helm_subst");
+  // r, inv, sub, c' read and x written; x_in with XIN; the coarse field with PRO
+  after_launch(c, "helm_subst",
+               sizeof(T) * ((XIN ? 6 : 5) * (uint64_t)ncol * nl +
+                            (PRO ? (uint64_t)ncoarse * nl : 0)));
 }
 
 template <class T>
@@ -623,17 +630,20 @@ void smooth_t(lfg_helm op, double omega, lfg_field x_in, lfg_field b, lfg_field 
   }
   T* r = (T*)rbuf;
   const size_t work = (size_t)op->ncol * ((op->nl + KC - 1) / KC);
+  // x, b and the four couplings read, r written; the coarse field with PRO
+  const uint64_t rhs_bytes = sizeof(T) * (7 * (uint64_t)op->ncol * op->nl +
+                                          (ig ? (uint64_t)ig->ncoarse * op->nl : 0));
   if (!ig) {
     k_helm_rhs<T, false><<<occ_grid(c, (const void*)k_helm_rhs<T, false>, 256, work), 256, 0, c->stream>>>(args_of<T>(op), (const T*)x_in->d,
                                                        (const T*)b->d, r, nullptr, nullptr, 0);
-    after_launch(c, "helm_rhs");
+    after_launch(c, "helm_rhs", rhs_bytes);
     launch_subst<T, true, false>(c, op->ncol, op->nl, r, sub, inv, cp, (const T*)x_in->d,
                                  nullptr, nullptr, 0, om, (T*)x_out->d);
   } else {
     k_helm_rhs<T, true><<<occ_grid(c, (const void*)k_helm_rhs<T, true>, 256, work), 256, 0, c->stream>>>(args_of<T>(op), (const T*)x_in->d,
                                                       (const T*)b->d, r, ig->parent,
                                                       (const T*)xc->d, ig->ncoarse);
-    after_launch(c, "helm_rhs");
+    after_launch(c, "helm_rhs", rhs_bytes);
     launch_subst<T, true, true>(c, op->ncol, op->nl, r, sub, inv, cp, (const T*)x_in->d,
                                 ig->parent, (const T*)xc->d, ig->ncoarse, om, (T*)x_out->d);
   }
@@ -673,7 +683,9 @@ void helm_apply(lfg_helm op, lfg_field y, lfg_field x, lfg_field dot_with, int s
     else
       k_helm_apply<T, false, false><<<occ_grid(c, (const void*)k_helm_apply<T, false, false>, bs, work), bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, nullptr, (T*)y->d, nullptr, r);
   }
-  after_launch(c, "helm_apply");
+  // x and the 7 coefficient arrays read, y written; w read for <y, w>
+  after_launch(c, "helm_apply",
+               (uint64_t)op->kind * op->ncol * op->nl * (slot >= 0 && dot_with ? 10 : 9));
 }
 
 void helm_residual(lfg_helm op, lfg_field r_out, lfg_field x, lfg_field b, int slot) {
@@ -697,7 +709,8 @@ void helm_residual(lfg_helm op, lfg_field r_out, lfg_field x, lfg_field b, int s
     else
       k_helm_apply<T, true, false><<<occ_grid(c, (const void*)k_helm_apply<T, true, false>, bs, work), bs, 0, c->stream>>>(args_of<T>(op), (const T*)x->d, (const T*)b->d, (T*)r_out->d, nullptr, r);
   }
-  after_launch(c, "helm_residual");
+  // x, b and the 7 coefficient arrays read, r written
+  after_launch(c, "helm_residual", (uint64_t)op->kind * op->ncol * op->nl * 10);
 }
 
 void helm_smooth(lfg_helm op, double omega, lfg_field x_in, lfg_field b, lfg_field x_out,
@@ -732,7 +745,9 @@ void helm_residual_restrict(lfg_helm op, lfg_intergrid ig, lfg_field x, lfg_fiel
     k_helm_resid_restrict<double><<<occ_grid(c, (const void*)k_helm_resid_restrict<double>, bs, work), bs, 0, c->stream>>>(args_of<double>(op), (const double*)x->d, (const double*)b->d, (double*)bc->d, ig->child, ig->ncoarse, ig->nx * ig->ny);
   else
     k_helm_resid_restrict<float><<<occ_grid(c, (const void*)k_helm_resid_restrict<float>, bs, work), bs, 0, c->stream>>>(args_of<float>(op), (const float*)x->d, (const float*)b->d, (float*)bc->d, ig->child, ig->ncoarse, ig->nx * ig->ny);
-  after_launch(c, "resid_restrict");
+  // x, b and the 7 coefficient arrays read, the coarse right-hand side written
+  after_launch(c, "resid_restrict",
+               (uint64_t)op->kind * op->nl * (9 * (uint64_t)op->ncol + ig->ncoarse));
 }
 
 void prolong_add(lfg_intergrid ig, lfg_field fine, lfg_field coarse) {
@@ -745,7 +760,8 @@ void prolong_add(lfg_intergrid ig, lfg_field fine, lfg_field coarse) {
     k_prolong_add<double><<<grid, bs, 0, c->stream>>>((double*)fine->d, (const double*)coarse->d, ig->parent, ig->nfine, ig->ncoarse, fine->nlev);
   else
     k_prolong_add<float><<<grid, bs, 0, c->stream>>>((float*)fine->d, (const float*)coarse->d, ig->parent, ig->nfine, ig->ncoarse, fine->nlev);
-  after_launch(c, "prolong_add");
+  after_launch(c, "prolong_add",
+               (uint64_t)fine->kind * fine->nlev * (2 * (uint64_t)ig->nfine + ig->ncoarse));
 }
 
 }  // namespace lfg
@@ -783,7 +799,7 @@ static void factor_helm(lfg_helm op) {
     k_helm_factor<double><<<grid, bs, 0, c->stream>>>((const double*)op->sub, (const double*)op->diag, (const double*)op->sup, (double*)op->inv, (double*)op->cp, op->ncol, op->nl);
   else
     k_helm_factor<float><<<grid, bs, 0, c->stream>>>((const float*)op->sub, (const float*)op->diag, (const float*)op->sup, (float*)op->inv, (float*)op->cp, op->ncol, op->nl);
-  after_launch(c, "helm_factor");
+  after_launch(c, "helm_factor", (uint64_t)op->kind * op->ncol * op->nl * 5);
   LFG_CUDA(cudaStreamSynchronize(c->stream));
 }
 
@@ -936,7 +952,7 @@ int lfg_helm_copy_kind(lfg_helm src, int kind, lfg_helm* out) {
         k_convert<float, double><<<g, kThreads, 0, c->stream>>>((float*)d_arr[a], (const double*)s_arr[a], m);
       else
         k_convert<double, float><<<g, kThreads, 0, c->stream>>>((double*)d_arr[a], (const float*)s_arr[a], m);
-      if (src->kind != kind) after_launch(c, "convert");
+      if (src->kind != kind) after_launch(c, "convert", (uint64_t)m * (src->kind + kind));
     }
     try {
       factor_helm(d);

@@ -134,6 +134,9 @@ struct lfg_ctx_s {
   cudaStream_t stream = nullptr;
   std::string last_error;
   uint64_t launches = 0;
+  // algorithmic bytes of the launched kernels: each array a kernel reads
+  // counted once, each array it writes counted once, at stored precision
+  uint64_t bytes = 0;
   // reduction slots
   double* red_partials = nullptr;  // [kRedSlots][kMaxRedBlocks]
   unsigned* red_counters = nullptr;
@@ -256,8 +259,9 @@ struct lfg_helm_s {
 namespace lfg {
 
 // Launch bookkeeping and error checks shared by all translation units.
-inline void after_launch(lfg_ctx ctx, const char* what) {
+inline void after_launch(lfg_ctx ctx, const char* what, uint64_t bytes = 0) {
   ctx->launches++;
+  ctx->bytes += bytes;
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess)
     throw Error(LFG_ERR_CUDA, std::string("launch of ") + what + ": " + cudaGetErrorString(e));

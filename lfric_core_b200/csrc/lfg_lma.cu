@@ -363,7 +363,11 @@ void launch_local(lfg_ctx c, lfg_lma m, const T* x, T* loc) {
   }
   else if (m->ndf_to == 1 && m->ndf_from == 1) go(k_lma_local<T, TR, 1, 1>, 1);
   else go(k_lma_local<T, TR, 0, 0>, 1);
-  after_launch(c, "lma_local");
+  // the element matrices and the input field; the local products are an
+  // intermediate (kept in L2) and not counted
+  const uint64_t nin = TR ? (uint64_t)m->nent_to * m->nlev_to
+                          : (uint64_t)m->nent_from * m->nlev_from;
+  after_launch(c, "lma_local", sizeof(T) * ((uint64_t)ncl * m->ndf_to * m->ndf_from + nin));
 }
 
 template <class T, bool INC>
@@ -381,7 +385,8 @@ void launch_gather_tab(lfg_ctx c, const int2* tab, int w, int nent, int nlev, in
     case 8: go(k_lma_gather_tab<T, INC, 8, KC>); break;
     default: go(k_lma_gather_tab<T, INC, 16, KC>); break;
   }
-  after_launch(c, "lma_gather");
+  // the output field written (and read with INC)
+  after_launch(c, "lma_gather", sizeof(T) * (uint64_t)nent * nlev * (INC ? 2 : 1));
 }
 
 void upload_matrix(lfg_lma m, const double* ls) {
@@ -533,7 +538,14 @@ int lfg_lma_apply(lfg_lma m, int mode, lfg_field lhs, lfg_field x) {
           k_lma_apply<T, false><<<grid, 128, 0, c->stream>>>(args_of<T>(m), m->inc_to_ptr, m->inc_to, (const T*)x->d, (T*)lhs->d);
       }
     });
-    after_launch(c, "lma_apply");
+    // element matrices, x read; lhs read (INC, TRANSPOSE) and written
+    const uint64_t nx = mode == LFG_LMA_TRANSPOSE ? (uint64_t)m->nent_to * m->nlev_to
+                                                  : (uint64_t)m->nent_from * m->nlev_from;
+    const uint64_t ny = mode == LFG_LMA_TRANSPOSE ? (uint64_t)m->nent_from * m->nlev_from
+                                                  : (uint64_t)m->nent_to * m->nlev_to;
+    after_launch(c, "lma_apply",
+                 (uint64_t)m->kind * ((uint64_t)m->ncell * m->nl * m->ndf_to * m->ndf_from + nx +
+                                      ny * (mode == LFG_LMA_WRITE ? 1 : 2)));
   });
 }
 

@@ -191,7 +191,7 @@ struct MgPrec : lfg_prec_s {
   // a graph removes the per-kernel launch gaps.
   struct Graph {
     cudaGraphExec_t exec = nullptr;
-    uint64_t nodes = 0;
+    uint64_t nodes = 0, bytes = 0;
   };
   std::map<std::pair<void*, void*>, Graph> graphs;
   std::set<std::pair<void*, void*>> seen;
@@ -234,7 +234,7 @@ struct MgPrec : lfg_prec_s {
     }
     if (it == graphs.end()) {
       Graph g;
-      const uint64_t n0 = ctx->launches;
+      const uint64_t n0 = ctx->launches, b0 = ctx->bytes;
       LFG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
       try {
         vcycle(0, x, y);
@@ -251,11 +251,14 @@ struct MgPrec : lfg_prec_s {
       if (e != cudaSuccess)
         throw Error(LFG_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
       g.nodes = ctx->launches - n0;
+      g.bytes = ctx->bytes - b0;
       ctx->launches = n0;
+      ctx->bytes = b0;
       it = graphs.emplace(key, g).first;
     }
     LFG_CUDA(cudaGraphLaunch(it->second.exec, st));
     ctx->launches += it->second.nodes;
+    ctx->bytes += it->second.bytes;
   }
 };
 

@@ -395,7 +395,8 @@ void launch_reg(lfg_ctx c, const TmaMaps& maps, int ncol, int nl, bool xin, T om
   };
   if (xin) by_nch(std::true_type{});
   else by_nch(std::false_type{});
-  after_launch(c, "helm_subst_tma");
+  // r, inv, sub, c' read and x written, x_in read when given
+  after_launch(c, "helm_subst_tma", sizeof(T) * (uint64_t)ncol * nl * (xin ? 6 : 5));
 }
 
 template <class T>
@@ -437,7 +438,7 @@ void subst_tma(lfg_ctx c, int ncol, int nl, const float* r, const float* sub, co
     k_subst_tma<true><<<grid, TC, smem, c->stream>>>(maps, ncol, nl, omega, xout, c->dev_err);
   else
     k_subst_tma<false><<<grid, TC, smem, c->stream>>>(maps, ncol, nl, omega, xout, c->dev_err);
-  after_launch(c, "helm_subst_tma");
+  after_launch(c, "helm_subst_tma", sizeof(float) * (uint64_t)ncol * nl * (xin ? 6 : 5));
 }
 
 void subst_tma(lfg_ctx c, int ncol, int nl, const double* r, const double* sub,

@@ -271,7 +271,9 @@ int lfg_w2_restrict(lfg_w2map m, int mode, lfg_field coarse, lfg_field fine) {
     else
       k_w2_restrict<float><<<grid, bs, 0, c->stream>>>(args_of(m), mode, (float*)coarse->d,
                                                        (const float*)fine->d);
-    after_launch(c, "w2_restrict");
+    // fine field read, coarse field written (whole fields, an upper bound
+    // for the partial restrictions)
+    after_launch(c, "w2_restrict", (uint64_t)coarse->kind * (fine->n() + coarse->n()));
   });
 }
 
@@ -285,7 +287,7 @@ int lfg_w2_prolong_weights(lfg_w2map m, lfg_field weights) {
     const size_t n = (size_t)m->ig->ncoarse * (m->nl + 1);
     k_w2_weights<<<(unsigned)((n + 127) / 128), 128, 0, c->stream>>>(args_of(m),
                                                                       (double*)weights->d);
-    after_launch(c, "w2_weights");
+    after_launch(c, "w2_weights", (uint64_t)8 * 2 * weights->n());
   });
 }
 
@@ -301,7 +303,8 @@ int lfg_w2_prolong(lfg_w2map m, lfg_field fine, lfg_field coarse, lfg_field weig
     const size_t n = (size_t)m->ig->ncoarse * (m->nl + 1);
     k_w2_prolong<<<(unsigned)((n + 127) / 128), 128, 0, c->stream>>>(
         args_of(m), (double*)fine->d, (const double*)coarse->d, (const double*)weights->d);
-    after_launch(c, "w2_prolong");
+    // fine read and written, weights read, coarse read
+    after_launch(c, "w2_prolong", (uint64_t)8 * (3 * fine->n() + coarse->n()));
   });
 }
 
