@@ -9,13 +9,16 @@
 //   sci_mm_diagonal_kernel_mod.F90:99-127           (lfg_lma_diagonal)
 //
 // The reference scatters each cell's y_e = A_e x_e into the shared dofs
-// (GH_INC) inside a coloured OpenMP loop.  Here every output dof GATHERS its
-// contributions: one thread per (level, output entity) walks the list of
-// (cell, local dof) incidences of its entity, in the reference's order
-// (cells ascending; for each cell the df2 loop outside the df loop), so the
-// result is deterministic without atomics.  Element matrices are stored
+// (GH_INC) inside a coloured OpenMP loop.  Here the applies run in two
+// phases: k_lma_local streams the element matrices once, coalesced, and
+// writes each cell-layer's local products; k_lma_gather_tab then has every
+// output dof GATHER the products of its (cell, local dof) incidences, in
+// cell order, through a padded incidence table, so the result is
+// deterministic without atomics.  Operators whose incidence lists are wider
+// than 16 keep the one-pass gathers (k_lma_apply, k_lma_apply_t), which
+// walk the incidence lists directly.  Element matrices are stored
 // [df_to][df_from][layer][cell]: at fixed (df, df2, layer) consecutive cells
-// are contiguous.  Algorithmic traffic: 8*ndf_to*ndf_from bytes per cell and
+// are contiguous.  Algorithmic traffic: w*ndf_to*ndf_from bytes per cell and
 // layer for the matrix plus one read of x and one write of y.
 #include "lfg_internal.cuh"
 
