@@ -11,10 +11,13 @@
 // sci_columnwise_op_appinv_kernel_mod.F90:77-145 (multiply by the inverse
 // denominator, c' not formed on the last row).
 //
-// Every kernel here is HBM-bandwidth bound (< 1 flop/byte).  One thread owns
-// one column and walks its levels, so at every level a warp reads 32
-// consecutive columns of each level-major array; the neighbour ids of a
-// column are read once, not once per level.
+// Every kernel here is HBM-bandwidth bound (< 1 flop/byte).  The
+// element-parallel kernels (apply, right-hand side, residual) give a thread
+// one column and KC levels; the substitutions give a thread one column and
+// walk its levels (on fine meshes through the TMA kernels of
+// lfg_subst_tma.cu; on small meshes S threads share a column in the
+// segmented sweep), so at every level a warp reads consecutive columns of
+// each level-major array.
 #include "lfg_internal.cuh"
 
 #include <algorithm>

@@ -1,5 +1,5 @@
 // The column substitutions of the block-Jacobi sweep with TMA staging
-// (FP32, fine meshes):
+// (fine meshes; FP32, and FP64 in the register form):
 //   d'_k = inv_k (r_k - sub_k d'_{k-1}),  z_k = d'_k - c'_k z_{k+1},
 //   x_out = omega z + (1 - omega) x_in            (x_in optional)
 //
@@ -9,15 +9,19 @@
 // issues each job as 2-D TMA tile loads (cp.async.bulk.tensor) into a ring
 // of NST shared-memory stages, completed on an mbarrier with an expected
 // byte count; all threads (one per column) wait on the stage's barrier,
-// compute, and leave the stage to the next job after a block barrier.  d'
-// stays in shared memory between the passes.  The bytes in flight are held
-// by the TMA engine, not by registers, so the loads of the next NST-1 chunks
-// overlap the recurrence of the current one.
+// compute, and leave the stage to the next job after a block barrier.  The
+// bytes in flight are held by the TMA engine, not by registers, so the
+// loads of the next NST-1 chunks overlap the recurrence of the current one.
+// Between the passes d' stays in registers (k_subst_tma_reg, columns of up
+// to 80 levels: the chunk count is a template parameter and the loops are
+// fully unrolled; FP32 tiles of 128 columns, FP64 tiles of 64) or, for
+// taller FP32 columns, in shared memory (k_subst_tma).
 //
-// Rules kept: every tile's first column is a multiple of TC, so the TMA's
-// innermost coordinate times 4 bytes is a multiple of 16; rows of the
-// level-major arrays are N floats apart, so N must be a multiple of 4 (the
-// host falls back to the per-column kernel otherwise); loads only (no TMA
+// Rules kept: every tile's first column is a multiple of the tile width,
+// so the TMA's innermost coordinate times the element size is a multiple of
+// 16 bytes; rows of the level-major arrays are N elements apart, so N must
+// be a multiple of 4 (FP32) or 2 (FP64) (the host falls back to the
+// per-column kernel otherwise); loads only (no TMA
 // store), so out-of-range columns and levels of the last tile read zeros.
 // Every wait is bounded: a barrier that does not complete within the spin
 // limit sets the context's device error word, the block waits (bounded) for
