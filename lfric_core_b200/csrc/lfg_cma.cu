@@ -11,7 +11,10 @@
 //   inter_mesh/sci_prolong_scalar_{unweighted,weighted}_kernel_mod.F90,
 //   inter_mesh/sci_restrict_w0_kernel_mod.F90, sci_prolong_w0_kernel_mod.F90.
 // The reference calls each once per column from the PSy layer; here one
-// launch covers the mesh and one thread owns a column (or a coarse column).
+// launch covers the mesh.  The banded apply and the intergrid transfers
+// give a thread one (column, row) or (column, block of levels); the line
+// solves give a thread one column, or, for FP64 columns of 13-96 rows, one
+// segment of a column (k_cma_subst_seg).
 #include "lfg_internal.cuh"
 
 #include <algorithm>
