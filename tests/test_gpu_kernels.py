@@ -214,33 +214,65 @@ def test_lma_transpose_golden(ctx):
     assert np.allclose(Y.export(), g["answer"], rtol=0, atol=g["tol_r_double"])
 
 
+@pytest.mark.parametrize("kind,tol", [(R_DOUBLE, TOL64), (R_SINGLE, 5e-6)])
 @pytest.mark.parametrize("n,nl", [(4, 3), (8, 10)])
-def test_lma_w0_against_oracle(ctx, n, nl):
+def test_lma_w0_against_oracle(ctx, n, nl, kind, tol):
+    """The W0 8x8 applies (FP32 fields against the FP64 oracle at 5e-6)."""
     p = w0_problem(n, nl, seed=n, top=nl * 1e3, kappa_sigma=0.5)
     A = p.matrix()
     nent, nlev = p.nvert, nl + 1
-    lma = api.LocalOperator(ctx, R_DOUBLE, p.ncell, nl, A, p.map, nent, nlev)
+    lma = api.LocalOperator(ctx, kind, p.ncell, nl, A, p.map, nent, nlev)
     rng = np.random.default_rng(4)
     x = rng.standard_normal(p.ndof)
     y0 = rng.standard_normal(p.ndof)
+    if kind == R_SINGLE:   # the oracle sees the values the device holds
+        x, y0 = x.astype(np.float32).astype(np.float64), y0.astype(np.float32).astype(np.float64)
+        A = A.astype(np.float32).astype(np.float64)
     m1 = (p.map + 1).astype(np.int32)
-    X = field_from(ctx, x, nent, nlev)
-    Y = field_from(ctx, y0, nent, nlev)
+    X = field_from(ctx, x, nent, nlev, kind=kind)
+    Y = field_from(ctx, y0, nent, nlev, kind=kind)
     lma.apply(api.LMA_INC, Y, X)
     ref = oh.lma_apply("matrix_vector", A, m1, m1, p.ncell, nl, x, y0=y0)
-    assert rel(Y.export(), ref) < TOL64
+    assert rel(Y.export(np.float64), ref) < tol
     lma.apply(api.LMA_WRITE, Y, X)
     ref0 = oh.lma_apply("matrix_vector", A, m1, m1, p.ncell, nl, x, y0=np.zeros(p.ndof))
-    assert rel(Y.export(), ref0) < TOL64
+    assert rel(Y.export(np.float64), ref0) < tol
     Y.import_(y0)
     lma.apply(api.LMA_TRANSPOSE, Y, X)
     # transpose_matrix_vector reads matrix(ik, df2, df1) = A(ik, df_to, df_from)
     ref = oh.lma_apply("transpose_matrix_vector", A, m1, m1, p.ncell, nl, x, y0=y0)
-    assert rel(Y.export(), ref) < TOL64
-    D = field_from(ctx, y0, nent, nlev)
+    assert rel(Y.export(np.float64), ref) < tol
+    D = field_from(ctx, y0, nent, nlev, kind=kind)
     lma.diagonal(D)
     ref = y0 + oh.mm_diagonal(A, m1, p.ncell, nl, p.ndof)
-    assert rel(D.export(), ref) < TOL64
+    assert rel(D.export(np.float64), ref) < tol
+
+
+def test_lma_wide_incidence_lists(ctx):
+    """An entity shared by 24 cells, more than the padded incidence table's
+    16 slots: the applies take the one-pass gathers over the incidence
+    lists (forward, write and transposed) and match the oracle."""
+    ncell, nl, nlev = 24, 5, 6
+    m = np.zeros((ncell, 3), dtype=np.int32)
+    for c in range(ncell):      # df 0 on the hub entity 0, dfs 1-2 on entity c+1
+        m[c] = [0, (c + 1) * nlev, (c + 1) * nlev + 1]
+    nent = ncell + 1
+    ndof = nent * nlev
+    rng = np.random.default_rng(51)
+    A = rng.standard_normal((ncell * nl, 3, 3)).ravel(order="F")
+    lma = api.LocalOperator(ctx, R_DOUBLE, ncell, nl, A, m, nent, nlev)
+    x, y0 = rng.standard_normal(ndof), rng.standard_normal(ndof)
+    m1 = m + 1
+    X, Y = field_from(ctx, x, nent, nlev), field_from(ctx, y0, nent, nlev)
+    lma.apply(api.LMA_INC, Y, X)
+    assert rel(Y.export(), oh.lma_apply("matrix_vector", A, m1, m1, ncell, nl, x, y0=y0)) < TOL64
+    lma.apply(api.LMA_WRITE, Y, X)
+    ref0 = oh.lma_apply("matrix_vector", A, m1, m1, ncell, nl, x, y0=np.zeros(ndof))
+    assert rel(Y.export(), ref0) < TOL64
+    Y.import_(y0)
+    lma.apply(api.LMA_TRANSPOSE, Y, X)
+    ref = oh.lma_apply("transpose_matrix_vector", A, m1, m1, ncell, nl, x, y0=y0)
+    assert rel(Y.export(), ref) < TOL64
 
 
 # ----------------------------------------------------------------- intergrid
