@@ -20,12 +20,14 @@ def rel(a, b):
 
 
 @pytest.mark.parametrize("n,nl,kind", [(8, 1, R_DOUBLE), (8, 2, R_SINGLE), (8, 150, R_DOUBLE),
-                                       (96, 150, R_SINGLE), (96, 1, R_SINGLE)])
+                                       (96, 150, R_SINGLE), (96, 1, R_SINGLE),
+                                       (96, 100, R_SINGLE), (96, 100, R_DOUBLE)])
 def test_helmholtz_column_heights(ctx, n, nl, kind):
-    """apply and both sweep forms for columns of 1, 2 and 150 levels, on a
-    mesh with few columns (segmented sweep, or its per-column fallback
-    above 384 levels) and on C96 (per-column substitution; the TMA form
-    takes at most 128 levels)."""
+    """apply and both sweep forms for columns of 1 to 150 levels, on a mesh
+    with few columns (segmented sweep, or its per-column fallback above 384
+    levels) and on C96: the TMA substitution with d' in registers up to 80
+    levels (FP32 and FP64), with d' in shared memory for 81-128 FP32
+    levels, one thread per column above that and for taller FP64 columns."""
     p = helmholtz_problem(n, nl, seed=21, mg_levels=1)
     dt = np.float64 if kind == R_DOUBLE else np.float32
     ora = OraHelm(p)
