@@ -364,6 +364,13 @@ bool subst_tma_applicable(lfg_ctx c, int ncol, int nl, const void* const* ptrs, 
 
 namespace {
 
+// f(n, kernel) for the register kernels of n = N, N-1, ..., 1 chunks
+template <class T, bool X, int N, class F>
+void for_reg_kernels(F&& f) {
+  f(N, (const void*)k_subst_tma_reg<T, X, N>);
+  if constexpr (N > 1) for_reg_kernels<T, X, N - 1>(f);
+}
+
 template <class T>
 void launch_reg(lfg_ctx c, const TmaMaps& maps, int ncol, int nl, bool xin, T omega, T* xout) {
   constexpr int TCT = tile_cols<T>();
@@ -371,34 +378,30 @@ void launch_reg(lfg_ctx c, const TmaMaps& maps, int ncol, int nl, bool xin, T om
   const size_t smem = sizeof(T) * (size_t)NST * NARR * KCH * TCT;
   static std::once_flag attr_reg;
   std::call_once(attr_reg, [&] {
-    const void* all[] = {
-        (const void*)k_subst_tma_reg<T, false, 1>, (const void*)k_subst_tma_reg<T, false, 2>,
-        (const void*)k_subst_tma_reg<T, false, 3>, (const void*)k_subst_tma_reg<T, false, 4>,
-        (const void*)k_subst_tma_reg<T, false, 5>, (const void*)k_subst_tma_reg<T, true, 1>,
-        (const void*)k_subst_tma_reg<T, true, 2>,  (const void*)k_subst_tma_reg<T, true, 3>,
-        (const void*)k_subst_tma_reg<T, true, 4>,  (const void*)k_subst_tma_reg<T, true, 5>};
-    for (const void* k : all)
+    auto set = [&](int, const void* k) {
       LFG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    };
+    for_reg_kernels<T, false, kRegChunks>(set);
+    for_reg_kernels<T, true, kRegChunks>(set);
   });
-  auto go = [&](auto kern) {
-    int per_sm = 0;
-    LFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TCT, smem));
-    const int ntile = (ncol + TCT - 1) / TCT;
-    const int grid = std::max(1, std::min(ntile, c->num_sms * std::max(per_sm, 1)));
-    kern<<<grid, TCT, smem, c->stream>>>(maps, ncol, nl, omega, xout, c->dev_err);
+  const void* kern = nullptr;
+  auto pick = [&](int n, const void* k) {
+    if (n == nch) kern = k;
   };
-  auto by_nch = [&](auto xtag) {
-    constexpr bool X = decltype(xtag)::value;
-    switch (nch) {
-      case 1: go(k_subst_tma_reg<T, X, 1>); break;
-      case 2: go(k_subst_tma_reg<T, X, 2>); break;
-      case 3: go(k_subst_tma_reg<T, X, 3>); break;
-      case 4: go(k_subst_tma_reg<T, X, 4>); break;
-      default: go(k_subst_tma_reg<T, X, 5>); break;
-    }
-  };
-  if (xin) by_nch(std::true_type{});
-  else by_nch(std::false_type{});
+  if (xin) for_reg_kernels<T, true, kRegChunks>(pick);
+  else for_reg_kernels<T, false, kRegChunks>(pick);
+  if (!kern) throw Error(LFG_ERR_ARG, "subst_tma: column taller than the register form");
+  int per_sm = 0;
+  LFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TCT, smem));
+  const int ntile = (ncol + TCT - 1) / TCT;
+  const int grid = std::max(1, std::min(ntile, c->num_sms * std::max(per_sm, 1)));
+  TmaMaps m = maps;
+  int nc = ncol, nlv = nl;
+  T om = omega;
+  T* xo = xout;
+  unsigned* err = c->dev_err;
+  void* args[] = {&m, &nc, &nlv, &om, &xo, &err};
+  LFG_CUDA(cudaLaunchKernel(kern, dim3(grid), dim3(TCT), args, smem, c->stream));
   // r, inv, sub, c' read and x written, x_in read when given
   after_launch(c, "helm_subst_tma", sizeof(T) * (uint64_t)ncol * nl * (xin ? 6 : 5));
 }
