@@ -363,14 +363,29 @@ __global__ void __launch_bounds__(256) k_helm_resid_restrict(HelmArgs<T> A,
 }
 
 // fine(c,k) += coarse(parent(c),k)   (prolong_scalar_unweighted on W3)
+// One thread per (column, block of KP levels), columns fastest, grid-stride:
+// the parent index is read once per block and the block's loads are all
+// issued before its stores.
+constexpr int KP = 4;
 template <class T>
 __global__ void k_prolong_add(T* __restrict__ fine, const T* __restrict__ coarse,
                               const int* __restrict__ parent, int nfine, int ncoarse, int nl) {
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
-  if (c >= nfine) return;
-  const int p = parent[c];
-  for (int k = 0; k < nl; ++k)
-    fine[(size_t)k * nfine + c] = fine[(size_t)k * nfine + c] + coarse[(size_t)k * ncoarse + p];
+  const size_t nblk = (size_t)nfine * ((nl + KP - 1) / KP);
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < nblk;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int c = (int)(t % nfine), k0 = (int)(t / nfine) * KP;
+    const int p = parent[c];
+    T fv[KP], cv[KP];
+#pragma unroll
+    for (int kk = 0; kk < KP; ++kk)
+      if (k0 + kk < nl) {
+        fv[kk] = fine[(size_t)(k0 + kk) * nfine + c];
+        cv[kk] = coarse[(size_t)(k0 + kk) * ncoarse + p];
+      }
+#pragma unroll
+    for (int kk = 0; kk < KP; ++kk)
+      if (k0 + kk < nl) fine[(size_t)(k0 + kk) * nfine + c] = fv[kk] + cv[kk];
+  }
 }
 
 // Galerkin coarse operator, one thread per coarse column (FP64).
@@ -753,16 +768,18 @@ void helm_residual_restrict(lfg_helm op, lfg_intergrid ig, lfg_field x, lfg_fiel
                (uint64_t)op->kind * op->nl * (9 * (uint64_t)op->ncol + ig->ncoarse));
 }
 
+bool helm_segmented(lfg_helm op) { return seg_threads(op->ctx, op->ncol, op->nl) > 0; }
+
 void prolong_add(lfg_intergrid ig, lfg_field fine, lfg_field coarse) {
   LFG_REQUIRE(fine->ncol == ig->nfine && coarse->ncol == ig->ncoarse &&
                   fine->nlev == coarse->nlev && fine->kind == coarse->kind,
               "prolong_add: bad fields");
   lfg_ctx c = fine->ctx;
-  const int bs = 128, grid = (ig->nfine + bs - 1) / bs;
+  const size_t work = (size_t)ig->nfine * ((fine->nlev + KP - 1) / KP);
   if (fine->kind == LFG_R_DOUBLE)
-    k_prolong_add<double><<<grid, bs, 0, c->stream>>>((double*)fine->d, (const double*)coarse->d, ig->parent, ig->nfine, ig->ncoarse, fine->nlev);
+    k_prolong_add<double><<<occ_grid(c, (const void*)k_prolong_add<double>, 256, work), 256, 0, c->stream>>>((double*)fine->d, (const double*)coarse->d, ig->parent, ig->nfine, ig->ncoarse, fine->nlev);
   else
-    k_prolong_add<float><<<grid, bs, 0, c->stream>>>((float*)fine->d, (const float*)coarse->d, ig->parent, ig->nfine, ig->ncoarse, fine->nlev);
+    k_prolong_add<float><<<occ_grid(c, (const void*)k_prolong_add<float>, 256, work), 256, 0, c->stream>>>((float*)fine->d, (const float*)coarse->d, ig->parent, ig->nfine, ig->ncoarse, fine->nlev);
   after_launch(c, "prolong_add",
                (uint64_t)fine->kind * fine->nlev * (2 * (uint64_t)ig->nfine + ig->ncoarse));
 }

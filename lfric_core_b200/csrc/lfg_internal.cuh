@@ -357,5 +357,8 @@ void helm_smooth(lfg_helm op, double omega, lfg_field x_in, lfg_field b, lfg_fie
 void helm_residual_restrict(lfg_helm op, lfg_intergrid ig, lfg_field x, lfg_field b,
                             lfg_field bc);
 void prolong_add(lfg_intergrid ig, lfg_field fine, lfg_field coarse);
+// True when the operator's sweeps take the segmented one-kernel form (small
+// meshes), false when they run as right-hand side + substitution.
+bool helm_segmented(lfg_helm op);
 
 }  // namespace lfg

@@ -122,9 +122,9 @@ FieldPtr make_field(lfg_ctx c, int kind, int ncol, int nlev) {
 // reference's multigrid glue lives outside lfric_core, it provides the
 // hierarchical operator/preconditioner types and the intergrid kernels):
 // n_pre block-Jacobi column sweeps from zero, residual fused with
-// restrict_mass_w3, the coarse-level cycle, prolong_scalar_unweighted fused
-// into the first of n_post sweeps; n_coarse sweeps from zero on the
-// coarsest level.
+// restrict_mass_w3, the coarse-level cycle, prolong_scalar_unweighted
+// (added in place on fine levels, fused into the first of the n_post sweeps
+// on small ones); n_coarse sweeps from zero on the coarsest level.
 struct MgPrec : lfg_prec_s {
   std::vector<lfg_helm> ops;
   std::vector<lfg_intergrid> maps;
@@ -179,10 +179,15 @@ struct MgPrec : lfg_prec_s {
     else vec_set(P, sc_const(0.0));
     helm_residual_restrict(ops[l], maps[l], P, b, bc[l + 1].get());
     vcycle(l + 1, bc[l + 1].get(), xa[l + 1].get());
-    if (n_post > 0)
+    if (n_post > 0 && helm_segmented(ops[l])) {
+      // small meshes: the correction fused into the first sweep's kernel
       sweeps(l, n_post, P, b, X, T, maps[l], xa[l + 1].get());
-    else
+    } else {
+      // fine meshes: P += prolong(coarse) in place, then the plain sweeps
+      // (the same x + P xc values the fused sweep forms on the fly)
       prolong_add(maps[l], P, xa[l + 1].get());
+      if (n_post > 0) sweeps(l, n_post, P, b, X, T, nullptr, nullptr);
+    }
   }
 
   // One captured CUDA graph per (input, output) buffer pair: the V-cycle is
