@@ -159,16 +159,13 @@ __global__ void k_helm_factor(const T* __restrict__ sub, const T* __restrict__ d
 // The block-Jacobi column sweep of A x = b,
 //   x_out = omega T'^{-1} (b + H_off x_in) + (1 - omega) x_in,
 // which equals x_in + omega T'^{-1} (b - A x_in), runs as two streaming
-// kernels.  PRO: x_in is the prolongation-corrected iterate x_in + P xc (P
-// adds the parent's coarse value), formed on the fly and never stored.
+// kernels.
 //
 // (1) k_helm_rhs: r = b + H_off x_in, one thread per (column, chunk of KC
 //     levels), loads issued before the stores.
-template <class T, bool PRO>
+template <class T>
 __global__ void __launch_bounds__(256) k_helm_rhs(HelmArgs<T> A, const T* __restrict__ xin,
-                                                  const T* __restrict__ b, T* __restrict__ r,
-                                                  const int* __restrict__ parent,
-                                                  const T* __restrict__ xc, int ncoarse) {
+                                                  const T* __restrict__ b, T* __restrict__ r) {
   const unsigned N = A.ncol;
   const int nl = A.nl;
   const size_t plane = (size_t)nl * N;
@@ -176,12 +173,9 @@ __global__ void __launch_bounds__(256) k_helm_rhs(HelmArgs<T> A, const T* __rest
   const unsigned total = N * (unsigned)nchunk;
   for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
     const unsigned kc = t / N, c = t - kc * N;
-    int nb[4], pn[4] = {0, 0, 0, 0};
+    int nb[4];
 #pragma unroll
-    for (int f = 0; f < 4; ++f) {
-      nb[f] = A.links[f * N + c];
-      if (PRO) pn[f] = parent[nb[f]];
-    }
+    for (int f = 0; f < 4; ++f) nb[f] = A.links[f * N + c];
     const int k0 = kc * KC;
     const int kn = min(KC, nl - k0);
     T out[KC];
@@ -191,11 +185,7 @@ __global__ void __launch_bounds__(256) k_helm_rhs(HelmArgs<T> A, const T* __rest
       const size_t i = (size_t)k * N + c;
       T hs = (T)0;
 #pragma unroll
-      for (int f = 0; f < 4; ++f) {
-        T xn = xin[(size_t)k * N + nb[f]];
-        if (PRO) xn = xn + xc[(size_t)k * ncoarse + pn[f]];
-        hs = hs + __ldcs(A.h + f * plane + i) * xn;
-      }
+      for (int f = 0; f < 4; ++f) hs = hs + __ldcs(A.h + f * plane + i) * xin[(size_t)k * N + nb[f]];
       out[kk] = __ldcs(b + i) + hs;
     }
 #pragma unroll
@@ -215,11 +205,10 @@ __global__ void __launch_bounds__(256) k_helm_rhs(HelmArgs<T> A, const T* __rest
 //     computes block b.
 constexpr int SP = 16;
 
-template <class T, bool XIN, bool PRO>
+template <class T, bool XIN>
 __global__ void __launch_bounds__(128) k_helm_subst(
     int ncol, int nl, const T* __restrict__ r, const T* __restrict__ sub,
-    const T* __restrict__ inv, const T* __restrict__ cp, const T* __restrict__ xin,
-    const int* __restrict__ parent, const T* __restrict__ xc, int ncoarse, T omega,
+    const T* __restrict__ inv, const T* __restrict__ cp, const T* __restrict__ xin, T omega,
     T* __restrict__ xout) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* sd = reinterpret_cast<T*>(smem_raw);     // [nl][blockDim]
@@ -265,14 +254,8 @@ __global__ void __launch_bounds__(128) k_helm_subst(
     }
   }
   // backward sweep
-  const int pc = PRO ? parent[c] : 0;
   const T om1 = (T)1 - omega;
-  auto xv_at = [&](int k) -> T {
-    const int kk = min(max(k, 0), nl - 1);
-    T v = xin[(size_t)kk * N + c];
-    if (PRO) v = v + xc[(size_t)kk * ncoarse + pc];
-    return v;
-  };
+  auto xv_at = [&](int k) -> T { return xin[(size_t)min(max(k, 0), nl - 1) * N + c]; };
   T ac[SP], ax[SP], bc[SP], bx[SP];
   const int ktop = nl - 1;
 #pragma unroll
@@ -438,20 +421,17 @@ __global__ void k_convert(TO* __restrict__ y, const TI* __restrict__ x, size_t n
 // the serial recurrences costs a memory latency.  S threads share a column,
 // each owning L = ceil(nl/S) consecutive levels (at most LMAX, kept in
 // registers), and the block has 128/S columns.  The right-hand side
-// r = b + H_off x_eff (x_eff = x_in, plus the parent's coarse value when PRO)
-// is formed in place, so the sweep is one kernel.  Both recurrences of the
+// r = b + H_off x_in is formed in place, so the sweep is one kernel.  Both recurrences of the
 // substitution,
 //   d_k = (r_k - sub_k d_{k-1}) inv_k,   z_k = d_k - c'_k z_{k+1},
 // are affine in the carried value: each thread composes its segment's map,
 // an inclusive scan of the maps over the S segments (shuffles of width S)
 // gives every segment its incoming value, and each segment then replays
 // its levels with exactly the sequential formulas from that value.
-template <class T, bool XIN, bool PRO, int S>
+template <class T, bool XIN, int S>
 __global__ void __launch_bounds__(128) k_helm_sweep_seg(HelmArgs<T> A, const T* __restrict__ b,
-                                                        const T* __restrict__ xin,
-                                                        const int* __restrict__ parent,
-                                                        const T* __restrict__ xc, int ncoarse,
-                                                        T omega, T* __restrict__ xout) {
+                                                        const T* __restrict__ xin, T omega,
+                                                        T* __restrict__ xout) {
   constexpr int LMAX = kSegLevels;
   const int tid = threadIdx.x, j = tid % S;
   const unsigned c = blockIdx.x * (128 / S) + tid / S;
@@ -460,15 +440,11 @@ __global__ void __launch_bounds__(128) k_helm_sweep_seg(HelmArgs<T> A, const T* 
   const size_t plane = (size_t)nl * N;
   const int L = (nl + S - 1) / S, k0 = j * L;
   const int nmy = c < N ? max(0, min(L, nl - k0)) : 0;
-  int nb[4] = {0, 0, 0, 0}, pn[4] = {0, 0, 0, 0}, pc = 0;
+  int nb[4] = {0, 0, 0, 0};
   if (XIN && nmy > 0) {
 #pragma unroll
-    for (int f = 0; f < 4; ++f) {
-      nb[f] = A.links[f * N + c];
-      if (PRO) pn[f] = parent[nb[f]];
-    }
+    for (int f = 0; f < 4; ++f) nb[f] = A.links[f * N + c];
   }
-  if (PRO && nmy > 0) pc = parent[c];
   T d[LMAX], iv[LMAX], sb[LMAX];
 #pragma unroll
   for (int u = 0; u < LMAX; ++u) {
@@ -479,11 +455,7 @@ __global__ void __launch_bounds__(128) k_helm_sweep_seg(HelmArgs<T> A, const T* 
       if (XIN) {
         T hs = (T)0;
 #pragma unroll
-        for (int f = 0; f < 4; ++f) {
-          T xn = xin[(size_t)k * N + nb[f]];
-          if (PRO) xn = xn + xc[(size_t)k * ncoarse + pn[f]];
-          hs = hs + A.h[f * plane + i] * xn;
-        }
+        for (int f = 0; f < 4; ++f) hs = hs + A.h[f * plane + i] * xin[(size_t)k * N + nb[f]];
         rv = rv + hs;
       }
       d[u] = rv;
@@ -547,11 +519,7 @@ __global__ void __launch_bounds__(128) k_helm_sweep_seg(HelmArgs<T> A, const T* 
       const size_t i = (size_t)k * N + c;
       z = k == nl - 1 ? d[u] : d[u] - cc[u] * z;
       T v = omega * z;
-      if (XIN) {
-        T xs = xin[i];
-        if (PRO) xs = xs + xc[(size_t)k * ncoarse + pc];
-        v = v + om1 * xs;
-      }
+      if (XIN) v = v + om1 * xin[i];
       xout[i] = v;
     }
 }
@@ -568,61 +536,51 @@ inline int seg_threads(lfg_ctx c, int ncol, int nl) {
   return S;
 }
 
-template <class T, bool XIN, bool PRO>
-void launch_sweep_seg(lfg_ctx c, int S, HelmArgs<T> A, const T* b, const T* xin,
-                      const int* parent, const T* xc, int ncoarse, T omega, T* xout) {
+template <class T, bool XIN>
+void launch_sweep_seg(lfg_ctx c, int S, HelmArgs<T> A, const T* b, const T* xin, T omega,
+                      T* xout) {
   const int cols = 128 / S;
   const unsigned grid = (unsigned)((A.ncol + cols - 1) / cols);
   switch (S) {
-    case 4: k_helm_sweep_seg<T, XIN, PRO, 4><<<grid, 128, 0, c->stream>>>(A, b, xin, parent, xc, ncoarse, omega, xout); break;
-    case 8: k_helm_sweep_seg<T, XIN, PRO, 8><<<grid, 128, 0, c->stream>>>(A, b, xin, parent, xc, ncoarse, omega, xout); break;
-    case 16: k_helm_sweep_seg<T, XIN, PRO, 16><<<grid, 128, 0, c->stream>>>(A, b, xin, parent, xc, ncoarse, omega, xout); break;
-    default: k_helm_sweep_seg<T, XIN, PRO, 32><<<grid, 128, 0, c->stream>>>(A, b, xin, parent, xc, ncoarse, omega, xout); break;
+    case 4: k_helm_sweep_seg<T, XIN, 4><<<grid, 128, 0, c->stream>>>(A, b, xin, omega, xout); break;
+    case 8: k_helm_sweep_seg<T, XIN, 8><<<grid, 128, 0, c->stream>>>(A, b, xin, omega, xout); break;
+    case 16: k_helm_sweep_seg<T, XIN, 16><<<grid, 128, 0, c->stream>>>(A, b, xin, omega, xout); break;
+    default: k_helm_sweep_seg<T, XIN, 32><<<grid, 128, 0, c->stream>>>(A, b, xin, omega, xout); break;
   }
-  // b, inv, sub, c' read and x written; x_in and the four couplings with
-  // XIN; the coarse field with PRO
-  const uint64_t n = (uint64_t)A.ncol * A.nl;
-  after_launch(c, "helm_sweep_seg",
-               sizeof(T) * ((XIN ? 10 : 5) * n + (PRO ? (uint64_t)ncoarse * A.nl : 0)));
+  // b, inv, sub, c' read and x written; x_in and the four couplings with XIN
+  after_launch(c, "helm_sweep_seg", sizeof(T) * (XIN ? 10 : 5) * (uint64_t)A.ncol * A.nl);
 }
 
-template <class T, bool XIN, bool PRO>
+template <class T, bool XIN>
 void launch_subst(lfg_ctx c, int ncol, int nl, const T* r, const T* sub, const T* inv,
-                  const T* cp, const T* xin, const int* parent, const T* xc, int ncoarse,
-                  T omega, T* xout) {
+                  const T* cp, const T* xin, T omega, T* xout) {
+  const void* ptrs[5] = {r, sub, inv, cp, xin};
+  if (subst_tma_applicable(c, ncol, nl, ptrs, 5, (int)sizeof(T))) {
+    subst_tma(c, ncol, nl, r, sub, inv, cp, XIN ? xin : nullptr, omega, xout);
+    return;
+  }
   // spread small meshes over every SM
   int bs = 128;
   while (bs > 32 && (ncol + bs - 1) / bs < 2 * c->num_sms) bs /= 2;
-  const size_t smem = (size_t)nl * bs * sizeof(T);
   constexpr size_t cap = 200 * 1024;
   if ((size_t)nl * 32 * sizeof(T) > cap)
     throw Error(LFG_ERR_ARG, "helm_smooth: column too tall for shared memory");
   while ((size_t)nl * bs * sizeof(T) > cap) bs /= 2;
-  if constexpr (!PRO) {
-    const void* ptrs[5] = {r, sub, inv, cp, xin};
-    if (subst_tma_applicable(c, ncol, nl, ptrs, 5, (int)sizeof(T))) {
-      subst_tma(c, ncol, nl, r, sub, inv, cp, XIN ? xin : nullptr, omega, xout);
-      return;
-    }
-  }
-  auto kern = k_helm_subst<T, XIN, PRO>;
+  auto kern = k_helm_subst<T, XIN>;
   static bool attr_set = false;
   if (!attr_set) {
     LFG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap));
     attr_set = true;
   }
   kern<<<(ncol + bs - 1) / bs, bs, (size_t)nl * bs * sizeof(T), c->stream>>>(
-      ncol, nl, r, sub, inv, cp, xin, parent, xc, ncoarse, omega, xout);
-  (void)smem;
-  // r, inv, sub, c' read and x written; x_in with XIN; the coarse field with PRO
-  after_launch(c, "helm_subst",
-               sizeof(T) * ((XIN ? 6 : 5) * (uint64_t)ncol * nl +
-                            (PRO ? (uint64_t)ncoarse * nl : 0)));
+      ncol, nl, r, sub, inv, cp, xin, omega, xout);
+  // r, inv, sub, c' read and x written; x_in with XIN
+  after_launch(c, "helm_subst", sizeof(T) * (XIN ? 6 : 5) * (uint64_t)ncol * nl);
 }
 
 template <class T>
 void smooth_t(lfg_helm op, double omega, lfg_field x_in, lfg_field b, lfg_field x_out,
-              lfg_intergrid ig, lfg_field xc, void* rbuf) {
+              void* rbuf) {
   lfg_ctx c = op->ctx;
   const T om = (T)omega;
   const T* sub = (const T*)op->sub;
@@ -631,40 +589,24 @@ void smooth_t(lfg_helm op, double omega, lfg_field x_in, lfg_field b, lfg_field 
   if (const int S = seg_threads(c, op->ncol, op->nl)) {
     const HelmArgs<T> A = args_of<T>(op);
     if (!x_in)
-      launch_sweep_seg<T, false, false>(c, S, A, (const T*)b->d, nullptr, nullptr, nullptr, 0, om,
-                                        (T*)x_out->d);
-    else if (!ig)
-      launch_sweep_seg<T, true, false>(c, S, A, (const T*)b->d, (const T*)x_in->d, nullptr,
-                                       nullptr, 0, om, (T*)x_out->d);
+      launch_sweep_seg<T, false>(c, S, A, (const T*)b->d, nullptr, om, (T*)x_out->d);
     else
-      launch_sweep_seg<T, true, true>(c, S, A, (const T*)b->d, (const T*)x_in->d, ig->parent,
-                                      (const T*)xc->d, ig->ncoarse, om, (T*)x_out->d);
+      launch_sweep_seg<T, true>(c, S, A, (const T*)b->d, (const T*)x_in->d, om, (T*)x_out->d);
     return;
   }
   if (!x_in) {
-    launch_subst<T, false, false>(c, op->ncol, op->nl, (const T*)b->d, sub, inv, cp, nullptr,
-                                  nullptr, nullptr, 0, om, (T*)x_out->d);
+    launch_subst<T, false>(c, op->ncol, op->nl, (const T*)b->d, sub, inv, cp, nullptr, om,
+                           (T*)x_out->d);
     return;
   }
   T* r = (T*)rbuf;
   const size_t work = (size_t)op->ncol * ((op->nl + KC - 1) / KC);
-  // x, b and the four couplings read, r written; the coarse field with PRO
-  const uint64_t rhs_bytes = sizeof(T) * (7 * (uint64_t)op->ncol * op->nl +
-                                          (ig ? (uint64_t)ig->ncoarse * op->nl : 0));
-  if (!ig) {
-    k_helm_rhs<T, false><<<occ_grid(c, (const void*)k_helm_rhs<T, false>, 256, work), 256, 0, c->stream>>>(args_of<T>(op), (const T*)x_in->d,
-                                                       (const T*)b->d, r, nullptr, nullptr, 0);
-    after_launch(c, "helm_rhs", rhs_bytes);
-    launch_subst<T, true, false>(c, op->ncol, op->nl, r, sub, inv, cp, (const T*)x_in->d,
-                                 nullptr, nullptr, 0, om, (T*)x_out->d);
-  } else {
-    k_helm_rhs<T, true><<<occ_grid(c, (const void*)k_helm_rhs<T, true>, 256, work), 256, 0, c->stream>>>(args_of<T>(op), (const T*)x_in->d,
-                                                      (const T*)b->d, r, ig->parent,
-                                                      (const T*)xc->d, ig->ncoarse);
-    after_launch(c, "helm_rhs", rhs_bytes);
-    launch_subst<T, true, true>(c, op->ncol, op->nl, r, sub, inv, cp, (const T*)x_in->d,
-                                ig->parent, (const T*)xc->d, ig->ncoarse, om, (T*)x_out->d);
-  }
+  k_helm_rhs<T><<<occ_grid(c, (const void*)k_helm_rhs<T>, 256, work), 256, 0, c->stream>>>(
+      args_of<T>(op), (const T*)x_in->d, (const T*)b->d, r);
+  // x, b and the four couplings read, r written
+  after_launch(c, "helm_rhs", sizeof(T) * 7 * (uint64_t)op->ncol * op->nl);
+  launch_subst<T, true>(c, op->ncol, op->nl, r, sub, inv, cp, (const T*)x_in->d, om,
+                        (T*)x_out->d);
 }
 
 void check_field(lfg_helm op, lfg_field f, const char* what) {
@@ -732,21 +674,16 @@ void helm_residual(lfg_helm op, lfg_field r_out, lfg_field x, lfg_field b, int s
 }
 
 void helm_smooth(lfg_helm op, double omega, lfg_field x_in, lfg_field b, lfg_field x_out,
-                 lfg_intergrid ig, lfg_field xc, void* rbuf) {
+                 void* rbuf) {
   check_field(op, b, "helm_smooth");
   check_field(op, x_out, "helm_smooth");
   if (x_in) {
     check_field(op, x_in, "helm_smooth");
     LFG_REQUIRE(x_in->d != x_out->d, "helm_smooth: x_out may not alias x_in");
   }
-  if (ig) {
-    LFG_REQUIRE(x_in && xc && ig->nfine == op->ncol && xc->ncol == ig->ncoarse &&
-                    xc->nlev == op->nl && xc->kind == op->kind,
-                "helm_smooth: bad prolongation arguments");
-  }
   if (x_in && !rbuf) rbuf = op->ctx->scratch((size_t)op->ncol * op->nl * op->kind);
-  if (op->kind == LFG_R_DOUBLE) smooth_t<double>(op, omega, x_in, b, x_out, ig, xc, rbuf);
-  else smooth_t<float>(op, omega, x_in, b, x_out, ig, xc, rbuf);
+  if (op->kind == LFG_R_DOUBLE) smooth_t<double>(op, omega, x_in, b, x_out, rbuf);
+  else smooth_t<float>(op, omega, x_in, b, x_out, rbuf);
 }
 
 void helm_residual_restrict(lfg_helm op, lfg_intergrid ig, lfg_field x, lfg_field b,
@@ -767,8 +704,6 @@ void helm_residual_restrict(lfg_helm op, lfg_intergrid ig, lfg_field x, lfg_fiel
   after_launch(c, "resid_restrict",
                (uint64_t)op->kind * op->nl * (9 * (uint64_t)op->ncol + ig->ncoarse));
 }
-
-bool helm_segmented(lfg_helm op) { return seg_threads(op->ctx, op->ncol, op->nl) > 0; }
 
 void prolong_add(lfg_intergrid ig, lfg_field fine, lfg_field coarse) {
   LFG_REQUIRE(fine->ncol == ig->nfine && coarse->ncol == ig->ncoarse &&
@@ -918,7 +853,7 @@ int lfg_helm_apply(lfg_helm op, lfg_field y, lfg_field x) {
 
 int lfg_helm_smooth(lfg_helm op, double omega, lfg_field x_in, lfg_field b, lfg_field x_out) {
   if (!op) return LFG_ERR_ARG;
-  return guard(op->ctx, [&] { helm_smooth(op, omega, x_in, b, x_out, nullptr, nullptr, nullptr); });
+  return guard(op->ctx, [&] { helm_smooth(op, omega, x_in, b, x_out, nullptr); });
 }
 
 int lfg_helm_coarsen(lfg_helm fine, lfg_intergrid ig, lfg_mesh cmesh, int kind,

@@ -349,16 +349,13 @@ void vec_scale_copy(lfg_field dst, Sc a, lfg_field src);        // dst = a src
 // Helmholtz launchers (lfg_helm.cu)
 void helm_apply(lfg_helm op, lfg_field y, lfg_field x, lfg_field dot_with, int slot);
 void helm_residual(lfg_helm op, lfg_field r, lfg_field x, lfg_field b, int norm_slot);
-// x_out = sweep(x_in [+ P xc]); x_in null: zero guess.  rbuf: workspace of
-// ncol*nl values of the operator's kind for the right-hand side (null: the
+// x_out = sweep(x_in); x_in null: zero guess.  rbuf: workspace of ncol*nl
+// values of the operator's kind for the right-hand side (null: the
 // context's scratch).
 void helm_smooth(lfg_helm op, double omega, lfg_field x_in, lfg_field b, lfg_field x_out,
-                 lfg_intergrid ig, lfg_field xc, void* rbuf);
+                 void* rbuf);
 void helm_residual_restrict(lfg_helm op, lfg_intergrid ig, lfg_field x, lfg_field b,
                             lfg_field bc);
 void prolong_add(lfg_intergrid ig, lfg_field fine, lfg_field coarse);
-// True when the operator's sweeps take the segmented one-kernel form (small
-// meshes), false when they run as right-hand side + substitution.
-bool helm_segmented(lfg_helm op);
 
 }  // namespace lfg

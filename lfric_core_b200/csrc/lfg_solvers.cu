@@ -122,9 +122,8 @@ FieldPtr make_field(lfg_ctx c, int kind, int ncol, int nlev) {
 // reference's multigrid glue lives outside lfric_core, it provides the
 // hierarchical operator/preconditioner types and the intergrid kernels):
 // n_pre block-Jacobi column sweeps from zero, residual fused with
-// restrict_mass_w3, the coarse-level cycle, prolong_scalar_unweighted
-// (added in place on fine levels, fused into the first of the n_post sweeps
-// on small ones); n_coarse sweeps from zero on the coarsest level.
+// restrict_mass_w3, the coarse-level cycle, prolong_scalar_unweighted added
+// in place, n_post sweeps; n_coarse sweeps from zero on the coarsest level.
 struct MgPrec : lfg_prec_s {
   std::vector<lfg_helm> ops;
   std::vector<lfg_intergrid> maps;
@@ -154,14 +153,12 @@ struct MgPrec : lfg_prec_s {
   }
 
   // s sweeps ending in `out`, alternating with `tmp`; the first reads `in`
-  // (null: zero guess), optionally prolongation-corrected by (ig, xc).
-  void sweeps(int l, int s, lfg_field in, lfg_field b, lfg_field out, lfg_field tmp,
-              lfg_intergrid ig, lfg_field xc) {
+  // (null: zero guess).
+  void sweeps(int l, int s, lfg_field in, lfg_field b, lfg_field out, lfg_field tmp) {
     lfg_field src = in;
     for (int i = 0; i < s; ++i) {
       lfg_field dst = ((s - 1 - i) % 2 == 0) ? out : tmp;
-      helm_smooth(ops[l], omega, src, b, dst, i == 0 ? ig : nullptr, i == 0 ? xc : nullptr,
-                  rr[l]->d);
+      helm_smooth(ops[l], omega, src, b, dst, rr[l]->d);
       src = dst;
     }
   }
@@ -170,24 +167,18 @@ struct MgPrec : lfg_prec_s {
     lfg_field T = xb[l].get();
     const int L = (int)ops.size();
     if (l == L - 1) {
-      if (n_coarse > 0) sweeps(l, n_coarse, nullptr, b, X, T, nullptr, nullptr);
+      if (n_coarse > 0) sweeps(l, n_coarse, nullptr, b, X, T);
       else vec_set(X, sc_const(0.0));
       return;
     }
     lfg_field P = (n_post % 2 == 0) ? X : T;  // iterate after pre-smoothing
-    if (n_pre > 0) sweeps(l, n_pre, nullptr, b, P, (P == X) ? T : X, nullptr, nullptr);
+    if (n_pre > 0) sweeps(l, n_pre, nullptr, b, P, (P == X) ? T : X);
     else vec_set(P, sc_const(0.0));
     helm_residual_restrict(ops[l], maps[l], P, b, bc[l + 1].get());
     vcycle(l + 1, bc[l + 1].get(), xa[l + 1].get());
-    if (n_post > 0 && helm_segmented(ops[l])) {
-      // small meshes: the correction fused into the first sweep's kernel
-      sweeps(l, n_post, P, b, X, T, maps[l], xa[l + 1].get());
-    } else {
-      // fine meshes: P += prolong(coarse) in place, then the plain sweeps
-      // (the same x + P xc values the fused sweep forms on the fly)
-      prolong_add(maps[l], P, xa[l + 1].get());
-      if (n_post > 0) sweeps(l, n_post, P, b, X, T, nullptr, nullptr);
-    }
+    // P += prolong(coarse) in place, then the post-smoothing sweeps
+    prolong_add(maps[l], P, xa[l + 1].get());
+    if (n_post > 0) sweeps(l, n_post, P, b, X, T);
   }
 
   // One captured CUDA graph per (input, output) buffer pair: the V-cycle is
