@@ -346,12 +346,7 @@ void launch_thomas_t(lfg_ctx c, const TriSrc<T>& s, const T* x, T* lhs) {
   const int bs = col_block(s.ncol, c->num_sms);
   const size_t smem = (size_t)MAXNL * bs * sizeof(T);
   auto kern = k_thomas<T, SRC, MAXNL>;
-  static bool attr = false;
-  if (!attr) {
-    LFG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                  (int)(MAXNL * 128 * sizeof(T))));
-    attr = true;
-  }
+  ensure_smem_attr((const void*)kern, (int)(MAXNL * 128 * sizeof(T)));
   kern<<<(s.ncol + bs - 1) / bs, bs, smem, c->stream>>>(s, x, lhs);
   // three bands and x read, the solution written
   after_launch(c, "thomas", sizeof(T) * 5 * (uint64_t)s.nrow * s.ncol);
@@ -746,11 +741,7 @@ int lfg_cma_apply_inverse(lfg_cma m, lfg_field lhs, lfg_field x) {
     while (smem_col * bs > 200 * 1024) bs /= 2;
     dispatch(m->kind, [&](auto tag) {
       using T = decltype(tag);
-      static std::once_flag attr;
-      std::call_once(attr, [] {
-        LFG_CUDA(cudaFuncSetAttribute(k_cma_subst<T>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                      200 * 1024));
-      });
+      ensure_smem_attr((const void*)k_cma_subst<T>, 200 * 1024);
       k_cma_subst<T><<<(m->ncol + bs - 1) / bs, bs, smem_col * bs, c->stream>>>(
           (const T*)m->bands, (const T*)m->finv, (const T*)m->fcp, m->ind_to, m->ncol, m->nrow,
           (const T*)x->d, (T*)lhs->d);

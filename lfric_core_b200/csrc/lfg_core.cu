@@ -11,6 +11,9 @@
 // runs are bit-identical.
 #include "lfg_internal.cuh"
 
+#include <map>
+#include <utility>
+
 #include <cstring>
 
 using namespace lfg;
@@ -648,6 +651,18 @@ void vec_scale_copy(lfg_field dst, Sc a, lfg_field src) {
 }  // namespace lfg
 
 namespace lfg {
+void ensure_smem_attr(const void* kern, int bytes) {
+  int dev = 0;
+  LFG_CUDA(cudaGetDevice(&dev));
+  static std::mutex mu;
+  static std::map<std::pair<const void*, int>, int> done;
+  std::lock_guard<std::mutex> lock(mu);
+  int& have = done[std::make_pair(kern, dev)];
+  if (have >= bytes) return;
+  LFG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes));
+  have = bytes;
+}
+
 void check_device_error(lfg_ctx c) {
   if (!c->dev_err) return;
   unsigned e = 0;

@@ -567,11 +567,7 @@ void launch_subst(lfg_ctx c, int ncol, int nl, const T* r, const T* sub, const T
     throw Error(LFG_ERR_ARG, "helm_smooth: column too tall for shared memory");
   while ((size_t)nl * bs * sizeof(T) > cap) bs /= 2;
   auto kern = k_helm_subst<T, XIN>;
-  static bool attr_set = false;
-  if (!attr_set) {
-    LFG_CUDA(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap));
-    attr_set = true;
-  }
+  ensure_smem_attr((const void*)kern, (int)cap);
   kern<<<(ncol + bs - 1) / bs, bs, (size_t)nl * bs * sizeof(T), c->stream>>>(
       ncol, nl, r, sub, inv, cp, xin, omega, xout);
   // r, inv, sub, c' read and x written; x_in with XIN

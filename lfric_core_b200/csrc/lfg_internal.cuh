@@ -268,12 +268,29 @@ inline void after_launch(lfg_ctx ctx, const char* what, uint64_t bytes = 0) {
 }
 
 void* dmalloc(size_t bytes);
+// Raises kern's dynamic shared-memory limit to `bytes` on the current
+// device; once per (kernel, device), thread-safe (the attribute belongs to
+// the kernel's module in each device's context).
+void ensure_smem_attr(const void* kern, int bytes);
 void dfree(void* p);
 void upload(void* d, const void* h, size_t bytes);
 
 // entry-point wrapper: converts exceptions into status codes
 template <class F>
 int guard(lfg_ctx ctx, F&& f) {
+  // the context's device is current for the call, the caller's afterwards
+  struct DeviceScope {
+    int prev = -1;
+    explicit DeviceScope(lfg_ctx c) {
+      int cur = 0;
+      if (c && cudaGetDevice(&cur) == cudaSuccess && cur != c->device &&
+          cudaSetDevice(c->device) == cudaSuccess)
+        prev = cur;
+    }
+    ~DeviceScope() {
+      if (prev >= 0) cudaSetDevice(prev);
+    }
+  } scope(ctx);
   try {
     f();
     return LFG_OK;

@@ -376,14 +376,6 @@ void launch_reg(lfg_ctx c, const TmaMaps& maps, int ncol, int nl, bool xin, T om
   constexpr int TCT = tile_cols<T>();
   const int nch = (nl + KCH - 1) / KCH;
   const size_t smem = sizeof(T) * (size_t)NST * NARR * KCH * TCT;
-  static std::once_flag attr_reg;
-  std::call_once(attr_reg, [&] {
-    auto set = [&](int, const void* k) {
-      LFG_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    };
-    for_reg_kernels<T, false, kRegChunks>(set);
-    for_reg_kernels<T, true, kRegChunks>(set);
-  });
   const void* kern = nullptr;
   auto pick = [&](int n, const void* k) {
     if (n == nch) kern = k;
@@ -391,6 +383,7 @@ void launch_reg(lfg_ctx c, const TmaMaps& maps, int ncol, int nl, bool xin, T om
   if (xin) for_reg_kernels<T, true, kRegChunks>(pick);
   else for_reg_kernels<T, false, kRegChunks>(pick);
   if (!kern) throw Error(LFG_ERR_ARG, "subst_tma: column taller than the register form");
+  ensure_smem_attr(kern, (int)smem);
   int per_sm = 0;
   LFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TCT, smem));
   const int ntile = (ncol + TCT - 1) / TCT;
@@ -431,12 +424,7 @@ void subst_tma(lfg_ctx c, int ncol, int nl, const float* r, const float* sub, co
   }
   const size_t smem = smem_bytes(nl);
   const void* kern = xin ? (const void*)k_subst_tma<true> : (const void*)k_subst_tma<false>;
-  static std::once_flag attr;
-  std::call_once(attr, [&] {
-    const int mx = (int)smem_bytes(kMaxLevels);
-    LFG_CUDA(cudaFuncSetAttribute(k_subst_tma<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-    LFG_CUDA(cudaFuncSetAttribute(k_subst_tma<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, mx));
-  });
+  ensure_smem_attr(kern, (int)smem_bytes(kMaxLevels));
   int per_sm = 0;
   LFG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TC, smem));
   const int ntile = (ncol + TC - 1) / TC;
