@@ -312,10 +312,13 @@ def measure_kernels(ctx, stream, peak: float) -> list:
         x.import_(prob.rhs)
         b.import_(prob.rhs)
         wl = f"C{N_FINE}x{NLAYERS} {tag}"
-        add("k_helm_apply (y = A x)", wl, 9 * N * w, time(lambda: H.apply(y, x)))
-        add("substitution from zero (k_subst_tma_reg FP32 / k_helm_subst FP64)", wl, 5 * N * w,
+        # couplings: 2 words per dof for FP64 operators (symmetric, each face
+        # read through one side), 4 for FP32 ones (per-side reads)
+        hw = 2 if kind == R_DOUBLE else 4
+        add("k_helm_apply (y = A x)", wl, (5 + hw) * N * w, time(lambda: H.apply(y, x)))
+        add("substitution from zero (k_subst_tma_reg)", wl, 5 * N * w,
             time(lambda: H.smooth(0.8, None, b, y)))
-        add("smoother sweep (k_helm_rhs + substitution)", wl, 13 * N * w,
+        add("smoother sweep (k_helm_rhs + substitution)", wl, (9 + hw) * N * w,
             time(lambda: H.smooth(0.8, x, b, y)))
         add("k_axpy (y = y + a x)", wl, 3 * N * w, time(lambda: y.axpy(0.5, x)))
         add("k_axpby (z = a x + b y)", wl, 3 * N * w, time(lambda: y.axpby(0.5, x, 0.25, b)))
@@ -510,7 +513,7 @@ def main():
                                                ys if i % 2 == 0 else xs))
     torch.cuda.nvtx.range_pop()
     subst_bytes = 5 * N * 4            # b, sub, inv, c' read; x written (FP32)
-    sweep_bytes = 10 * N * 4           # x, b, 4 couplings, sub, inv, c' read; x written
+    sweep_bytes = 13 * N * 4           # rhs: x, b, 4 couplings, r; subst: r, inv, sub, c', x_in, x
     peak, peak_kind = measured_hbm_peak()
     achieved = subst_bytes / (subst_ms * 1e-3) / 1e9
     traffic = None

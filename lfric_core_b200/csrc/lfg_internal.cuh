@@ -182,6 +182,13 @@ struct lfg_mesh_s {
   int ncol = 0;
   int* links = nullptr;  // device, SoA [4][ncol]
   std::vector<int> h_links;  // host copy, [ncol][4]
+  // For each side f of column c, the side whose coupling stands for its face:
+  // hsrc[f][c] = g << 29 | d reads side g of column d.  Of a face's two sides
+  // the one with the larger side index (N > E > S > W; then the smaller
+  // column) is read for both, so inside a panel a column reads its own E and
+  // N couplings and its W and S neighbours' E and N ones.  Null when the
+  // links do not pair up.
+  int* hsrc = nullptr;  // device [4][ncol]
 };
 
 struct lfg_intergrid_s {
@@ -250,6 +257,9 @@ struct lfg_helm_s {
   void* diag = nullptr;
   void* sup = nullptr;
   void* h = nullptr;     // [4][nl][ncol]
+  // every face's two sides carry the same coupling bit for bit, so the
+  // kernels read each face through mesh->hsrc (half the coupling traffic)
+  bool hsym = false;
   // Thomas factors of T' (columnwise_op_appinv's inverse denominators and
   // c'), functions of the matrix alone: computed once per operator
   void* inv = nullptr;   // [nl][ncol]

@@ -46,6 +46,29 @@ def test_helmholtz_column_heights(ctx, n, nl, kind):
     ctx.synchronize()
 
 
+@pytest.mark.parametrize("n", [8, 96])
+def test_helmholtz_nonsymmetric_couplings(ctx, n):
+    """Couplings whose two sides of a face differ are read per side (the
+    kernels read each face through one designated side only when every face
+    agrees bit for bit): apply and both sweep forms against the oracle, on
+    the segmented (C8) and the element-parallel + TMA (C96) sweep paths."""
+    p = helmholtz_problem(n, 10, seed=27, mg_levels=1)
+    hf = p.hf.copy().reshape(-1, 4)
+    hf[5, 0] *= 1.5                        # one side of one face
+    p.hf = hf.ravel()
+    ora = OraHelm(p)
+    H = api.Helmholtz(ctx, R_DOUBLE, api.Mesh(ctx, p.links), p.nlayers, p.cm, p.hf)
+    rng = np.random.default_rng(28)
+    x, b = rng.standard_normal(p.ndof), rng.standard_normal(p.ndof)
+    X, B, Y = H.field(x), H.field(b), H.field()
+    H.apply(Y, X)
+    assert rel(Y.export(), ora.apply(x)) < 1e-12
+    H.smooth(0.8, X, B, Y)
+    assert rel(Y.export(), ora.smooth(x, b, 0.8)) < 1e-12
+    H.smooth(0.8, None, B, Y)
+    assert rel(Y.export(), ora.smooth(None, b, 0.8)) < 1e-12
+
+
 @pytest.mark.parametrize("nl,kind", [(1, R_DOUBLE), (2, R_SINGLE), (13, R_DOUBLE), (33, R_DOUBLE),
                                      (33, R_SINGLE), (70, R_DOUBLE), (100, R_DOUBLE)])
 def test_cma_appinv_column_heights(ctx, nl, kind):

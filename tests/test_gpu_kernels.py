@@ -453,21 +453,24 @@ def test_multigrid_vcycle(ctx, helm_small, kind):
         assert rel(Y.export(np.float64), ora.mg_apply(b.astype(np.float32))) < 1e-5
 
 
-@pytest.mark.parametrize("n,sweep_words", [(8, 10), (96, 13)])
+@pytest.mark.parametrize("n,sweep_words", [(8, 6), (96, 9)])
 @pytest.mark.parametrize("kind,w", [(R_DOUBLE, 8), (R_SINGLE, 4)])
 def test_algorithmic_byte_counter(ctx, kind, w, n, sweep_words):
     """lfg_ctx_algorithmic_bytes adds each kernel's arrays once per launch:
-    9 words per dof for the Helmholtz apply, 3 for axpy, 2 for a dot, 5 for
-    the smoother sweep from zero; the sweep from a guess is 10 words as one
-    segmented kernel (C8) and 7 + 6 as right-hand side + substitution
-    (C96)."""
+    5 words per dof plus the couplings for the Helmholtz apply, 3 for axpy,
+    2 for a dot, 5 for the smoother sweep from zero; the sweep from a guess
+    is 6 words plus the couplings as one segmented kernel (C8) and 3 + 6
+    plus the couplings as right-hand side + substitution (C96).  The
+    couplings count 2 words per dof for the FP64 operator (symmetric, each
+    face read through one side) and 4 for the FP32 one."""
     p = helmholtz_problem(n, 12, seed=41, mg_levels=1)
     H = api.Helmholtz(ctx, kind, api.Mesh(ctx, p.links), p.nlayers, p.cm, p.hf)
     X, Y, B = H.field(p.rhs), H.field(), H.field(p.rhs)
     ndof = p.ndof
-    for fn, words in ((lambda: H.apply(Y, X), 9), (lambda: Y.axpy(0.5, X), 3),
+    hw = 2 if kind == R_DOUBLE else 4
+    for fn, words in ((lambda: H.apply(Y, X), 5 + hw), (lambda: Y.axpy(0.5, X), 3),
                       (lambda: X.dot(Y), 2), (lambda: H.smooth(0.8, None, B, Y), 5),
-                      (lambda: H.smooth(0.8, X, B, Y), sweep_words)):
+                      (lambda: H.smooth(0.8, X, B, Y), sweep_words + hw)):
         b0 = ctx.algorithmic_bytes()
         fn()
         assert ctx.algorithmic_bytes() - b0 == words * ndof * w
