@@ -18,6 +18,12 @@
 // lfg_subst_tma.cu; on small meshes S threads share a column in the
 // segmented sweep), so at every level a warp reads consecutive columns of
 // each level-major array.
+//
+// H_off is symmetric: the two sides of a face hold one coupling.  A mesh
+// names one designated side per face (hsrc); an FP64 operator whose sides
+// all equal their designated sides bit for bit (checked once, k_face_check)
+// is read through them (the CF kernel variants), 2 coupling words per dof
+// instead of 4.
 #include "lfg_internal.cuh"
 
 #include <algorithm>
