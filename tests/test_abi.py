@@ -35,3 +35,18 @@ def test_version_and_null_handles():
     assert lib.lfg_ctx_synchronize(None) == 3          # LFG_ERR_ARG
     assert lib.lfg_field_import(None, None, 8) == 3
     assert lib.lfg_solver_apply(None, None, None, None, None) == 3
+
+
+def test_python_constants_match_the_header():
+    """The Python front end's kinds, statuses and solver methods carry the
+    header's values (the Fortran binding reads the same header)."""
+    from lfric_core_b200 import api
+    text = _lib.HEADER.read_text()
+    defs = {m.group(1): int(m.group(2))
+            for m in re.finditer(r"#define\s+(LFG_\w+)\s+(\d+)\b", text)}
+    assert (api.R_SINGLE, api.R_DOUBLE) == (defs["LFG_R_SINGLE"], defs["LFG_R_DOUBLE"])
+    assert (api.OK, api.NOT_CONVERGED, api.NAN_STATUS) == (
+        defs["LFG_OK"], defs["LFG_NOT_CONVERGED"], defs["LFG_NAN"])
+    solvers = {k[len("LFG_SOLVER_"):].lower(): v for k, v in defs.items()
+               if k.startswith("LFG_SOLVER_")}
+    assert solvers == api.SOLVERS
