@@ -137,58 +137,88 @@ def host_threads() -> int:
         return os.cpu_count() or 1
 
 
-_CPU_PROBLEMS = {}
+_CPU = {}
 
 
-def cpu_sample(n_sample: int, threads: int):
-    """The oracle's mixed solve on C_{n_sample} x 70 on `threads` OpenMP
-    threads; returns (seconds, status, info).  Problem setup is not timed."""
+def cpu_oracle(n: int):
+    """The seeded C_n x 70 problem and the oracle's view of it on the -O3
+    -march=native -fopenmp build (built on this host); set-up is not timed."""
     from lfric_core_b200.problems import helmholtz_problem
-    from oracle.oracle import Helmholtz as OraHelm, lib
-    used = lib().ora_threads(threads)
-    if n_sample not in _CPU_PROBLEMS:
-        p = helmholtz_problem(n_sample, NLAYERS, seed=SEED, mg_levels=MG_LEVELS)
-        _CPU_PROBLEMS[n_sample] = (p, OraHelm(p))
-    p, ora = _CPU_PROBLEMS[n_sample]
+    from oracle.oracle import Helmholtz as OraHelm
+    if n not in _CPU:
+        p = helmholtz_problem(n, NLAYERS, seed=SEED, mg_levels=MG_LEVELS)
+        _CPU[n] = (p, OraHelm(p, native=True))
+    return _CPU[n]
+
+
+def cpu_solve(n: int, threads: int, form: str = "mixed"):
+    """One complete solve of the C_n x 70 system by the oracle on `threads`
+    OpenMP threads, from zero to 1e-8: the mixed form (FP32 inner GCR(10) +
+    multigrid, FP64 refinement) or the plain FP64 GCR(10) + multigrid.
+    Returns (seconds, threads used)."""
+    p, ora = cpu_oracle(n)
+    used = ora.L.ora_threads(threads)
     t0 = time.perf_counter()
-    _, st, info = ora.mixed_solve(p.rhs)
+    if form == "mixed":
+        _, st, _ = ora.mixed_solve(p.rhs)
+    else:
+        _, st, _ = ora.gcr_mg_solve(p.rhs)
     dt = time.perf_counter() - t0
-    return dt, st, info, used
+    if st != 0:
+        raise RuntimeError(f"CPU {form} solve on C{n} ended with status {st}")
+    return dt, used
 
 
-def reference_sample_size(n: int, threads: int) -> int:
-    """The full C_n workload when the host has the cores to finish it in a few
-    seconds a solve, else C_{n/2} with the throughput scaled by the dof ratio."""
-    return n if threads >= 32 else max(24, n // 2)
+def cpu_baselines(n: int, n_all: int) -> dict:
+    """The CPU path on the full C_n x 70 workload: `n_all` mixed solves and
+    one FP64 solve on all host threads, and one mixed solve on one thread."""
+    threads = host_threads()
+    _, used = cpu_solve(n, threads)                    # first touch of the work arrays
+    t_all = [cpu_solve(n, threads)[0] for _ in range(n_all)]
+    t64, _ = cpu_solve(n, threads, "fp64")
+    t1, _ = cpu_solve(n, 1)
+    lib_note = "oracle C restatement built -O3 -march=native -fopenmp on this host"
+    return {
+        "all_threads": {"value": n_all / sum(t_all), "unit": "solves/s", "cores": used,
+                        "sample": f"{n_all} mixed solves on C{n}x{NLAYERS}, {used} OpenMP threads "
+                                  f"({lib_note}), {sum(t_all):.1f} s"},
+        "fp64_all_threads": {"value": 1.0 / t64, "unit": "solves/s", "cores": used,
+                             "sample": f"1 FP64 GCR(10)+MG solve on C{n}x{NLAYERS}, "
+                                       f"{used} threads, {t64:.1f} s"},
+        "one_thread": {"value": 1.0 / t1, "unit": "solves/s", "cores": 1,
+                       "sample": f"1 mixed solve on C{n}x{NLAYERS}, 1 thread, {t1:.1f} s"},
+    }
 
 
 def run_reference(args, rank, world):
-    """CPU reference arm: rank 0 alone times the oracle on all host cores."""
+    """CPU reference arm: rank 0 alone times the oracle's mixed solve on the
+    full C192 x 70 workload on all host threads (the Fortran reference
+    cannot be compiled here, so the restatement stands in for it)."""
     if rank != 0:
         return
     threads = host_threads()
-    n_sample = reference_sample_size(args.n, threads)
-    scale = (n_sample / args.n) ** 2          # solve cost scales with the dof count
     for _ in range(args.warmup):
-        cpu_sample(n_sample, threads)
-    times = []
+        cpu_solve(args.n, threads)
+    times, used = [], threads
     for _ in range(args.steps):
-        dt, st, info, used = cpu_sample(n_sample, threads)
+        dt, used = cpu_solve(args.n, threads)
         times.append(dt)
     t = float(np.sum(times))
-    value = args.steps * scale / t
-    sample = (f"one full mixed solve per step on C{n_sample}x{NLAYERS} (the C oracle, "
-              f"{used} OpenMP threads)" + (f", throughput scaled to C{args.n} by the dof "
-                                           f"ratio {scale:.4f}" if n_sample != args.n else ""))
+    value = args.steps / t
+    t1, _ = cpu_solve(args.n, 1)
+    sample = (f"one full mixed solve per step on C{args.n}x{NLAYERS} (oracle C restatement built "
+              f"-O3 -march=native -fopenmp on this host, {used} OpenMP threads)")
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": "solves/s",
         "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1e3 * t / args.steps / scale, "higher_is_better": True,
+        "ms_per_step": 1e3 * t / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64", "data": "synthetic",
         "config": {"workload": f"helmholtz_c{args.n}x{NLAYERS}_gcr10_mg{MG_LEVELS}_mixed_to_1e-8",
-                   "sample": f"C{n_sample}x{NLAYERS}"},
+                   "sample": f"C{args.n}x{NLAYERS}"},
         "cpu_baseline": {"value": value, "unit": "solves/s", "cores": used, "kind": "port",
                          "sample": sample},
+        "one_thread": {"value": 1.0 / t1, "unit": "solves/s", "cores": 1,
+                       "sample": f"1 mixed solve on C{args.n}x{NLAYERS}, 1 thread, {t1:.1f} s"},
         "e2e": {"value": value, "unit": "solves/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -306,6 +336,8 @@ def measure_kernels(ctx, stream, peak: float) -> list:
     prob = helmholtz_problem(N_FINE, NLAYERS, seed=SEED, mg_levels=2)
     N = prob.ndof
     mesh = api.Mesh(ctx, prob.links)
+    ig = api.Intergrid(ctx, prob.mg_child[0], prob.ncol)
+    nc = prob.mg_child[0].shape[0]
     for kind, w, tag in ((R_SINGLE, 4, "FP32"), (R_DOUBLE, 8, "FP64")):
         H = api.Helmholtz(ctx, kind, mesh, NLAYERS, prob.cm, prob.hf)
         x, b, y = H.field(), H.field(), H.field()
@@ -316,17 +348,23 @@ def measure_kernels(ctx, stream, peak: float) -> list:
         # read through one side), 4 for FP32 ones (per-side reads)
         hw = 2 if kind == R_DOUBLE else 4
         add("k_helm_apply (y = A x)", wl, (5 + hw) * N * w, time(lambda: H.apply(y, x)))
+        add("k_helm_rhs (r = b + H_off x)", wl, (3 + hw) * N * w,
+            time(lambda: H.sweep_rhs(x, b, y)))
+        Cb = Field(ctx, kind, nc, NLAYERS)
+        add("k_helm_resid_restrict (restrict_mass_w3(b - A x))",
+            f"C{N_FINE}->C{N_FINE // 2}x{NLAYERS} {tag}", (5 + hw) * N * w + nc * NLAYERS * w,
+            time(lambda: H.residual_restrict(ig, x, b, Cb)))
         add("substitution from zero (k_subst_tma_reg)", wl, 5 * N * w,
             time(lambda: H.smooth(0.8, None, b, y)))
         add("smoother sweep (k_helm_rhs + substitution)", wl, (9 + hw) * N * w,
             time(lambda: H.smooth(0.8, x, b, y)))
         add("k_axpy (y = y + a x)", wl, 3 * N * w, time(lambda: y.axpy(0.5, x)))
         add("k_axpby (z = a x + b y)", wl, 3 * N * w, time(lambda: y.axpby(0.5, x, 0.25, b)))
-        add("k_dot (<x, y>, FP64 accumulation)", wl, 2 * N * w, time(lambda: x.dot(b)))
-        del H, x, b, y
+        dres = torch.zeros(1, dtype=torch.float64, device="cuda")
+        add("k_dot (<x, y>, FP64 accumulation, result left on the device)", wl, 2 * N * w,
+            time(lambda: x.dot_into(b, dres.data_ptr())))
+        del H, x, b, y, Cb
     # intergrid C192 -> C96 (FP64): restrict_mass_w3 and prolong_scalar_unweighted
-    ig = api.Intergrid(ctx, prob.mg_child[0], prob.ncol)
-    nc = prob.mg_child[0].shape[0]
     F = Field(ctx, R_DOUBLE, prob.ncol, NLAYERS)
     Cc = Field(ctx, R_DOUBLE, nc, NLAYERS)
     F.set_scalar(1.0)
@@ -485,10 +523,11 @@ def main():
     R.aypx(-1.0, system.b64)
     true_rel = R.norm() / system.b64.norm()
 
-    # ---- roofline of the dominant kernel family: the column substitution
-    # (the zero-start smoother sweep is exactly one launch of it,
-    # k_subst_tma_reg on FP32 fine meshes), on the C192 level; the full sweep from a nonzero
-    # guess (k_helm_rhs + the substitution) is timed beside it
+    # ---- roofline of the dominant kernel: the sweep right-hand side
+    # r = b + H_off x (k_helm_rhs<float>, the largest single share of the
+    # mixed solve's time), on the C192 level, FP32; the substitution from
+    # zero (one launch of the TMA substitution) and the whole sweep from a
+    # nonzero guess (k_helm_rhs + the substitution) are timed beside it
     op32 = system.levels32[0]
     xs, bs, ys = op32.field(), op32.field(), op32.field()
     xs.copy(system.x64)
@@ -508,40 +547,32 @@ def main():
         return e0.elapsed_time(e1) / nrep
 
     torch.cuda.nvtx.range_push("smoother_roofline")
+    rhs_ms = time_loop(lambda i: op32.sweep_rhs(xs, bs, ys))
     subst_ms = time_loop(lambda i: op32.smooth(0.8, None, bs, ys if i % 2 == 0 else xs))
     sweep_ms = time_loop(lambda i: op32.smooth(0.8, xs if i % 2 == 0 else ys, bs,
                                                ys if i % 2 == 0 else xs))
     torch.cuda.nvtx.range_pop()
+    rhs_bytes = 7 * N * 4              # x, b, the 4 per-side couplings read; r written
     subst_bytes = 5 * N * 4            # b, sub, inv, c' read; x written (FP32)
     sweep_bytes = 13 * N * 4           # rhs: x, b, 4 couplings, r; subst: r, inv, sub, c', x_in, x
     peak, peak_kind = measured_hbm_peak()
-    achieved = subst_bytes / (subst_ms * 1e-3) / 1e9
-    traffic = None
+    traffic = {}
     tp = ROOT / "profiles" / "roofline_traffic.json"
     if tp.exists():
-        t = json.loads(tp.read_text())
-        traffic = t["dram_bytes_per_launch"] * N / t["dofs"]
+        for name, t in json.loads(tp.read_text()).get("kernels", {}).items():
+            traffic[name] = t["dram_bytes_per_launch"] * N / t["dofs"]
 
     # ---- batched persistent solves (every rank: replicas)
     torch.cuda.nvtx.range_push("batched")
     batched = measure_batched(ctx, stream, max(1, args.steps), max(1, args.warmup), world=world)
     torch.cuda.nvtx.range_pop()
 
-    # ---- CPU baseline (rank 0, N=1 only): the oracle on a bounded sample
+    # ---- CPU baseline (rank 0, N=1 only): the oracle on the same workload
     cpu = None
     if rank == 0 and world == 1:
-        threads = host_threads()
-        n_sample = max(24, args.n // 2)
-        scale = (n_sample / args.n) ** 2
-        times = []
-        while len(times) < 2 or (sum(times) < 10.0 and len(times) < 20):
-            dt, st, info, used = cpu_sample(n_sample, threads)
-            times.append(dt)
-        dt = float(np.median(times))
-        cpu = {"value": scale / dt, "unit": "solves/s", "cores": used, "kind": "port",
-               "sample": f"{len(times)} mixed solves on C{n_sample}x{NLAYERS} with the C oracle "
-                         f"on {used} OpenMP threads (median {dt:.2f} s), scaled to C{args.n} "
-                         f"by the dof ratio {scale:.4f}"}
+        cb = cpu_baselines(args.n, 3)
+        cpu = dict(cb["all_threads"], kind="port", one_thread=cb["one_thread"],
+                   fp64_all_threads=cb["fp64_all_threads"])
 
     value = world * args.steps / (ms_mixed * 1e-3)
     fp64_value = world * args.steps / (ms_fp64 * 1e-3)
@@ -573,14 +604,21 @@ def main():
                        "frac": nb / (ms * 1e-3 / args.steps) / 1e9 / peak}
                 for form, nb, ms in (("mixed", bytes_mixed, ms_mixed), ("fp64", bytes_fp64, ms_fp64))},
             "roofline": {"bound": "hbm",
-                         "kernel": "k_subst_tma_reg<false,5> zero-start column sweep (TMA-staged, d' in registers), C192x70",
-                         "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "peak_source": peak_kind,
-                         "traffic": traffic, "algorithmic_bytes": subst_bytes,
-                         "ms_per_launch": subst_ms},
-            "smoother_sweep": {"kernels": "k_helm_rhs + k_subst_tma_reg<true,5>, FP32, C192x70",
+                         "kernel": "k_helm_rhs<float> sweep right-hand side r = b + H_off x, C192x70",
+                         "achieved": rhs_bytes / (rhs_ms * 1e-3) / 1e9, "peak": peak,
+                         "unit": "GB/s", "frac": rhs_bytes / (rhs_ms * 1e-3) / 1e9 / peak,
+                         "peak_source": peak_kind, "traffic": traffic.get("k_helm_rhs"),
+                         "algorithmic_bytes": rhs_bytes, "ms_per_launch": rhs_ms},
+            "substitution": {"kernel": "k_subst_tma_reg<float,0,5> zero-start column "
+                                       "substitution (TMA-staged, d' in registers), C192x70",
+                             "ms": subst_ms, "algorithmic_bytes": subst_bytes,
+                             "GB/s": subst_bytes / (subst_ms * 1e-3) / 1e9,
+                             "frac": subst_bytes / (subst_ms * 1e-3) / 1e9 / peak,
+                             "traffic": traffic.get("k_subst_tma_reg")},
+            "smoother_sweep": {"kernels": "k_helm_rhs + k_subst_tma_reg<float,1,5>, FP32, C192x70",
                                "ms": sweep_ms, "algorithmic_bytes": sweep_bytes,
-                               "GB/s": sweep_bytes / (sweep_ms * 1e-3) / 1e9},
+                               "GB/s": sweep_bytes / (sweep_ms * 1e-3) / 1e9,
+                               "frac": sweep_bytes / (sweep_ms * 1e-3) / 1e9 / peak},
             "batched": batched,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),

@@ -7,8 +7,11 @@
  * *_device_ptr / lfg_field_wrap entry points, which exchange raw CUDA device
  * pointers.  Index arrays are 0-based (the Fortran iso_c_binding shim
  * subtracts one), except the CMA's indirection maps and column-banded
- * dofmaps, which keep the reference's 1-based row and column numbers.  A Fortran caller binds these with bind(C) interfaces; see
- * INTEGRATION.md for the module that extends the reference's abstract types.
+ * dofmaps, which keep the reference's 1-based row and column numbers.  A
+ * Fortran caller binds these with bind(C) interfaces, wrapped in types that
+ * extend the reference's abstract_linear_operator_type,
+ * abstract_preconditioner_type, abstract_vector_type and
+ * abstract_iterative_solver_type.
  *
  * Field layout.  A field is the set of dofs of one function space on an
  * extruded mesh: ncol horizontal entities (cells for W3/Wtheta, vertices
@@ -74,6 +77,14 @@ int lfg_ctx_kernel_launches(lfg_ctx ctx, uint64_t* count);
  * bandwidth.  A diagnostic of this library, with no counterpart in the
  * reference. */
 int lfg_ctx_algorithmic_bytes(lfg_ctx ctx, uint64_t* bytes);
+/* Test hook, no counterpart in the reference: the TMA column substitutions
+ * of kernels launched from now on (lfg_helm_smooth on fine meshes) give up
+ * a stage wait after `spins` polls (0: at once), record the failure and
+ * return after their issued loads have landed, so the next
+ * lfg_ctx_synchronize reports LFG_ERR_STATE.  A negative value restores the
+ * built-in limit.  Kernels already captured in a solver's CUDA graphs keep
+ * the limit they were captured with. */
+int lfg_ctx_test_tma_spin_limit(lfg_ctx ctx, long long spins);
 /* Message of the last failed call on this context (never NULL). */
 const char* lfg_last_error(lfg_ctx ctx);
 /* Library version string and the compute capability it was built for. */
@@ -109,6 +120,11 @@ int lfg_X_divideby_Y(lfg_field z, lfg_field x, lfg_field y);            /* Z = X
  * (sci_psykal_light_mod.f90:72-214); deterministic two-level reduction. */
 int lfg_X_innerproduct_Y(lfg_field x, lfg_field y, double* result);
 int lfg_X_innerproduct_X(lfg_field x, double* result);
+/* The same inner product written to one double of device memory, in the
+ * context's stream order, without waiting for it (no counterpart in the
+ * reference, whose inner products return to the host): for callers that
+ * keep Krylov scalars on the device. */
+int lfg_X_innerproduct_Y_device(lfg_field x, lfg_field y, void* device_result);
 
 /* ---------------------------------------------------------------- meshes */
 /* Horizontal cubed-sphere connectivity: links[4*c + f] is the neighbour of
@@ -192,14 +208,22 @@ int lfg_tri_solve(lfg_field y, lfg_field x, lfg_field tri_0, lfg_field tri_plus,
  * the GPU's memory up front, a caching pool) or that are recovering from an
  * out-of-memory error, and so cannot call cudaMalloc or create a context.
  * The caller passes level-major device arrays (nlev*ncol values of `kind`)
- * and a cudaStream_t (NULL: the legacy default stream).  Working storage is
- * one file-scope device array of LFG_NOALLOC_SCRATCH_BYTES that every GPU
- * loading the library keeps until exit; a call needs 2*nlev*ncol*kind bytes
- * of it and fails with LFG_ERR_ARG beyond that.  The first call on a device
- * looks up the array's device address.  All calls share the array: calls
- * whose kernels overlap on the GPU (different streams, or other host
- * threads) race on it.  Nothing in it needs clearing; each call writes its
- * part before reading it. */
+ * on the current device and a cudaStream_t (NULL: the legacy default
+ * stream).  Working storage is one file-scope device array of
+ * LFG_NOALLOC_SCRATCH_BYTES that every GPU loading the library keeps until
+ * exit; a call needs 2*nlev*ncol*kind bytes of it and fails with
+ * LFG_ERR_ARG beyond that.
+ * Set-up per device: the array's device address is looked up and the
+ * library's device code loaded on that device, which may itself need
+ * memory.  lfg_ctx_create does this for its device.  On a device where no
+ * context was ever created, the first call does it instead: make that first
+ * call (or create a context) before memory runs short, and before any
+ * stream capture.
+ * The status is that of this call's own launch; errors left by the caller's
+ * earlier work are neither reported nor cleared.  All calls share the
+ * array: calls whose kernels overlap on the GPU (different streams, or
+ * other host threads) race on it.  Nothing in it needs clearing; each call
+ * writes its part before reading it. */
 #define LFG_NOALLOC_SCRATCH_BYTES (32u << 20)
 int lfg_tri_solve_noalloc(int kind, int ncol, int nlev, const void* x, const void* tri_0,
                           const void* tri_plus, const void* tri_minus, void* y,
@@ -269,6 +293,16 @@ int lfg_helm_apply(lfg_helm helm, lfg_field y, lfg_field x);          /* y = A x
  * x_in NULL means a zero initial guess. */
 int lfg_helm_smooth(lfg_helm helm, double omega, lfg_field x_in, lfg_field b,
                     lfg_field x_out);
+/* The multigrid V-cycle's building blocks, one launch each (no counterpart
+ * in the reference, whose multigrid lives in the applications):
+ * coarse_b = restrict_mass_w3(b - A x), the residual summed over each coarse
+ * cell's children in cell_map order
+ * (sci_restrict_mass_w3_kernel_mod.F90:126-179 applied to b - A x); */
+int lfg_helm_residual_restrict(lfg_helm helm, lfg_intergrid ig, lfg_field x, lfg_field b,
+                               lfg_field coarse_b);
+/* r = b + H_off x, the right-hand side T' x_out = r of a block-Jacobi
+ * column sweep (lfg_helm_smooth's first kernel on fine meshes). */
+int lfg_helm_sweep_rhs(lfg_helm helm, lfg_field x, lfg_field b, lfg_field r);
 /* Galerkin coarse operator R A P (R = restrict_mass_w3, P = prolong_scalar_unweighted). */
 int lfg_helm_coarsen(lfg_helm fine, lfg_intergrid ig, lfg_mesh coarse_mesh, int kind,
                      lfg_helm* coarse);

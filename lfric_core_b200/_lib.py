@@ -32,7 +32,7 @@ class lfg_batch_cfg(C.Structure):
 def _ctype(tok: str):
     t = " ".join(tok.replace("const ", "").split())
     table = {
-        "int": C.c_int, "double": C.c_double, "void*": C.c_void_p, "void *": C.c_void_p,
+        "int": C.c_int, "long long": C.c_longlong, "double": C.c_double, "void*": C.c_void_p, "void *": C.c_void_p,
         "int*": C.POINTER(C.c_int), "double*": C.POINTER(C.c_double),
         "uint64_t*": C.POINTER(C.c_uint64), "int64_t*": C.POINTER(C.c_int64),
         "char*": C.c_char_p,

@@ -85,6 +85,12 @@ class Context:
     def set_stream(self, stream_ptr: int | None):
         self.check(self.lib.lfg_ctx_set_stream(self.h, C.c_void_p(stream_ptr or 0)), "set_stream")
 
+    def test_tma_spin_limit(self, spins: int):
+        """Test hook: TMA stage waits give up after `spins` polls (< 0: the
+        built-in limit)."""
+        self.check(self.lib.lfg_ctx_test_tma_spin_limit(self.h, C.c_longlong(spins)),
+                   "test_tma_spin_limit")
+
     def kernel_launches(self) -> int:
         n = C.c_uint64()
         self.check(self.lib.lfg_ctx_kernel_launches(self.h, C.byref(n)))
@@ -201,6 +207,13 @@ class Field(_Handle):
         r = C.c_double()
         self.ctx.check(self.ctx.lib.lfg_X_innerproduct_Y(self.h, x.h, C.byref(r)), "innerproduct")
         return r.value
+
+    def dot_into(self, x: "Field", device_ptr: int):
+        """<self, x> written to the double at device_ptr in stream order
+        (no host synchronisation)."""
+        self.ctx.check(self.ctx.lib.lfg_X_innerproduct_Y_device(self.h, x.h,
+                                                                C.c_void_p(device_ptr)),
+                       "innerproduct_device")
 
     def norm(self) -> float:
         r = C.c_double()
@@ -429,6 +442,16 @@ class Helmholtz(_Handle):
     def smooth(self, omega: float, x_in: Field | None, b: Field, x_out: Field):
         self.ctx.check(self.ctx.lib.lfg_helm_smooth(self.h, omega, None if x_in is None else x_in.h,
                                                     b.h, x_out.h), "helm_smooth")
+
+    def residual_restrict(self, ig: "Intergrid", x: Field, b: Field, coarse_b: Field):
+        """coarse_b = restrict_mass_w3(b - A x) in one launch."""
+        self.ctx.check(self.ctx.lib.lfg_helm_residual_restrict(self.h, ig.h, x.h, b.h,
+                                                               coarse_b.h),
+                       "helm_residual_restrict")
+
+    def sweep_rhs(self, x: Field, b: Field, r: Field):
+        """r = b + H_off x (the right-hand side of a column sweep)."""
+        self.ctx.check(self.ctx.lib.lfg_helm_sweep_rhs(self.h, x.h, b.h, r.h), "helm_sweep_rhs")
 
     def coarsen(self, ig: Intergrid, coarse_mesh: Mesh, kind: int) -> "Helmholtz":
         h = C.c_void_p()

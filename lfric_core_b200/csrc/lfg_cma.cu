@@ -510,7 +510,38 @@ __device__ __align__(256) unsigned char g_noalloc_scratch[LFG_NOALLOC_SCRATCH_BY
 std::mutex g_noalloc_mu;
 std::vector<void*> g_noalloc_addr;  // per device ordinal, null until looked up
 
+// The array's device address on device `dev` (the current device), looked
+// up once.  The lookup and cudaFuncGetAttributes on both kernels make the
+// runtime load this library's device code on that device (lazy module
+// loading), which may allocate: lfg_ctx_create does it, so a caller that
+// made a context on the device never pays it inside lfg_tri_solve_noalloc.
+cudaError_t noalloc_lookup(int dev, void** out) {
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if ((int)g_noalloc_addr.size() <= dev) g_noalloc_addr.resize(dev + 1, nullptr);
+  if (!g_noalloc_addr[dev]) {
+    void* p = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    if (!p) return cudaErrorInvalidSymbol;
+    cudaFuncAttributes fa;
+    e = cudaFuncGetAttributes(&fa, (const void*)k_thomas_scratch<double, SRC_FIELDS>);
+    if (e == cudaSuccess)
+      e = cudaFuncGetAttributes(&fa, (const void*)k_thomas_scratch<float, SRC_FIELDS>);
+    if (e != cudaSuccess) return e;
+    g_noalloc_addr[dev] = p;
+  }
+  *out = g_noalloc_addr[dev];
+  return cudaSuccess;
+}
+
 }  // namespace
+
+namespace lfg {
+cudaError_t noalloc_prepare(int dev) {
+  void* p = nullptr;
+  return noalloc_lookup(dev, &p);
+}
+}  // namespace lfg
 
 extern "C" {
 
@@ -524,30 +555,32 @@ int lfg_tri_solve_noalloc(int kind, int ncol, int nlev, const void* x, const voi
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) return LFG_ERR_CUDA;
   void* scratch = nullptr;
-  {
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if ((int)g_noalloc_addr.size() <= dev) g_noalloc_addr.resize(dev + 1, nullptr);
-    if (!g_noalloc_addr[dev]) {
-      void* p = nullptr;
-      if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return LFG_ERR_CUDA;
-      g_noalloc_addr[dev] = p;
-    }
-    scratch = g_noalloc_addr[dev];
-  }
+  if (noalloc_lookup(dev, &scratch) != cudaSuccess) return LFG_ERR_CUDA;
   const int bs = 128, grid = (ncol + bs - 1) / bs;
   cudaStream_t st = (cudaStream_t)stream;
+  // launched through cudaLaunchKernel so that the status returned is this
+  // launch's own, and no error left by the caller's earlier work is cleared
+  cudaError_t e;
   if (kind == LFG_R_DOUBLE) {
     TriSrc<double> s{ncol, nlev, nullptr, (const double*)tri_0, (const double*)tri_plus,
                      (const double*)tri_minus, nullptr, 0};
-    k_thomas_scratch<double, SRC_FIELDS><<<grid, bs, 0, st>>>(s, (const double*)x, (double*)y,
-                                                               (double*)scratch);
+    const double* xd = (const double*)x;
+    double* yd = (double*)y;
+    double* wd = (double*)scratch;
+    void* args[] = {&s, &xd, &yd, &wd};
+    e = cudaLaunchKernel((const void*)k_thomas_scratch<double, SRC_FIELDS>, dim3(grid),
+                         dim3(bs), args, 0, st);
   } else {
     TriSrc<float> s{ncol, nlev, nullptr, (const float*)tri_0, (const float*)tri_plus,
                     (const float*)tri_minus, nullptr, 0};
-    k_thomas_scratch<float, SRC_FIELDS><<<grid, bs, 0, st>>>(s, (const float*)x, (float*)y,
-                                                              (float*)scratch);
+    const float* xf = (const float*)x;
+    float* yf = (float*)y;
+    float* wf = (float*)scratch;
+    void* args[] = {&s, &xf, &yf, &wf};
+    e = cudaLaunchKernel((const void*)k_thomas_scratch<float, SRC_FIELDS>, dim3(grid), dim3(bs),
+                         args, 0, st);
   }
-  return cudaGetLastError() == cudaSuccess ? LFG_OK : LFG_ERR_CUDA;
+  return e == cudaSuccess ? LFG_OK : LFG_ERR_CUDA;
 }
 
 // ------------------------------------------------------------- CMA objects

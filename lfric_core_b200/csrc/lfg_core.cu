@@ -490,13 +490,16 @@ void launch_ew(lfg_ctx c, const Op& op, size_t n, bool vec, const char* what, in
   after_launch(c, what, (uint64_t)words * n * sizeof(T));
 }
 
+// out: where the reduction's result goes (null: the slot's result word)
 template <class T, class Op>
 void launch_ewr(lfg_ctx c, const Op& op, size_t n, bool vec, int slot, const char* what,
-                int words) {
+                int words, double* out = nullptr) {
   const size_t work = vec ? n / kVec<T> + n % kVec<T> : n;
   // the reduction's partials live in kMaxRedBlocks slots per reduction
   const int g = std::min(occ_grid(c, (const void*)k_ewr<T, Op>, kThreads, work), kMaxRedBlocks);
-  k_ewr<T, Op><<<g, kThreads, 0, c->stream>>>(op, n, vec, c->red(slot));
+  Red r = c->red(slot);
+  if (out) r.result = out;
+  k_ewr<T, Op><<<g, kThreads, 0, c->stream>>>(op, n, vec, r);
   after_launch(c, what, (uint64_t)words * n * sizeof(T));
 }
 
@@ -583,6 +586,14 @@ void vec_dot(lfg_field x, lfg_field y, int slot) {
   DISPATCH_KIND(x->kind, T,
                 launch_ewr<T>(c, DotOp<T>{(const T*)x->d, (const T*)y->d}, x->n(),
                               all_aligned(x->d, y->d), slot, "dot", 2));
+}
+
+static void vec_dot_to(lfg_field x, lfg_field y, double* out) {
+  same_kind(x, y, "X_innerproduct_Y");
+  lfg_ctx c = x->ctx;
+  DISPATCH_KIND(x->kind, T,
+                launch_ewr<T>(c, DotOp<T>{(const T*)x->d, (const T*)y->d}, x->n(),
+                              all_aligned(x->d, y->d), 0, "dot", 2, out));
 }
 
 void vec_mgs_step(lfg_field v, lfg_field pv, lfg_field vj, lfg_field pvj, Sc alpha,
@@ -732,6 +743,9 @@ int lfg_ctx_create(int device, lfg_ctx* out) {
     LFG_CUDA(cudaMallocHost(&c->host_results, sizeof(double) * kRedSlots));
     c->dev_err = (unsigned*)dmalloc(sizeof(unsigned));
     LFG_CUDA(cudaMemset(c->dev_err, 0, sizeof(unsigned)));
+    // lfg_tri_solve_noalloc's set-up on this device, done here while
+    // memory can still be had
+    LFG_CUDA(noalloc_prepare(device));
   });
   if (st != LFG_OK) {
     fprintf(stderr, "lfg_ctx_create: %s\n", c->last_error.c_str());
@@ -760,6 +774,12 @@ int lfg_ctx_destroy(lfg_ctx c) {
 int lfg_ctx_set_stream(lfg_ctx c, void* stream) {
   if (!c) return LFG_ERR_ARG;
   c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+  return LFG_OK;
+}
+
+int lfg_ctx_test_tma_spin_limit(lfg_ctx c, long long spins) {
+  if (!c) return LFG_ERR_ARG;
+  c->tma_stage_spins = spins < 0 ? -1 : spins;
   return LFG_OK;
 }
 
@@ -928,6 +948,13 @@ int lfg_X_innerproduct_Y(lfg_field x, lfg_field y, double* result) {
 }
 int lfg_X_innerproduct_X(lfg_field x, double* result) {
   return lfg_X_innerproduct_Y(x, x, result);
+}
+int lfg_X_innerproduct_Y_device(lfg_field x, lfg_field y, void* device_result) {
+  if (!x || !y || !device_result) return LFG_ERR_ARG;
+  return guard(x->ctx, [&] {
+    LFG_REQUIRE(x->n() == y->n(), "X_innerproduct_Y: fields differ in size");
+    vec_dot_to(x, y, (double*)device_result);
+  });
 }
 
 }  // extern "C"

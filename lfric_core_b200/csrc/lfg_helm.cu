@@ -604,6 +604,18 @@ void launch_subst(lfg_ctx c, int ncol, int nl, const T* r, const T* sub, const T
   after_launch(c, "helm_subst", sizeof(T) * (XIN ? 6 : 5) * (uint64_t)ncol * nl);
 }
 
+// r = b + H_off x (k_helm_rhs)
+template <class T>
+void launch_rhs(lfg_helm op, const T* x, const T* b, T* r) {
+  lfg_ctx c = op->ctx;
+  const size_t work = (size_t)op->ncol * ((op->nl + KC - 1) / KC);
+  auto rk = op->hsym ? k_helm_rhs<T, true> : k_helm_rhs<T, false>;
+  rk<<<occ_grid(c, (const void*)rk, 256, work), 256, 0, c->stream>>>(args_of<T>(op), x, b, r);
+  // x, b and the couplings read, r written
+  after_launch(c, "helm_rhs",
+               (uint64_t)(sizeof(T) * (3 + coupling_words(op)) * (double)op->ncol * op->nl));
+}
+
 template <class T>
 void smooth_t(lfg_helm op, double omega, lfg_field x_in, lfg_field b, lfg_field x_out,
               void* rbuf) {
@@ -627,13 +639,7 @@ void smooth_t(lfg_helm op, double omega, lfg_field x_in, lfg_field b, lfg_field 
     return;
   }
   T* r = (T*)rbuf;
-  const size_t work = (size_t)op->ncol * ((op->nl + KC - 1) / KC);
-  auto rk = op->hsym ? k_helm_rhs<T, true> : k_helm_rhs<T, false>;
-  rk<<<occ_grid(c, (const void*)rk, 256, work), 256, 0, c->stream>>>(
-      args_of<T>(op), (const T*)x_in->d, (const T*)b->d, r);
-  // x, b and the couplings read, r written
-  after_launch(c, "helm_rhs",
-               (uint64_t)(sizeof(T) * (3 + coupling_words(op)) * (double)op->ncol * op->nl));
+  launch_rhs<T>(op, (const T*)x_in->d, (const T*)b->d, r);
   launch_subst<T, true>(c, op->ncol, op->nl, r, sub, inv, cp, (const T*)x_in->d, om,
                         (T*)x_out->d);
 }
@@ -974,6 +980,26 @@ int lfg_helm_apply(lfg_helm op, lfg_field y, lfg_field x) {
 int lfg_helm_smooth(lfg_helm op, double omega, lfg_field x_in, lfg_field b, lfg_field x_out) {
   if (!op) return LFG_ERR_ARG;
   return guard(op->ctx, [&] { helm_smooth(op, omega, x_in, b, x_out, nullptr); });
+}
+
+int lfg_helm_residual_restrict(lfg_helm op, lfg_intergrid ig, lfg_field x, lfg_field b,
+                               lfg_field coarse_b) {
+  if (!op || !ig || !x || !b || !coarse_b) return LFG_ERR_ARG;
+  return guard(op->ctx, [&] { helm_residual_restrict(op, ig, x, b, coarse_b); });
+}
+
+int lfg_helm_sweep_rhs(lfg_helm op, lfg_field x, lfg_field b, lfg_field r) {
+  if (!op) return LFG_ERR_ARG;
+  return guard(op->ctx, [&] {
+    check_field(op, x, "helm_sweep_rhs");
+    check_field(op, b, "helm_sweep_rhs");
+    check_field(op, r, "helm_sweep_rhs");
+    LFG_REQUIRE(r->d != x->d, "helm_sweep_rhs: r may not alias x");
+    if (op->kind == LFG_R_DOUBLE)
+      launch_rhs<double>(op, (const double*)x->d, (const double*)b->d, (double*)r->d);
+    else
+      launch_rhs<float>(op, (const float*)x->d, (const float*)b->d, (float*)r->d);
+  });
 }
 
 int lfg_helm_coarsen(lfg_helm fine, lfg_intergrid ig, lfg_mesh cmesh, int kind,

@@ -151,6 +151,9 @@ struct lfg_ctx_s {
   // device error word: kernels whose bounded waits ran out record a code
   // here (0 = none); read by check_device_error
   unsigned* dev_err = nullptr;
+  // polls of a TMA stage wait before the substitution kernels give up
+  // (< 0: their built-in limit); lfg_ctx_test_tma_spin_limit sets it
+  long long tma_stage_spins = -1;
 
   lfg::Red red(int slot) {
     return lfg::Red{red_partials + (size_t)slot * lfg::kMaxRedBlocks, red_counters + slot,
@@ -342,6 +345,10 @@ inline int occ_grid(lfg_ctx c, const void* kern, int threads, size_t work, size_
 
 // Throws LFG_ERR_STATE when a kernel recorded a device error (synchronises).
 void check_device_error(lfg_ctx c);
+
+// Looks up lfg_tri_solve_noalloc's device array on device `dev` (current)
+// and loads its kernels there (lfg_cma.cu); called by lfg_ctx_create.
+cudaError_t noalloc_prepare(int dev);
 
 // TMA-staged column substitution (lfg_subst_tma.cu), fine meshes; FP64
 // for columns of at most 80 levels.

@@ -25,7 +25,9 @@
 // store), so out-of-range columns and levels of the last tile read zeros.
 // Every wait is bounded: a barrier that does not complete within the spin
 // limit sets the context's device error word, the block waits (bounded) for
-// the loads it has issued and returns.
+// the loads it has issued and returns.  The stage-wait limit is a kernel
+// argument, so a test can make the waits run out
+// (lfg_ctx_test_tma_spin_limit); the drain keeps the built-in limit.
 #include <cuda.h>
 #include <cudaTypedefs.h>
 #include <cuda_runtime.h>
@@ -80,8 +82,9 @@ __device__ __forceinline__ bool mbar_try_wait(unsigned long long* bar, unsigned 
   return ok != 0;
 }
 
-__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity) {
-  for (long long i = 0; i < kSpinLimit; ++i)
+__device__ __forceinline__ bool mbar_wait_bounded(unsigned long long* bar, unsigned parity,
+                                                  long long spins = kSpinLimit) {
+  for (long long i = 0; i < spins; ++i)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }
@@ -98,7 +101,7 @@ __device__ __forceinline__ void tma_load_2d(void* dst, const CUtensorMap* map, i
 template <bool XIN>
 __global__ void __launch_bounds__(TC) k_subst_tma(const __grid_constant__ TmaMaps maps, int ncol,
                                                   int nl, float omega, float* __restrict__ xout,
-                                                  unsigned* err) {
+                                                  unsigned* err, long long stage_spins) {
   extern __shared__ __align__(128) unsigned char smem[];
   float* stage = reinterpret_cast<float*>(smem);                       // [NST][NARR][KCH][TC]
   float* sd = stage + NST * NARR * KCH * TC;                           // [nl][TC]
@@ -145,7 +148,7 @@ __global__ void __launch_bounds__(TC) k_subst_tma(const __grid_constant__ TmaMap
   for (; j < njobs; ++j) {
     const int s = j % NST;
     const unsigned parity = (unsigned)((j / NST) & 1);
-    if (!mbar_wait_bounded(&full[s], parity)) {
+    if (!mbar_wait_bounded(&full[s], parity, stage_spins)) {
       atomicCAS(err, 0u, kErrTmaWait);
       s_abort = 1;
     }
@@ -208,7 +211,7 @@ __host__ __device__ constexpr int tile_cols() { return 512 / (int)sizeof(T); }
 template <class T, bool XIN, int NCH>
 __global__ void __launch_bounds__(tile_cols<T>(), 3)
     k_subst_tma_reg(const __grid_constant__ TmaMaps maps, int ncol, int nl, T omega,
-                    T* __restrict__ xout, unsigned* err) {
+                    T* __restrict__ xout, unsigned* err, long long stage_spins) {
   constexpr int TCT = tile_cols<T>();
   extern __shared__ __align__(128) unsigned char smem[];
   T* stage = reinterpret_cast<T*>(smem);  // [NST][NARR][KCH][TCT]
@@ -247,7 +250,7 @@ __global__ void __launch_bounds__(tile_cols<T>(), 3)
   };
   // wait for job j's stage; false (for the whole block) when a wait ran out
   auto acquire = [&](int j) {
-    if (!mbar_wait_bounded(&full[j % NST], (unsigned)((j / NST) & 1))) {
+    if (!mbar_wait_bounded(&full[j % NST], (unsigned)((j / NST) & 1), stage_spins)) {
       atomicCAS(err, 0u, kErrTmaWait);
       s_abort = 1;
     }
@@ -341,6 +344,13 @@ CUtensorMap make_map(const T* base, int ncol, int nl) {
   return m;
 }
 
+// Stage-wait limit of a launch: the context's test setting, else the
+// built-in one.  The drain after a wait ran out always uses the built-in
+// limit, so every load a block issued has landed before it returns.
+long long stage_spins(lfg_ctx c) {
+  return c->tma_stage_spins >= 0 ? c->tma_stage_spins : kSpinLimit;
+}
+
 size_t smem_bytes(int nl) {
   return sizeof(float) * ((size_t)NST * NARR * KCH * TC + (size_t)nl * TC);
 }
@@ -393,7 +403,8 @@ void launch_reg(lfg_ctx c, const TmaMaps& maps, int ncol, int nl, bool xin, T om
   T om = omega;
   T* xo = xout;
   unsigned* err = c->dev_err;
-  void* args[] = {&m, &nc, &nlv, &om, &xo, &err};
+  long long spins = stage_spins(c);
+  void* args[] = {&m, &nc, &nlv, &om, &xo, &err, &spins};
   LFG_CUDA(cudaLaunchKernel(kern, dim3(grid), dim3(TCT), args, smem, c->stream));
   // r, inv, sub, c' read and x written, x_in read when given
   after_launch(c, "helm_subst_tma", sizeof(T) * (uint64_t)ncol * nl * (xin ? 6 : 5));
@@ -430,9 +441,11 @@ void subst_tma(lfg_ctx c, int ncol, int nl, const float* r, const float* sub, co
   const int ntile = (ncol + TC - 1) / TC;
   const int grid = std::max(1, std::min(ntile, c->num_sms * std::max(per_sm, 1)));
   if (xin)
-    k_subst_tma<true><<<grid, TC, smem, c->stream>>>(maps, ncol, nl, omega, xout, c->dev_err);
+    k_subst_tma<true><<<grid, TC, smem, c->stream>>>(maps, ncol, nl, omega, xout, c->dev_err,
+                                                     stage_spins(c));
   else
-    k_subst_tma<false><<<grid, TC, smem, c->stream>>>(maps, ncol, nl, omega, xout, c->dev_err);
+    k_subst_tma<false><<<grid, TC, smem, c->stream>>>(maps, ncol, nl, omega, xout, c->dev_err,
+                                                      stage_spins(c));
   after_launch(c, "helm_subst_tma", sizeof(float) * (uint64_t)ncol * nl * (xin ? 6 : 5));
 }
 

@@ -3,10 +3,20 @@
 TEST INFRASTRUCTURE ONLY: imported by tests/, by the smoke check and by the
 CPU-baseline leg of bench.py, never by the product package.  It builds the
 oracle from source on first use if the shared library is missing.
+
+Two builds of the same C sources:
+* lib() -- the strict build the tests check against (-O2, no FMA
+  contraction);
+* lib(native=True) -- the CPU baseline the benchmark times (-O3
+  -march=native -fopenmp), built on the host that runs it under a name keyed
+  by the host's CPU model and instruction-set flags, so a library built on
+  one machine is never loaded on another.
 """
 from __future__ import annotations
 
 import ctypes as C
+import hashlib
+import platform
 import subprocess
 from pathlib import Path
 
@@ -28,22 +38,49 @@ def build(force: bool = False) -> Path:
     return LIB_PATH
 
 
-_lib = None
+def _cpu_tag() -> str:
+    """Short hash of the CPU model, its instruction-set flags and the
+    compiler: what -march=native code depends on."""
+    info = platform.processor() or ""
+    try:
+        txt = Path("/proc/cpuinfo").read_text()
+        keep = [ln for ln in txt.splitlines() if ln.startswith(("model name", "flags"))]
+        info += "\n".join(sorted(set(keep)))
+    except OSError:
+        pass
+    try:
+        info += subprocess.run(["gcc", "--version"], capture_output=True, text=True).stdout
+    except OSError:
+        pass
+    return hashlib.sha1(info.encode()).hexdigest()[:12]
 
 
-def lib() -> C.CDLL:
-    global _lib
-    if _lib is None:
-        build()
-        _lib = C.CDLL(str(LIB_PATH))
-        _lib.ora_dot_d.restype = C.c_double
-        _lib.ora_norm_d.restype = C.c_double
-        _lib.ora_dot_f.restype = C.c_double
-        _lib.ora_norm_f.restype = C.c_double
-        _lib.ora_mg_work_size_d.restype = C.c_long
-        _lib.ora_mg_work_size_f.restype = C.c_long
-        _setup_signatures(_lib)
-    return _lib
+def build_native(force: bool = False) -> Path:
+    """The -O3 -march=native -fopenmp build for this host's CPU."""
+    out = HERE / "_native" / f"liblfg_oracle_{_cpu_tag()}.so"
+    srcs = [HERE / f for f in ("ora_kernels.c", "ora_solvers.c", "ora_real.inc", "lfg_oracle.h")]
+    if force or not out.exists() or any(s.stat().st_mtime > out.stat().st_mtime for s in srcs):
+        subprocess.run(["make", "-s", "-C", str(HERE), "native", f"NATIVE_OUT={out}"],
+                       check=True)
+    return out
+
+
+_libs = {}
+
+
+def lib(native: bool = False) -> C.CDLL:
+    if native not in _libs:
+        path = build_native() if native else build()
+        L = C.CDLL(str(path))
+        L.ora_dot_d.restype = C.c_double
+        L.ora_norm_d.restype = C.c_double
+        L.ora_dot_f.restype = C.c_double
+        L.ora_norm_f.restype = C.c_double
+        L.ora_mg_work_size_d.restype = C.c_long
+        L.ora_mg_work_size_f.restype = C.c_long
+        _setup_signatures(L)
+        _libs[native] = L
+    return _libs[native]
 
 
 def ptr(a: np.ndarray):
@@ -86,8 +123,11 @@ class MixedInfo(C.Structure):
 class Helmholtz:
     """Oracle view of a HelmholtzProblem: operators of every MG level."""
 
-    def __init__(self, prob, dtype=np.float64):
-        L = lib()
+    def __init__(self, prob, dtype=np.float64, native: bool = False):
+        """native: run on the -O3 -march=native build (CPU timing) instead
+        of the strict build the tests check against."""
+        L = lib(native)
+        self.L = L
         self.prob = prob
         self.nl = prob.nlayers
         self.keep = []
@@ -126,7 +166,7 @@ class Helmholtz:
             s.op[l] = self.op(l, dtype)
         for l in range(nlev - 1):
             s.child[l] = self.child[l].ctypes.data
-        L = lib()
+        L = self.L
         sfx = "d" if dtype == np.float64 else "f"
         nwork = getattr(L, f"ora_mg_work_size_{sfx}")(C.byref(s))
         work = np.zeros(nwork, dtype=dtype)
@@ -138,7 +178,7 @@ class Helmholtz:
         dtype = x.dtype
         y = np.zeros_like(x)
         op = self.op(level, dtype)
-        fn = lib().ora_helm_apply_d if dtype == np.float64 else lib().ora_helm_apply_f
+        fn = self.L.ora_helm_apply_d if dtype == np.float64 else self.L.ora_helm_apply_f
         fn(C.byref(op), ptr(x), ptr(y))
         return y
 
@@ -147,7 +187,7 @@ class Helmholtz:
         op = self.op(level, dtype)
         out = np.zeros_like(b)
         work = np.zeros(b.size + 2 * self.nl, dtype=dtype)
-        fn = lib().ora_helm_smooth_d if dtype == np.float64 else lib().ora_helm_smooth_f
+        fn = self.L.ora_helm_smooth_d if dtype == np.float64 else self.L.ora_helm_smooth_f
         fn(C.byref(op), C.c_double(omega), None if x_in is None else ptr(x_in), ptr(b),
            ptr(out), ptr(work))
         return out
@@ -155,12 +195,12 @@ class Helmholtz:
     def mg_apply(self, b: np.ndarray, **kw) -> np.ndarray:
         s = self.mg(b.dtype, **kw)
         x = np.zeros_like(b)
-        fn = lib().ora_mg_apply_d if b.dtype == np.float64 else lib().ora_mg_apply_f
+        fn = self.L.ora_mg_apply_d if b.dtype == np.float64 else self.L.ora_mg_apply_f
         fn(C.byref(s), ptr(b), ptr(x))
         return x
 
     def gcr_mg_solve(self, b, gcrk=10, r_tol=1e-8, max_iter=20, dtype=np.float64, **mgkw):
-        L = lib()
+        L = self.L
         sfx = "d" if dtype == np.float64 else "f"
         b = np.ascontiguousarray(b, dtype=dtype)
         n = b.size
@@ -178,7 +218,7 @@ class Helmholtz:
 
     def mixed_solve(self, b, tol=1e-8, max_outer=10, gcrk=10, inner_tol=1e-4,
                     inner_max_iter=2, **mgkw):
-        L = lib()
+        L = self.L
         b = np.ascontiguousarray(b, dtype=np.float64)
         op = self.op(0, np.float64)
         mg = self.mg(np.float32, **mgkw)
@@ -192,7 +232,7 @@ class Helmholtz:
 
     def mixed_cg_col_solve(self, b, tol=1e-8, max_outer=10, inner_tol=1e-5, max_inner=200):
         """Refinement with an inner FP32 CG preconditioned by T'^{-1}."""
-        L = lib()
+        L = self.L
         b = np.ascontiguousarray(b, dtype=np.float64)
         x = np.zeros_like(b)
         info = MixedInfo()

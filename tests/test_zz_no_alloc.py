@@ -54,6 +54,48 @@ def test_noalloc_matches_tri_solve_twice(ctx, kind, tol, ncol, nlev):
         ctx.set_stream(None)
 
 
+def _check_on_null_stream(ctx, rng, ncol, nlev, kind, tol):
+    """Two calls in a row on the legacy default stream (stream NULL),
+    against lfg_tri_solve on the context's stream."""
+    import torch
+    for call in range(2):
+        x, t0, tp, tm = _system(rng, ncol, nlev)
+        F = [field_from(ctx, a, ncol, nlev, kind=kind) for a in (x, t0, tp, tm)]
+        ref = Field(ctx, kind, ncol, nlev)
+        api.tri_solve(ref, *F)
+        out = Field(ctx, kind, ncol, nlev)
+        out.set_scalar(-3.0)
+        ctx.synchronize()              # inputs written on the context's own stream
+        st = ctx.lib.lfg_tri_solve_noalloc(
+            kind, ncol, nlev, *[C.c_void_p(f.device_ptr()) for f in F],
+            C.c_void_p(out.device_ptr()), None)
+        assert st == api.OK, f"call {call}: status {st}"
+        torch.cuda.synchronize()       # the legacy default stream's work is done
+        a, b = out.export(np.float64), ref.export(np.float64)
+        assert np.linalg.norm(a - b) / np.linalg.norm(b) < tol, f"call {call}"
+
+
+@pytest.mark.parametrize("kind,tol", [(R_DOUBLE, 1e-12), (R_SINGLE, 1e-5)])
+def test_noalloc_on_the_legacy_default_stream(ctx, kind, tol):
+    _check_on_null_stream(ctx, np.random.default_rng(77), 2000, 64, kind, tol)
+
+
+def test_noalloc_on_a_second_device():
+    """Each device has its own copy of the array: one call on every device
+    (the first two), each through a context made on that device."""
+    import torch
+    if torch.cuda.device_count() < 2:
+        pytest.skip("one CUDA device")
+    for dev in (0, 1):
+        torch.cuda.set_device(dev)
+        c = api.Context(dev)
+        try:
+            _check_on_null_stream(c, np.random.default_rng(5 + dev), 1500, 40, R_DOUBLE, 1e-12)
+        finally:
+            c.close()
+    torch.cuda.set_device(0)
+
+
 def test_noalloc_rejects_sizes_beyond_its_array(ctx):
     kind = R_DOUBLE
     nlev = 70
