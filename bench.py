@@ -305,6 +305,232 @@ def measure_batched(ctx, stream, steps: int, warmup: int, n_rhs: int = 64, n_une
     }
 
 
+def _cpu_time(fn, threads: int, lib, reps: int = 1) -> float:
+    """Seconds per call of fn() on `threads` OpenMP threads (mean of reps)."""
+    lib.ora_threads(threads)
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        fn()
+    return (time.perf_counter() - t0) / reps
+
+
+def measure_configs(ctx, stream, steps: int, peak: float, cpu: bool) -> dict:
+    """The other workloads, each GPU figure beside the oracle's CPU time
+    (the -O3 -march=native -fopenmp build, all host threads and one thread):
+    config1_cg_w0, config2_line_solve, config4_adjoint and the CPU side of
+    the batched workload."""
+    import torch
+    from lfric_core_b200 import api
+    from lfric_core_b200.api import R_DOUBLE, R_SINGLE, Field, field_from
+    from lfric_core_b200.problems import w0_problem, helmholtz_problem, batch_workload
+    threads = host_threads()
+    out = {}
+
+    def gpu_ms(fn, n):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    # ---- config 1: C24 x 20 W0 mass + stiffness, Jacobi-CG FP64 to 1e-8
+    p = w0_problem(24, 20, seed=1, top=20e3)
+    A = p.matrix()
+    nent, nlev = p.nvert, p.nlayers + 1
+    lma = api.LocalOperator(ctx, R_DOUBLE, p.ncell, p.nlayers, A, p.map, nent, nlev)
+    diag = Field(ctx, R_DOUBLE, nent, nlev)
+    lma.diagonal(diag)
+    sol = api.IterativeSolver(api.LinearOperator.from_lma(lma), api.Preconditioner.diagonal(diag),
+                              diag, "cg", r_tol=1e-8, max_iter=2000)
+    B, X = field_from(ctx, p.rhs, nent, nlev), Field(ctx, R_DOUBLE, nent, nlev)
+    res = {}
+
+    def cg_once():
+        X.set_scalar(0.0)
+        res["r"] = sol.apply(X, B)
+
+    for _ in range(3):
+        cg_once()
+    ms = gpu_ms(cg_once, max(5, steps))
+    c1 = {"workload": "C24x20 W0 mass+stiffness (kappa 1), Jacobi-preconditioned CG FP64 to 1e-8",
+          "ndof": p.ndof, "iterations": res["r"].iterations, "ms_per_solve": ms,
+          "solves_per_s": 1e3 / ms,
+          "note": "each solve reads the monitored residual norm on the host every iteration "
+                  "(the reference's monitor_convergence), so it is launch- and "
+                  "synchronisation-bound at this size"}
+    if cpu:
+        from oracle.oracle import W0 as OraW0
+        o = OraW0(p, A, native=True)
+        o.cg_solve(p.rhs)
+        t_all = _cpu_time(lambda: o.cg_solve(p.rhs), threads, o.L, 5)
+        t_one = _cpu_time(lambda: o.cg_solve(p.rhs), 1, o.L, 5)
+        c1["cpu"] = {"all_threads": {"solves_per_s": 1 / t_all, "cores": threads},
+                     "one_thread": {"solves_per_s": 1 / t_one, "cores": 1},
+                     "kind": "port", "sample": "5 solves each; the LMA apply (GH_INC scatter) "
+                                               "runs serially in the restatement"}
+    out["config1_cg_w0"] = c1
+    del sol, lma, diag, B, X
+
+    # ---- config 2: C96 x 70 CMA tridiagonal line solve, FP64 and FP32 + FP64 refinement
+    p = helmholtz_problem(96, NLAYERS, seed=2, mg_levels=1)
+    ncol, nl = p.ncol, p.nlayers
+    n = ncol * nl
+    ind = np.arange(1, nl + 1, dtype=np.int32)
+    A64 = api.ColumnwiseOperator(ctx, R_DOUBLE, ncol, nl, nl, 3, 1, 1, 1, 1, ind, ind, p.cm)
+    A32 = api.ColumnwiseOperator(ctx, R_SINGLE, ncol, nl, nl, 3, 1, 1, 1, 1, ind, ind, p.cm)
+    B = field_from(ctx, p.rhs, ncol, nl)
+    X, X2, R = (Field(ctx, R_DOUBLE, ncol, nl) for _ in range(3))
+    R32, E32 = Field(ctx, R_SINGLE, ncol, nl), Field(ctx, R_SINGLE, ncol, nl)
+    nref = 3
+
+    def refine():
+        # FP32 Thomas on the residual, FP64 update and residual (nref corrections)
+        X2.set_scalar(0.0)
+        R.copy(B)
+        for _ in range(nref):
+            R32.copy(R)
+            A32.apply_inverse(E32, R32)
+            X2.axpy(1.0, E32)
+            R.copy(B)
+            R.scale(-1.0)
+            A64.apply(R, X2)
+            R.scale(-1.0)
+
+    for _ in range(3):
+        A64.apply_inverse(X, B)
+        refine()
+    ms64 = gpu_ms(lambda: A64.apply_inverse(X, B), 20)
+    B32 = Field(ctx, R_SINGLE, ncol, nl)
+    B32.copy(B)
+    ms32 = gpu_ms(lambda: A32.apply_inverse(E32, B32), 20)
+    msref = gpu_ms(refine, 10)
+    x64, xr = X.export(), X2.export()
+    c2 = {"workload": "C96x70 W3 tridiagonal (diagonal ratio U(1.5,3)), seeded rhs",
+          "ndof": n,
+          "fp64_solve": {"us": ms64 * 1e3, "algorithmic_bytes": 5 * n * 8,
+                         "GB/s": 5 * n * 8 / (ms64 * 1e-3) / 1e9,
+                         "frac": 5 * n * 8 / (ms64 * 1e-3) / 1e9 / peak},
+          "fp32_solve": {"us": ms32 * 1e3, "algorithmic_bytes": 5 * n * 4,
+                         "GB/s": 5 * n * 4 / (ms32 * 1e-3) / 1e9,
+                         "frac": 5 * n * 4 / (ms32 * 1e-3) / 1e9 / peak},
+          "fp32_plus_fp64_refinement": {
+              "us": msref * 1e3, "corrections": nref,
+              "rel_diff_to_fp64": float(np.linalg.norm(xr - x64) / np.linalg.norm(x64))}}
+    if cpu:
+        from oracle.oracle import lib as olib, ptr
+        L = olib(True)
+        cmc = np.ascontiguousarray(p.cm)
+        cm32 = cmc.astype(np.float32)
+        b64 = np.ascontiguousarray(p.rhs)
+        b32 = b64.astype(np.float32)
+        y64, y32 = np.zeros(n), np.zeros(n, dtype=np.float32)
+        f64 = lambda: L.ora_cma_appinv_mesh_d(ncol, nl, ptr(cmc), ptr(b64), ptr(y64))
+        f32 = lambda: L.ora_cma_appinv_mesh_f(ncol, nl, ptr(cm32), ptr(b32), ptr(y32))
+        f64()
+        c2["cpu"] = {"fp64_solve": {"all_threads_us": 1e6 * _cpu_time(f64, threads, L, 10),
+                                    "one_thread_us": 1e6 * _cpu_time(f64, 1, L, 5)},
+                     "fp32_solve": {"all_threads_us": 1e6 * _cpu_time(f32, threads, L, 10),
+                                    "one_thread_us": 1e6 * _cpu_time(f32, 1, L, 5)},
+                     "cores": threads, "kind": "port",
+                     "sample": "columnwise_op_appinv over all 55296 columns, 10 (all threads) "
+                               "and 5 (one thread) calls"}
+    out["config2_line_solve"] = c2
+    del A64, A32, B, X, X2, R, R32, E32, B32
+
+    # ---- config 4: gradients of J = 0.5 ||u - u_obs||^2 through the C48 x 30
+    # W0 diffusion solve (log-normal kappa, sigma 0.5), FP64, solves to 1e-13
+    from lfric_core_b200.autograd import DiffusionSolve, W0Diffusion
+    p = w0_problem(48, 30, seed=4, top=30e3, kappa_sigma=0.5, kappa_scale=1e6)
+    nl = p.nlayers
+    sysm = W0Diffusion(ctx, p, r_tol=1e-13, max_iter=5000)
+    dev = torch.device("cuda")
+    lm = lambda a, nc_, nv_: torch.tensor(np.ascontiguousarray(
+        np.asarray(a).reshape(nc_, nv_).T), dtype=torch.float64, device=dev).reshape(-1)
+    f = lm(p.rhs, p.nvert, nl + 1)
+    kap = lm(p.kappa.ravel(), p.ncell, nl)
+    rng = np.random.default_rng(7)
+    with torch.no_grad():
+        u_nom = DiffusionSolve.apply(f, kap, sysm)
+        uobs = u_nom + 0.1 * u_nom.std() * torch.tensor(rng.standard_normal(p.ndof),
+                                                        dtype=torch.float64, device=dev)
+
+    def forward():
+        with torch.no_grad():
+            return DiffusionSolve.apply(f, kap, sysm)
+
+    def gradient():
+        ff, kk = f.clone().requires_grad_(True), kap.clone().requires_grad_(True)
+        u = DiffusionSolve.apply(ff, kk, sysm)
+        (0.5 * torch.sum((u - uobs) ** 2)).backward()
+        return ff.grad, kk.grad
+
+    def fd16():
+        h = 1e-6
+        for _ in range(16):
+            with torch.no_grad():
+                DiffusionSolve.apply(f + h * f, kap, sysm)
+                DiffusionSolve.apply(f - h * f, kap, sysm)
+
+    def host_ms(fn, n):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(n):
+            fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) * 1e3 / n
+
+    for _ in range(2):
+        forward()
+        gradient()
+    fwd_ms = host_ms(forward, 3)
+    grad_ms = host_ms(gradient, 3)
+    fd_ms = host_ms(fd16, 1)
+    c4 = {"workload": "C48x30 W0 diffusion, log-normal kappa (sigma 0.5), CG to 1e-13, "
+                      "gradient of J w.r.t. rhs and kappa",
+          "ndof": p.ndof, "forward_solve_ms": fwd_ms,
+          "adjoint_gradient_ms": grad_ms, "fd_16_directions_ms": fd_ms,
+          "gradient_over_forward": grad_ms / fwd_ms, "fd_over_gradient": fd_ms / grad_ms,
+          "note": "timed on the host clock around device-synchronised calls (the solves read "
+                  "their residual norms on the host)"}
+    if cpu:
+        from oracle.oracle import W0 as OraW0
+        o = OraW0(p, native=True)
+        t1 = _cpu_time(lambda: o.cg_solve(p.rhs, r_tol=1e-13, max_iter=5000), threads, o.L, 1)
+        c4["cpu"] = {"forward_solve_s": t1, "fd_16_directions_s": 32 * t1,
+                     "cores": threads, "kind": "port",
+                     "sample": "one Jacobi-CG forward solve timed; the central-difference "
+                               "gradient over 16 directions costs 32 such solves"}
+    out["config4_adjoint"] = c4
+    del sysm
+    ctx.set_stream(stream.cuda_stream)        # W0Diffusion ran the library on its own stream
+
+    # ---- config 5, CPU side: the oracle's refinement + CG + column solve on a sample
+    if cpu:
+        from oracle.oracle import Helmholtz as OraHelm
+        wl = batch_workload()
+        pick = [0, 1, 2, 3] + [64 + j for j in range(4)]
+        ndof, t = 0, 0.0
+        L = None
+        for i in pick:
+            op = wl.operators[wl.problem_op[i]]
+            o = OraHelm(op, native=True)
+            L = o.L
+            L.ora_threads(threads)
+            t0 = time.perf_counter()
+            _, st, _ = o.mixed_cg_col_solve(wl.rhs[i])
+            t += time.perf_counter() - t0
+            ndof += op.ncol * op.nlayers
+        out["config5_batched_cpu"] = {
+            "problems": len(pick), "ndof": ndof, "seconds": t, "Mdof_per_s": ndof / t / 1e6,
+            "problems_per_s": len(pick) / t, "cores": threads, "kind": "port",
+            "sample": "problems 0-3 (C48x30, shared operator) and 64-67 (uneven) of the "
+                      "batched workload, one after another, each on all threads"}
+    return out
+
+
 def measure_kernels(ctx, stream, peak: float) -> list:
     """Every hot-path kernel timed alone (CUDA events on the library's
     stream, 3 warm-up + 20 timed launches, inputs larger than L2 where the
@@ -567,6 +793,12 @@ def main():
     batched = measure_batched(ctx, stream, max(1, args.steps), max(1, args.warmup), world=world)
     torch.cuda.nvtx.range_pop()
 
+    # ---- the other workloads (configs 1, 2 and 4; the CPU side of the batched one)
+    torch.cuda.nvtx.range_push("configs")
+    configs = measure_configs(ctx, stream, args.steps, measured_hbm_peak()[0],
+                              cpu=(rank == 0 and world == 1))
+    torch.cuda.nvtx.range_pop()
+
     # ---- CPU baseline (rank 0, N=1 only): the oracle on the same workload
     cpu = None
     if rank == 0 and world == 1:
@@ -619,7 +851,9 @@ def main():
                                "ms": sweep_ms, "algorithmic_bytes": sweep_bytes,
                                "GB/s": sweep_bytes / (sweep_ms * 1e-3) / 1e9,
                                "frac": sweep_bytes / (sweep_ms * 1e-3) / 1e9 / peak},
-            "batched": batched,
+            "batched": dict(batched, problems_Mdof_per_s=batched["ndof"] /
+                            (batched["ms_per_batch"] * 1e-3) / 1e6),
+            **configs,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
         }

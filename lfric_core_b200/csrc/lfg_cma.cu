@@ -18,6 +18,7 @@
 #include "lfg_internal.cuh"
 
 #include <algorithm>
+#include <cmath>
 #include <mutex>
 
 using namespace lfg;
@@ -386,6 +387,31 @@ __global__ void k_cma_app(const T* __restrict__ bands, const int* __restrict__ i
   lhs[o] = acc;
 }
 
+// The same with V adjacent columns per thread (16-byte loads and stores of
+// the bands, x and lhs), for fields whose rows start on 16-byte boundaries;
+// the same operations in the same order as k_cma_app.
+template <class T, int V>
+__global__ void k_cma_app_v(const T* __restrict__ bands, const int* __restrict__ ind_to,
+                            const int* __restrict__ ind_from, const int* __restrict__ jminus,
+                            const int* __restrict__ jplus, int ncol, int nrow, int ncolumn,
+                            const T* __restrict__ x, T* __restrict__ lhs) {
+  const int c = (blockIdx.x * blockDim.x + threadIdx.x) * V;
+  const int i = blockIdx.y;
+  if (c >= ncol) return;
+  const size_t N = ncol, plane = (size_t)nrow * N;
+  const int jm = jminus[i];
+  const int jlo = max(0, jm), jhi = min(ncolumn - 1, jplus[i]);
+  const size_t o = (size_t)ind_to[i] * N + c;
+  Vec<T, V> acc = vld<false, T, V>(lhs + o);
+  for (int j = jlo; j <= jhi; ++j) {
+    const Vec<T, V> a = vld<true, T, V>(bands + (size_t)(j - jm) * plane + (size_t)i * N + c);
+    const Vec<T, V> xv = vld<false, T, V>(x + (size_t)ind_from[j] * N + c);
+#pragma unroll
+    for (int v = 0; v < V; ++v) acc.e[v] = acc.e[v] + a.e[v] * xv.e[v];
+  }
+  vst<T, V>(lhs + o, acc);
+}
+
 // lhs(ind_from(j)) += sum over rows i whose band reaches column j of
 // band(j - j_minus(i), i) x(ind_to(i)): the transpose of k_cma_app.  The
 // rows reaching each column are listed per column (CSR, rows ascending).
@@ -625,6 +651,8 @@ int lfg_cma_create(lfg_ctx c, int kind, int ncol, int nrow, int ncolumn, int bw,
     m->gp = gamma_p;
     m->max_ind_to = max_to;
     m->max_ind_from = max_from;
+    m->ind_identity = true;
+    for (int i = 0; i < nrow; ++i) m->ind_identity &= ind_to[i] == i + 1;
     const size_t n = (size_t)bw * nrow * ncol;
     std::vector<double> dev(n);
     for (int col = 0; col < ncol; ++col)
@@ -688,12 +716,24 @@ int lfg_cma_apply(lfg_cma m, lfg_field lhs, lfg_field x) {
                     lhs->nlev >= m->max_ind_to && x->nlev >= m->max_ind_from &&
                     lhs->kind == m->kind && x->kind == m->kind,
                 "cma_apply: fields do not match the operator");
-    dim3 grid((m->ncol + 127) / 128, m->nrow);
+    // 16-byte vectors of columns when every row starts on a 16-byte boundary
+    const int V = 16 / m->kind;
+    const bool vec = m->ncol % V == 0 && reinterpret_cast<uintptr_t>(x->d) % 16 == 0 &&
+                     reinterpret_cast<uintptr_t>(lhs->d) % 16 == 0;
     dispatch(m->kind, [&](auto tag) {
       using T = decltype(tag);
-      k_cma_app<T><<<grid, 128, 0, c->stream>>>((const T*)m->bands, m->ind_to, m->ind_from,
-                                                m->jminus, m->jplus, m->ncol, m->nrow,
-                                                m->ncolumn, (const T*)x->d, (T*)lhs->d);
+      if (vec) {
+        constexpr int VT = 16 / sizeof(T);
+        dim3 grid((m->ncol / VT + 127) / 128, m->nrow);
+        k_cma_app_v<T, VT><<<grid, 128, 0, c->stream>>>(
+            (const T*)m->bands, m->ind_to, m->ind_from, m->jminus, m->jplus, m->ncol, m->nrow,
+            m->ncolumn, (const T*)x->d, (T*)lhs->d);
+      } else {
+        dim3 grid((m->ncol + 127) / 128, m->nrow);
+        k_cma_app<T><<<grid, 128, 0, c->stream>>>((const T*)m->bands, m->ind_to, m->ind_from,
+                                                  m->jminus, m->jplus, m->ncol, m->nrow,
+                                                  m->ncolumn, (const T*)x->d, (T*)lhs->d);
+      }
     });
     after_launch(c, "cma_app", (uint64_t)m->kind * m->ncol * ((uint64_t)(m->bw + 2) * m->nrow + m->ncolumn));
   });
@@ -750,6 +790,23 @@ int lfg_cma_apply_inverse(lfg_cma m, lfg_field lhs, lfg_field x) {
       });
       after_launch(c, "cma_factor", (uint64_t)m->kind * 5 * m->ncol * m->nrow);
       m->fvalid = true;
+    }
+    // Fields of exactly nrow levels with the identity row map: the
+    // TMA-staged column substitution of the Helmholtz smoother, which does
+    // the same arithmetic on the same factors (x_out = 1 * z)
+    if (m->ind_identity && lhs->nlev == m->nrow && x->nlev == m->nrow) {
+      const void* ptrs[5] = {x->d, m->bands, m->finv, m->fcp, nullptr};
+      if (subst_tma_applicable(c, m->ncol, m->nrow, ptrs, 5, m->kind)) {
+        if (m->kind == LFG_R_DOUBLE)
+          subst_tma(c, m->ncol, m->nrow, (const double*)x->d, (const double*)m->bands,
+                    (const double*)m->finv, (const double*)m->fcp, nullptr, 1.0,
+                    (double*)lhs->d);
+        else
+          subst_tma(c, m->ncol, m->nrow, (const float*)x->d, (const float*)m->bands,
+                    (const float*)m->finv, (const float*)m->fcp, nullptr, 1.0f,
+                    (float*)lhs->d);
+        return;
+      }
     }
     // FP64: segmented form; FP32 columns (half the bytes per row) measured
     // faster one thread per column
@@ -842,11 +899,46 @@ int lfg_intergrid_create(lfg_ctx c, int ncoarse, int nfine, int nx, int ny,
     g->nx = nx;
     g->ny = ny;
     g->h_child.assign(cell_map, cell_map + (size_t)nq * ncoarse);
+    // 2x2 maps between structured cubed-sphere meshes: the same child
+    // placement in every coarse cell of a panel
+    std::vector<int> cedge;
+    if (nx == 2 && ny == 2) {
+      const long nc = std::lround(std::sqrt((double)ncoarse / 6.0)), nf = 2 * nc;
+      bool ok = nc >= 3 && 6 * nc * nc == ncoarse && 6 * nf * nf == nfine && nf < (1 << 14);
+      unsigned long long code = 0;
+      for (long P = 0; P < 6 && ok; ++P)
+        for (int q = 0; q < 4 && ok; ++q) {
+          int pos = -1;
+          for (long J = 0; J < nc && ok; ++J)
+            for (long I = 0; I < nc && ok; ++I) {
+              const long C = P * nc * nc + J * nc + I;
+              const long d = child[(size_t)q * ncoarse + C] - (P * nf * nf + 2 * J * nf + 2 * I);
+              const int dp = d == 0 ? 0 : d == 1 ? 1 : d == nf ? 2 : d == nf + 1 ? 3 : -1;
+              if (dp < 0 || (pos >= 0 && dp != pos)) ok = false;
+              pos = dp;
+            }
+          code |= (unsigned long long)pos << (8 * P + 2 * q);
+        }
+      if (ok) {
+        g->pnc = (int)nc;
+        g->qpos = code;
+        for (long P = 0; P < 6; ++P)
+          for (long J = 0; J < nc; ++J)
+            for (long I = 0; I < nc; ++I)
+              if (I == 0 || J == 0 || I == nc - 1 || J == nc - 1)
+                cedge.push_back((int)(P * nc * nc + J * nc + I));
+      }
+    }
     try {
       g->child = (int*)dmalloc(child.size() * sizeof(int));
       g->parent = (int*)dmalloc(parent.size() * sizeof(int));
       upload(g->child, child.data(), child.size() * sizeof(int));
       upload(g->parent, parent.data(), parent.size() * sizeof(int));
+      if (!cedge.empty()) {
+        g->cedge = (int*)dmalloc(cedge.size() * sizeof(int));
+        upload(g->cedge, cedge.data(), cedge.size() * sizeof(int));
+        g->ncedge = (int)cedge.size();
+      }
       if (ccorners && fcorners) {
         int nvc = 0, nvf = 0;
         for (size_t i = 0; i < (size_t)4 * ncoarse; ++i) nvc = std::max(nvc, ccorners[i] + 1);
@@ -927,6 +1019,7 @@ int lfg_intergrid_destroy(lfg_intergrid g) {
   dfree(g->w0_inj);
   dfree(g->w0_src);
   dfree(g->w0_w);
+  dfree(g->cedge);
   delete g;
   return LFG_OK;
 }

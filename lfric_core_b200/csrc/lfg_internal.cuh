@@ -16,6 +16,7 @@
 #include <unordered_map>
 #include <stdexcept>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/lfg.h"
@@ -192,6 +193,22 @@ struct lfg_mesh_s {
   // N couplings and its W and S neighbours' E and N ones.  Null when the
   // links do not pair up.
   int* hsrc = nullptr;  // device [4][ncol]
+  // Structured cubed-sphere numbering, detected at creation (pn = 0: none):
+  // 6 panels of pn x pn cells, numbered row-major inside each panel, and
+  // every cell off a panel's border has its side-f neighbour at
+  // c + base[(f + roll_p) & 3], base = {-1, +pn, +1, -pn},
+  // roll_p = (proll >> 2p) & 3.  pcf: the interior cells' hsrc codes follow
+  // from it (a side f >= 2 is its own face's designated side, a side f < 2
+  // reads its neighbour's side f + 2).
+  int pn = 0;
+  unsigned proll = 0;
+  bool pcf = false;
+  // First columns of the kPanelMargin-wide border groups of the
+  // element-parallel panel kernels (every group of rows 0 and pn-1, the
+  // first and last group of every other row); built when
+  // pn % kPanelMargin == 0 and pn >= 3 kPanelMargin, else null.
+  int* pedge = nullptr;  // device
+  int npedge = 0;
 };
 
 struct lfg_intergrid_s {
@@ -205,6 +222,15 @@ struct lfg_intergrid_s {
   double* w0_w = nullptr;  // device [nvert_fine][5] weights NE,SE,SW,NW and term count
   int nvert_coarse = 0, nvert_fine = 0;
   std::vector<int> h_child;  // [ncoarse][ny][nx]
+  // 2x2 maps between structured meshes (pnc = coarse panel side, 0: none):
+  // child slot q of coarse cell (panel P, column I, row J) is the fine cell
+  // P nf^2 + (2J + dy) nf + 2I + dx, nf = 2 pnc, with
+  // 2 dy + dx = (qpos >> (8P + 2q)) & 3.  cedge: the coarse cells on a
+  // panel's border (I or J in {0, pnc-1}).
+  int pnc = 0;
+  unsigned long long qpos = 0;
+  int* cedge = nullptr;  // device
+  int ncedge = 0;
 };
 
 struct lfg_cma_s {
@@ -217,6 +243,7 @@ struct lfg_cma_s {
   int* jminus = nullptr;      // [nrow] first band column of each row (0-based)
   int* jplus = nullptr;       // [nrow] last band column of each row
   int max_ind_to = 0, max_ind_from = 0;  // largest 1-based column offsets
+  bool ind_identity = false;  // ind_to(i) = i for every row (W3 -> W3 style maps)
   int* tptr = nullptr;        // [ncolumn+1] rows reaching each column (transpose)
   int* trow = nullptr;
   // Thomas factors of a square tridiagonal operator (columnwise_op_appinv's
@@ -342,6 +369,63 @@ inline int occ_grid(lfg_ctx c, const void* kern, int threads, size_t work, size_
   const size_t cap = (size_t)c->num_sms * nb;
   return (int)std::max<size_t>(1, std::min(need, cap));
 }
+
+// ------------------------------------------------------- vector accesses
+// V consecutive values of a V*sizeof(T)-aligned address moved by one load
+// or store instruction (8 or 16 bytes).
+template <class T, int V>
+struct Vec {
+  T e[V];
+};
+
+// V consecutive values from a V*sizeof(T)-aligned address (8 or 16 bytes:
+// one load); STREAM: evict-first, for arrays read once.  Four-wide FP32
+// loads ignore STREAM: the FP32 panel kernels measured faster with plain
+// loads (C192x70: sweep right-hand side 76 against 83 us, apply 104
+// against 107 us).
+template <bool STREAM, class T, int V>
+__device__ __forceinline__ Vec<T, V> vld(const T* p) {
+  Vec<T, V> r;
+  if constexpr (std::is_same_v<T, float> && V == 4) {
+    const float4 q = *reinterpret_cast<const float4*>(p);
+    r.e[0] = q.x; r.e[1] = q.y; r.e[2] = q.z; r.e[3] = q.w;
+  } else if constexpr (std::is_same_v<T, float> && V == 2) {
+    const float2 q = STREAM ? __ldcs(reinterpret_cast<const float2*>(p))
+                            : *reinterpret_cast<const float2*>(p);
+    r.e[0] = q.x; r.e[1] = q.y;
+  } else if constexpr (std::is_same_v<T, double> && V == 2) {
+    const double2 q = STREAM ? __ldcs(reinterpret_cast<const double2*>(p))
+                             : *reinterpret_cast<const double2*>(p);
+    r.e[0] = q.x; r.e[1] = q.y;
+  } else if constexpr (std::is_same_v<T, int> && V == 4) {
+    const int4 q = *reinterpret_cast<const int4*>(p);
+    r.e[0] = q.x; r.e[1] = q.y; r.e[2] = q.z; r.e[3] = q.w;
+  } else if constexpr (std::is_same_v<T, int> && V == 2) {
+    const int2 q = *reinterpret_cast<const int2*>(p);
+    r.e[0] = q.x; r.e[1] = q.y;
+  } else {
+    static_assert(V == 1, "vld: unsupported width");
+    r.e[0] = STREAM ? __ldcs(p) : *p;
+  }
+  return r;
+}
+
+template <class T, int V>
+__device__ __forceinline__ void vst(T* p, const Vec<T, V>& v) {
+  if constexpr (std::is_same_v<T, float> && V == 4)
+    *reinterpret_cast<float4*>(p) = make_float4(v.e[0], v.e[1], v.e[2], v.e[3]);
+  else if constexpr (std::is_same_v<T, float> && V == 2)
+    *reinterpret_cast<float2*>(p) = make_float2(v.e[0], v.e[1]);
+  else if constexpr (std::is_same_v<T, double> && V == 2)
+    *reinterpret_cast<double2*>(p) = make_double2(v.e[0], v.e[1]);
+  else
+    p[0] = v.e[0];
+}
+
+// Columns at each end of a panel row that the element-parallel panel
+// kernels leave to their per-column edge path (a multiple of every vector
+// width they use).
+constexpr int kPanelMargin = 4;
 
 // Throws LFG_ERR_STATE when a kernel recorded a device error (synchronises).
 void check_device_error(lfg_ctx c);

@@ -231,6 +231,58 @@ class ExtrudedMesh:
     def w0_ndof(self) -> int:
         return self.surface.nvert * (self.nlayers + 1)
 
+    def w2_dofmap(self) -> tuple[np.ndarray, int]:
+        """Lowest-order W2 dofmap, (ncell, 6) for the faces W, S, E, N, B, T,
+        and the number of dofs.
+
+        Numbered as dofmap_setup numbers one partition
+        (infrastructure/source/function_space/
+        function_space_constructor_helper_functions_mod.F90:1890-2020):
+        cells in order; each side face W, S, E, N not numbered yet gets a
+        column of nlayers dofs (the neighbour across it shares the column);
+        then the cell's vertical faces get one column of nlayers+1 dofs,
+        the bottom face at its start and the top face one further, so that
+        map(df) + k is the dof of layer k of face df.  0-based.
+        """
+        links = self.surface.face_links
+        ncell, nl = self.ncell, self.nlayers
+        m = np.full((ncell, 6), -1, dtype=np.int64)
+        nxt = 0
+        for c in range(ncell):
+            for f in range(4):
+                if m[c, f] < 0:
+                    m[c, f] = nxt
+                    nb = links[c, f]
+                    back = [g for g in range(4) if links[nb, g] == c and m[nb, g] < 0]
+                    if nb != c and back:
+                        m[nb, back[0]] = nxt
+                    nxt += nl
+            m[c, 4] = nxt
+            m[c, 5] = nxt + 1
+            nxt += nl + 1
+        return m, nxt
+
+    def w2_face_selectors(self) -> tuple[np.ndarray, np.ndarray]:
+        """Face selectors (ew, ns) of a W2 restriction onto this mesh: every
+        cell writes its W and S faces, and also its E (N) face when the
+        neighbour across it does not reach that face as its own W or S
+        (ew, ns = 2), so every face is written by at least one of its two
+        cells (restrict_w2's loop over face_selector_ew + face_selector_ns
+        faces, components/science/source/kernel/inter_mesh/
+        sci_restrict_w2_kernel_mod.F90:212-215).  A face that both cells
+        reach writes the same value from each: the same fine faces summed."""
+        links = self.surface.face_links
+        ncell = self.ncell
+        ew = np.ones(ncell, dtype=np.int32)
+        ns = np.ones(ncell, dtype=np.int32)
+        for c in range(ncell):
+            for f, sel in ((E, ew), (N, ns)):
+                nb = links[c, f]
+                back = [g for g in range(4) if links[nb, g] == c]
+                if not any(g in (W, S) for g in back):
+                    sel[c] = 2
+        return ew, ns
+
     def w0_coords(self) -> np.ndarray:
         """Cartesian coordinates of every W0 dof, (nvert*(nlayers+1), 3)."""
         r = self.radius + self.heights                  # (nl+1,)

@@ -237,6 +237,8 @@ typedef struct {
                               void* pctx, int k, double r_tol, double a_tol, int max_iter,\
                               int monitor, int nf, const int* field_of, T* x, const T* b, \
                               T* work /* (2 + 2k) n */, ora_solve_info* info);            \
+  void ora_cma_appinv_mesh_##S(int ncol, int nrow, const T* cm, const T* x, T* lhs);   \
+  void ora_cma_app_mesh_##S(int ncol, int nrow, const T* cm, const T* x, T* lhs);      \
   void ora_helm_apply_cb_##S(void* op, const T* x, T* y);                               \
   void ora_mg_apply_cb_##S(void* mg, const T* x, T* y);
 ORA_DECL_SOLVERS(double, d)

@@ -21,18 +21,22 @@
 #define REAL double
 #define S d
 #define APPINV ora_columnwise_op_appinv_code_r_double
+#define APP ora_columnwise_op_app_code_r_double
 #include "ora_real.inc"
 #undef REAL
 #undef S
 #undef APPINV
+#undef APP
 
 #define REAL float
 #define S f
 #define APPINV ora_columnwise_op_appinv_code_r_single
+#define APP ora_columnwise_op_app_code_r_single
 #include "ora_real.inc"
 #undef REAL
 #undef S
 #undef APPINV
+#undef APP
 
 /* Galerkin coarse operator R A P (project-defined multigrid set-up).
  * child is (ncoarse, 2(y), 2(x)) with y N->S, x W->E in each coarse cell's

@@ -243,6 +243,53 @@ class Helmholtz:
         return x, st, info
 
 
+class Lma(C.Structure):
+    """ora_lma: an LMA operator (local_stencil(ncell*nlayers, ndf, ndf),
+    1-based map(ndf, ncell))."""
+    _fields_ = [("ncell", C.c_int), ("nlayers", C.c_int), ("ndf", C.c_int), ("undf", C.c_int),
+                ("matrix", C.c_void_p), ("map", C.c_void_p)]
+
+
+class DiagPrec(C.Structure):
+    _fields_ = [("n", C.c_long), ("diag", C.c_void_p)]
+
+
+class W0:
+    """Oracle view of a W0 LMA problem (mass + stiffness): the matrix_vector
+    apply over every cell, mm_diagonal and the Jacobi-preconditioned
+    cg_solve, as the reference's mass_matrix_solver_alg composes them."""
+
+    def __init__(self, prob, matrix=None, native: bool = False):
+        self.L = lib(native)
+        self.prob = prob
+        self.A = np.ascontiguousarray(prob.matrix() if matrix is None else matrix,
+                                      dtype=np.float64)
+        self.map1 = np.ascontiguousarray(prob.map + 1, dtype=np.int32)
+        self.lma = Lma(prob.ncell, prob.nlayers, self.map1.shape[1], prob.ndof,
+                       self.A.ctypes.data, self.map1.ctypes.data)
+        self.diag = np.zeros(prob.ndof)
+        self.L.ora_lma_diagonal(C.byref(self.lma), ptr(self.diag))
+        self.dprec = DiagPrec(prob.ndof, self.diag.ctypes.data)
+
+    def apply(self, x: np.ndarray) -> np.ndarray:
+        y = np.zeros(self.prob.ndof)
+        self.L.ora_lma_apply_cb(C.byref(self.lma), ptr(np.ascontiguousarray(x)), ptr(y))
+        return y
+
+    def cg_solve(self, b, r_tol=1e-8, max_iter=2000):
+        n = self.prob.ndof
+        x = np.zeros(n)
+        work = np.zeros(3 * n)
+        info = SolveInfo()
+        L = self.L
+        st = L.ora_cg_solve_d(C.c_long(n), C.cast(L.ora_lma_apply_cb, C.c_void_p),
+                              C.byref(self.lma), C.cast(L.ora_diag_prec_apply, C.c_void_p),
+                              C.byref(self.dprec), C.c_double(r_tol), C.c_double(0.0), max_iter,
+                              1, ptr(x), ptr(np.ascontiguousarray(b, dtype=np.float64)), ptr(work),
+                              C.byref(info))
+        return x, st, info
+
+
 def _setup_signatures(L):
     L.ora_gcr_solve_d.argtypes = [C.c_long, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p,
                                   C.c_int, C.c_double, C.c_double, C.c_int, C.c_int, _dp, _dp,

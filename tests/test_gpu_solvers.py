@@ -95,8 +95,7 @@ def test_cg_jacobi_w0_parity(ctx, n, nl):
     """W0 mass + stiffness with a constant coefficient 1.0, uniform 1 km
     layers, Jacobi-preconditioned CG to 1e-8; (24, 20) is the full C24 x 20
     plain-method workload."""
-    import ctypes as C
-    from oracle.oracle import lib, ptr, SolveInfo
+    from oracle.oracle import W0 as OraW0
     p = w0_problem(n, nl, seed=1, top=nl * 1e3)
     A = p.matrix()
     nent, nlev = p.nvert, p.nlayers + 1
@@ -107,27 +106,7 @@ def test_cg_jacobi_w0_parity(ctx, n, nl):
                               diag, "cg", r_tol=1e-8, max_iter=2000)
     B, X = field_from(ctx, p.rhs, nent, nlev), Field(ctx, R_DOUBLE, nent, nlev)
     out = sol.apply(X, B)
-    L = lib()
-
-    class Lma(C.Structure):
-        _fields_ = [("ncell", C.c_int), ("nlayers", C.c_int), ("ndf", C.c_int), ("undf", C.c_int),
-                    ("matrix", C.c_void_p), ("map", C.c_void_p)]
-    m1 = np.ascontiguousarray(p.map + 1, dtype=np.int32)
-    Ac = np.ascontiguousarray(A)
-    lo = Lma(p.ncell, p.nlayers, 8, p.ndof, Ac.ctypes.data, m1.ctypes.data)
-    d = np.zeros(p.ndof)
-    L.ora_lma_diagonal(C.byref(lo), ptr(d))
-
-    class Dg(C.Structure):
-        _fields_ = [("n", C.c_long), ("diag", C.c_void_p)]
-    dp = Dg(p.ndof, d.ctypes.data)
-    x = np.zeros(p.ndof)
-    work = np.zeros(3 * p.ndof)
-    info = SolveInfo()
-    st = L.ora_cg_solve_d(C.c_long(p.ndof), C.cast(L.ora_lma_apply_cb, C.c_void_p), C.byref(lo),
-                          C.cast(L.ora_diag_prec_apply, C.c_void_p), C.byref(dp),
-                          C.c_double(1e-8), C.c_double(0.0), 2000, 1, ptr(x), ptr(np.ascontiguousarray(p.rhs)),
-                          ptr(work), C.byref(info))
+    x, st, info = OraW0(p, A).cg_solve(p.rhs, r_tol=1e-8, max_iter=2000)
     assert out.status == st == 0
     assert out.iterations == info.iterations
     assert rel(X.export(), x) < 1e-12
