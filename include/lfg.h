@@ -99,6 +99,17 @@ int lfg_field_wrap(lfg_ctx ctx, int kind, int ncol, int nlev, void* device_ptr,
                    lfg_field* field);
 int lfg_field_destroy(lfg_field field);
 int lfg_field_device_ptr(lfg_field field, void** device_ptr);
+/* Halo plumbing of a column-partitioned field (no counterpart in the
+ * reference, whose halo exchange is YAXT's, infrastructure/source/utilities/
+ * halo_comms_mod.F90): device_buf[k*ncols + i] = field(device_cols[i], k) for
+ * every level (pack), the reverse (unpack), and field columns
+ * [first, first+count) set to zero at every level.  device_cols and
+ * device_buf are device pointers; the calls run on the context's stream. */
+int lfg_field_pack_columns(lfg_field field, const int* device_cols, int ncols,
+                           void* device_buf);
+int lfg_field_unpack_columns(lfg_field field, const int* device_cols, int ncols,
+                             const void* device_buf);
+int lfg_field_zero_columns(lfg_field field, int first, int count);
 /* Copy a host array in the reference's column-contiguous order into the
  * field (import_field, sci_field_vector_mod.x90:307-331); host_kind may
  * differ from the field's kind (the value is converted). */
@@ -165,6 +176,16 @@ typedef struct lfg_w2map_s* lfg_w2map;
 int lfg_w2map_create(lfg_intergrid ig, int nlayers, int ndf, const int* map_coarse,
                      int undf_coarse, const int* map_fine, int undf_fine,
                      const int* face_selector_ew, const int* face_selector_ns, lfg_w2map* map);
+/* The same transfers on W2 fields held as level-major columns, the layout
+ * the LMA operators use (no counterpart in the reference, whose W2 fields
+ * are flat): every side face and every cell's vertical faces form one
+ * column of nlayers+1 levels (a side face uses the first nlayers), a field
+ * is (ncol, nlayers+1), and col_coarse[C*ndf + df] / col_fine[c*ndf + df]
+ * give the column of cell dof df (T is read through B's column). */
+int lfg_w2map_create_columns(lfg_intergrid ig, int nlayers, int ndf, const int* col_coarse,
+                             int ncol_coarse, const int* col_fine, int ncol_fine,
+                             const int* face_selector_ew, const int* face_selector_ns,
+                             lfg_w2map* map);
 int lfg_w2map_destroy(lfg_w2map map);
 #define LFG_W2_FULL 0   /* restrict_w2  (sci_restrict_w2_kernel_mod.F90)  */
 #define LFG_W2_H 1      /* restrict_w2h (sci_restrict_w2h_kernel_mod.F90) */
@@ -329,6 +350,15 @@ int lfg_prec_diagonal(lfg_field diag, lfg_prec* prec);     /* y = x / diag */
  * level, n_coarse sweeps on the coarsest level, relaxation omega. */
 int lfg_prec_multigrid(int nlevels, const lfg_helm* levels, const lfg_intergrid* maps,
                        int n_pre, int n_post, int n_coarse, double omega, lfg_prec* prec);
+/* Multigrid V-cycle over W2 LMA operators (abstract_hierarchical_preconditioner_type,
+ * components/science/source/solver/sci_hierarchical_preconditioner_mod.f90:22-38):
+ * levels[l] is the r_double W2 operator of level l (6 dofs per cell, fields
+ * of lfg_w2map_create_columns's layout), maps[l] joins level l to level
+ * l+1; weighted Jacobi smoothing (n_pre / n_post sweeps, n_coarse on the
+ * coarsest level, relaxation omega), restrict_w2 of the residual and
+ * prolong_w2 of the correction. */
+int lfg_prec_w2_multigrid(int nlevels, const lfg_lma* levels, const lfg_w2map* maps,
+                          int n_pre, int n_post, int n_coarse, double omega, lfg_prec* prec);
 int lfg_prec_destroy(lfg_prec prec);
 int lfg_prec_apply(lfg_prec prec, lfg_field x, lfg_field y);         /* y = P^{-1} x */
 

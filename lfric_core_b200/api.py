@@ -300,6 +300,26 @@ class W2Map(_Handle):
         super().__init__(ig.ctx, h, [ig])
         self.undf_coarse, self.undf_fine = undf_coarse, undf_fine
 
+    @classmethod
+    def columns(cls, ig: "Intergrid", nlayers: int, col_coarse, ncol_coarse: int, col_fine,
+                ncol_fine: int, sel_ew, sel_ns) -> "W2Map":
+        """The same transfers on W2 fields held as level-major columns
+        (ncol, nlayers+1), the layout of the W2 LMA operators: col_* (ncell,
+        ndf) give the column of each cell dof."""
+        mc = np.ascontiguousarray(col_coarse, dtype=np.int32)
+        mf = np.ascontiguousarray(col_fine, dtype=np.int32)
+        ew = np.ascontiguousarray(sel_ew, dtype=np.int32)
+        ns = np.ascontiguousarray(sel_ns, dtype=np.int32)
+        h = C.c_void_p()
+        ig.ctx.check(ig.ctx.lib.lfg_w2map_create_columns(
+            ig.h, nlayers, mc.shape[1], _iptr(mc), ncol_coarse, _iptr(mf), ncol_fine, _iptr(ew),
+            _iptr(ns), C.byref(h)), "w2map_create_columns")
+        self = cls.__new__(cls)
+        _Handle.__init__(self, ig.ctx, h, [ig])
+        self.undf_coarse = ncol_coarse * (nlayers + 1)
+        self.undf_fine = ncol_fine * (nlayers + 1)
+        return self
+
     def restrict(self, mode: int, coarse: "Field", fine: "Field"):
         self.ctx.check(self.ctx.lib.lfg_w2_restrict(self.h, mode, coarse.h, fine.h), "w2_restrict")
 
@@ -517,6 +537,21 @@ class Preconditioner(_Handle):
                                              n_coarse, omega, C.byref(h)), "prec_multigrid")
         return cls(ctx, h, [*levels, *maps])
 
+    @classmethod
+    def w2_multigrid(cls, levels: list, maps: list, n_pre=2, n_post=2, n_coarse=8,
+                     omega=0.6) -> "Preconditioner":
+        """V-cycle over W2 LMA operators (finest first) joined by column-layout
+        W2Maps: weighted Jacobi smoothing, restrict_w2 / prolong_w2."""
+        ctx = levels[0].ctx
+        lv = (C.c_void_p * len(levels))(*[l.h.value for l in levels])
+        mp = (C.c_void_p * max(1, len(maps)))(*[m.h.value for m in maps])
+        h = C.c_void_p()
+        ctx.check(ctx.lib.lfg_prec_w2_multigrid(len(levels), C.cast(lv, C.POINTER(C.c_void_p)),
+                                                C.cast(mp, C.POINTER(C.c_void_p)), n_pre,
+                                                n_post, n_coarse, omega, C.byref(h)),
+                  "prec_w2_multigrid")
+        return cls(ctx, h, [*levels, *maps])
+
     def apply(self, x: Field, y: Field):
         self.ctx.check(self.ctx.lib.lfg_prec_apply(self.h, x.h, y.h), "prec_apply")
 
@@ -723,3 +758,36 @@ class HelmholtzSystem:
 
     def solution(self) -> np.ndarray:
         return self.x64.export(np.float64)
+
+
+class W2System:
+    """A W2 hierarchy (problems.W2Hierarchy) on the device: each level's LMA
+    operator on (columns, nlayers+1) fields, the column-layout W2 maps
+    between consecutive levels, and the multigrid preconditioner over them."""
+
+    def __init__(self, ctx: Context, hier, n_pre=2, n_post=2, n_coarse=8, omega=0.6):
+        self.ctx, self.hier = ctx, hier
+        self.ops, self.maps, self.igs = [], [], []
+        for lev in hier.levels:
+            nlev = lev.nlayers + 1
+            cmap = (lev.ent.astype(np.int64) * nlev + lev.off).astype(np.int32)
+            self.ops.append(LocalOperator(ctx, R_DOUBLE, lev.ncell, lev.nlayers, lev.matrix,
+                                          cmap, lev.nent, nlev))
+        for l, cm in enumerate(hier.cell_maps):
+            fine, coarse = hier.levels[l], hier.levels[l + 1]
+            ig = Intergrid(ctx, cm, fine.ncell)
+            self.igs.append(ig)
+            self.maps.append(W2Map.columns(ig, fine.nlayers, coarse.ent, coarse.nent, fine.ent,
+                                           fine.nent, coarse.ew, coarse.ns))
+        self.prec = Preconditioner.w2_multigrid(self.ops, self.maps, n_pre, n_post, n_coarse,
+                                                omega)
+
+    def field(self, flat=None, level: int = 0) -> Field:
+        lev = self.hier.levels[level]
+        f = Field(self.ctx, R_DOUBLE, lev.nent, lev.nlayers + 1)
+        if flat is not None:
+            f.import_(lev.to_columns(flat))
+        return f
+
+    def flat(self, f: Field, level: int = 0) -> np.ndarray:
+        return self.hier.levels[level].from_columns(f.export())

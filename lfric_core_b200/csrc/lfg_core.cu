@@ -860,6 +860,66 @@ int lfg_field_device_ptr(lfg_field f, void** p) {
   return LFG_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+// buf[k*ncols + i] = field(cols[i], k) for every level k (PACK), or the
+// reverse (unpack): the halo columns of a partitioned field moved through
+// one contiguous buffer per neighbouring rank.
+template <class T, bool PACK>
+__global__ void k_columns(T* __restrict__ f, int ncol, int nlev, const int* __restrict__ cols,
+                          int ncols, T* __restrict__ buf) {
+  const size_t n = (size_t)ncols * nlev;
+  for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < n;
+       t += (size_t)gridDim.x * blockDim.x) {
+    const int k = (int)(t / ncols), i = (int)(t - (size_t)k * ncols);
+    const size_t o = (size_t)k * ncol + cols[i];
+    if (PACK) buf[t] = f[o];
+    else f[o] = buf[t];
+  }
+}
+
+template <bool PACK>
+int columns_op(lfg_field f, const int* cols, int ncols, void* buf) {
+  if (!f || (ncols > 0 && (!cols || !buf)) || ncols < 0) return LFG_ERR_ARG;
+  lfg_ctx c = f->ctx;
+  return guard(c, [&] {
+    if (ncols == 0) return;
+    const size_t n = (size_t)ncols * f->nlev;
+    if (f->kind == LFG_R_DOUBLE)
+      k_columns<double, PACK><<<c->stream_grid(n), kThreads, 0, c->stream>>>(
+          (double*)f->d, f->ncol, f->nlev, cols, ncols, (double*)buf);
+    else
+      k_columns<float, PACK><<<c->stream_grid(n), kThreads, 0, c->stream>>>(
+          (float*)f->d, f->ncol, f->nlev, cols, ncols, (float*)buf);
+    after_launch(c, PACK ? "pack_columns" : "unpack_columns", (uint64_t)2 * f->kind * n);
+  });
+}
+
+}  // namespace
+
+extern "C" {
+
+int lfg_field_pack_columns(lfg_field f, const int* device_cols, int ncols, void* device_buf) {
+  return columns_op<true>(f, device_cols, ncols, device_buf);
+}
+
+int lfg_field_unpack_columns(lfg_field f, const int* device_cols, int ncols,
+                             const void* device_buf) {
+  return columns_op<false>(f, device_cols, ncols, const_cast<void*>(device_buf));
+}
+
+int lfg_field_zero_columns(lfg_field f, int first, int count) {
+  if (!f || first < 0 || count < 0 || first + count > f->ncol) return LFG_ERR_ARG;
+  lfg_ctx c = f->ctx;
+  return guard(c, [&] {
+    if (count == 0) return;
+    LFG_CUDA(cudaMemset2DAsync((char*)f->d + (size_t)first * f->kind, (size_t)f->ncol * f->kind,
+                               0, (size_t)count * f->kind, f->nlev, c->stream));
+  });
+}
+
 int lfg_field_import(lfg_field f, const void* host, int host_kind) {
   if (!f) return LFG_ERR_ARG;
   lfg_ctx c = f->ctx;

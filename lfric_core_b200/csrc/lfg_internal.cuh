@@ -233,6 +233,19 @@ struct lfg_intergrid_s {
   int ncedge = 0;
 };
 
+// W2 intergrid maps (lfg_w2.cu)
+struct lfg_w2map_s {
+  lfg_ctx ctx = nullptr;
+  lfg_intergrid ig = nullptr;
+  int nl = 0, ndf = 0, undf_c = 0, undf_f = 0;
+  int nent_c = 0, nent_f = 0;  // level-major columns (0: flat fields)
+  bool has_sel = false;
+  int* mapc = nullptr;
+  int* mapf = nullptr;
+  int* sel_ew = nullptr;
+  int* sel_ns = nullptr;
+};
+
 struct lfg_cma_s {
   lfg_ctx ctx = nullptr;
   int kind = LFG_R_DOUBLE;

@@ -258,6 +258,97 @@ struct MgPrec : lfg_prec_s {
   }
 };
 
+// Multigrid V-cycle over W2 LMA operators: the hierarchical preconditioner
+// of abstract_hierarchical_preconditioner_type
+// (components/science/source/solver/sci_hierarchical_preconditioner_mod.f90:22-38),
+// each level holding the operator of its own mesh.  Every level smooths
+// with weighted Jacobi, x += omega (b - A x) / diag(A) (the diagonal of
+// mm_diagonal_kernel_code; dofs no cell reaches, the unused top level of the
+// side-face columns, keep a unit diagonal and stay zero); the residual goes
+// down with restrict_w2 (sci_restrict_w2_kernel_mod.F90) and the coarse
+// correction comes up with prolong_w2 (sci_prolong_w2_kernel_mod.F90,
+// weights from weights_prolong_w2) and is added; n_coarse sweeps from zero
+// on the coarsest level.  Fields are (columns, nlayers+1), FP64.
+__global__ void k_unit_zeros(double* __restrict__ d, size_t n) {
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
+       i += (size_t)gridDim.x * blockDim.x)
+    if (d[i] == 0.0) d[i] = 1.0;
+}
+
+struct W2MgPrec : lfg_prec_s {
+  std::vector<lfg_lma> ops;
+  std::vector<lfg_w2map> maps;
+  int n_pre, n_post, n_coarse;
+  double omega;
+  std::vector<FieldPtr> diag, res, ax, bc, xc, tp, pw;  // per level
+
+  W2MgPrec(int nlev, const lfg_lma* levels, const lfg_w2map* m, int pre, int post, int coarse,
+           double om)
+      : n_pre(pre), n_post(post), n_coarse(coarse), omega(om) {
+    ctx = levels[0]->ctx;
+    for (int l = 0; l < nlev; ++l) ops.push_back(levels[l]);
+    for (int l = 0; l + 1 < nlev; ++l) maps.push_back(m[l]);
+    for (int l = 0; l < nlev; ++l) {
+      const lfg_lma a = ops[l];
+      const int nc = a->nent_to, nv = a->nlev_to;
+      diag.push_back(make_field(ctx, LFG_R_DOUBLE, nc, nv));
+      res.push_back(make_field(ctx, LFG_R_DOUBLE, nc, nv));
+      ax.push_back(make_field(ctx, LFG_R_DOUBLE, nc, nv));
+      bc.push_back(make_field(ctx, LFG_R_DOUBLE, nc, nv));
+      xc.push_back(make_field(ctx, LFG_R_DOUBLE, nc, nv));
+      tp.push_back(make_field(ctx, LFG_R_DOUBLE, nc, nv));
+      pw.push_back(make_field(ctx, LFG_R_DOUBLE, nc, nv));
+      check(lfg_lma_diagonal(a, diag[l].get()));
+      const size_t n = diag[l]->n();
+      k_unit_zeros<<<ctx->stream_grid(n), kThreads, 0, ctx->stream>>>((double*)diag[l]->d, n);
+      after_launch(ctx, "unit_zeros", 8 * 2 * (uint64_t)n);
+      if (l + 1 < nlev) check(lfg_w2_prolong_weights(maps[l], pw[l].get()));
+    }
+  }
+
+  void check(int st) const {
+    if (st != LFG_OK) throw Error(st, ctx->last_error);
+  }
+
+  // x += omega (b - A x) / diag
+  void sweep(int l, lfg_field b, lfg_field x) {
+    lfg_field r = res[l].get(), y = ax[l].get();
+    check(lfg_lma_apply(ops[l], LFG_LMA_WRITE, y, x));
+    vec_copy(r, b);
+    vec_axpy(r, sc_const(-1.0), y);
+    vec_divide(r, r, diag[l].get());
+    vec_axpy(x, sc_const(omega), r);
+  }
+
+  void vcycle(int l, lfg_field b, lfg_field x) {
+    const int L = (int)ops.size();
+    vec_set(x, sc_const(0.0));
+    if (l == L - 1) {
+      for (int i = 0; i < n_coarse; ++i) sweep(l, b, x);
+      return;
+    }
+    for (int i = 0; i < n_pre; ++i) sweep(l, b, x);
+    lfg_field r = res[l].get(), y = ax[l].get();
+    check(lfg_lma_apply(ops[l], LFG_LMA_WRITE, y, x));
+    vec_copy(r, b);
+    vec_axpy(r, sc_const(-1.0), y);
+    check(lfg_w2_restrict(maps[l], LFG_W2_FULL, bc[l + 1].get(), r));
+    vcycle(l + 1, bc[l + 1].get(), xc[l + 1].get());
+    check(lfg_w2_prolong(maps[l], tp[l].get(), xc[l + 1].get(), pw[l].get()));
+    vec_axpy(x, sc_const(1.0), tp[l].get());
+    for (int i = 0; i < n_post; ++i) sweep(l, b, x);
+  }
+
+  void apply(lfg_field x, lfg_field y) override {
+    const lfg_lma a = ops[0];
+    LFG_REQUIRE(x->ncol == a->nent_to && x->nlev == a->nlev_to && x->kind == LFG_R_DOUBLE &&
+                    y->ncol == a->nent_to && y->nlev == a->nlev_to && y->kind == LFG_R_DOUBLE,
+                "w2 multigrid apply: fields do not match the finest operator");
+    LFG_REQUIRE(x->d != y->d, "w2 multigrid apply: x and y may not alias");
+    vcycle(0, x, y);
+  }
+};
+
 }  // namespace
 
 // ----------------------------------------------------------------- solvers
@@ -910,6 +1001,32 @@ int lfg_prec_multigrid(int nlevels, const lfg_helm* levels, const lfg_intergrid*
                     "prec_multigrid: intergrid map does not join the levels");
     }
     *out = new MgPrec(nlevels, levels, maps, n_pre, n_post, n_coarse, omega);
+  });
+}
+
+int lfg_prec_w2_multigrid(int nlevels, const lfg_lma* levels, const lfg_w2map* maps,
+                          int n_pre, int n_post, int n_coarse, double omega, lfg_prec* out) {
+  if (!levels || nlevels < 1 || !levels[0] || !out) return LFG_ERR_ARG;
+  lfg_ctx c = levels[0]->ctx;
+  return guard(c, [&] {
+    LFG_REQUIRE(n_pre >= 0 && n_post >= 0 && n_coarse >= 0 && omega > 0.0,
+                "prec_w2_multigrid: bad smoothing parameters");
+    for (int l = 0; l < nlevels; ++l) {
+      const lfg_lma m = levels[l];
+      LFG_REQUIRE(m && m->kind == LFG_R_DOUBLE && m->ndf_to == 6 && m->ndf_from == 6 &&
+                      m->nent_to == m->nent_from && m->nlev_to == m->nlev_from &&
+                      m->nlev_to == m->nl + 1,
+                  "prec_w2_multigrid: levels must be r_double W2 LMA operators on "
+                  "(columns, nlayers+1) fields");
+      if (l + 1 < nlevels) {
+        const lfg_w2map w = maps ? maps[l] : nullptr;
+        LFG_REQUIRE(w && w->ndf == 6 && w->nent_f == m->nent_to &&
+                        w->nent_c == levels[l + 1]->nent_to && w->nl == m->nl,
+                    "prec_w2_multigrid: maps[l] must join level l to level l+1 in the "
+                    "column layout");
+      }
+    }
+    *out = new W2MgPrec(nlevels, levels, maps, n_pre, n_post, n_coarse, omega);
   });
 }
 

@@ -34,7 +34,15 @@ struct W2Args {
   const int* mapf;   // [nfine][ndf]
   const int* sel_ew; // [ncoarse]
   const int* sel_ns;
+  // 0: flat fields in the reference's dof order (the dof of level k is
+  // map + k); else level-major columns (nent columns of nlayers+1 levels,
+  // the maps hold column ids, the dof of level k is k*nent + map)
+  int nent_c, nent_f;
 };
+
+__device__ __forceinline__ size_t dof_at(int map, int k, int nent) {
+  return nent ? (size_t)k * nent + map : (size_t)map + k;
+}
 
 __device__ __forceinline__ int fcell(const W2Args& a, int C, int x, int y) {
   return a.child[(size_t)(y * a.nx + x) * a.ncoarse + C];
@@ -60,8 +68,9 @@ __global__ void k_w2_restrict(W2Args a, int mode, T* __restrict__ coarse,
   if (mode == LFG_W2_V) {   // restrict_w2v: dof 1 of the W2V map
     T acc = (T)0;
     for (int y = 0; y < a.ny; ++y)
-      for (int x = 0; x < a.nx; ++x) acc = acc + fine[a.mapf[(size_t)fcell(a, C, x, y) * a.ndf] + k];
-    coarse[a.mapc[(size_t)C * a.ndf] + k] = acc;
+      for (int x = 0; x < a.nx; ++x)
+        acc = acc + fine[dof_at(a.mapf[(size_t)fcell(a, C, x, y) * a.ndf], k, a.nent_f)];
+    coarse[dof_at(a.mapc[(size_t)C * a.ndf], k, a.nent_c)] = acc;
     return;
   }
   if (k < a.nl) {
@@ -74,16 +83,16 @@ __global__ void k_w2_restrict(W2Args a, int mode, T* __restrict__ coarse,
       T acc = (T)0;
       for (int y = y0; y <= y1; ++y)
         for (int x = x0; x <= x1; ++x)
-          acc = acc + fine[a.mapf[(size_t)fcell(a, C, x, y) * a.ndf + df] + k];
-      coarse[a.mapc[(size_t)C * a.ndf + df] + k] = acc;
+          acc = acc + fine[dof_at(a.mapf[(size_t)fcell(a, C, x, y) * a.ndf + df], k, a.nent_f)];
+      coarse[dof_at(a.mapc[(size_t)C * a.ndf + df], k, a.nent_c)] = acc;
     }
   }
   if (mode == LFG_W2_FULL) {
     T acc = (T)0;
     for (int y = 0; y < a.ny; ++y)
       for (int x = 0; x < a.nx; ++x)
-        acc = acc + fine[a.mapf[(size_t)fcell(a, C, x, y) * a.ndf + DB] + k];
-    coarse[a.mapc[(size_t)C * a.ndf + DB] + k] = acc;
+        acc = acc + fine[dof_at(a.mapf[(size_t)fcell(a, C, x, y) * a.ndf + DB], k, a.nent_f)];
+    coarse[dof_at(a.mapc[(size_t)C * a.ndf + DB], k, a.nent_c)] = acc;
   }
 }
 
@@ -94,7 +103,7 @@ __global__ void k_w2_weights(W2Args a, double* __restrict__ w) {
   const int C = (int)(t / nk), k = (int)(t % nk);
   const int nx = a.nx, ny = a.ny;
   auto W = [&](int df, int x, int y) -> double& {
-    return w[a.mapf[(size_t)fcell(a, C, x, y) * a.ndf + df] + k];
+    return w[dof_at(a.mapf[(size_t)fcell(a, C, x, y) * a.ndf + df], k, a.nent_f)];
   };
   if (k < a.nl) {
     for (int x = 0; x < nx; ++x) {
@@ -123,9 +132,9 @@ __global__ void k_w2_prolong(W2Args a, double* __restrict__ fine,
   const int C = (int)(t / nk), k = (int)(t % nk);
   const int nx = a.nx, ny = a.ny;
   auto F = [&](int df, int x, int y) {
-    return (size_t)a.mapf[(size_t)fcell(a, C, x, y) * a.ndf + df] + k;
+    return dof_at(a.mapf[(size_t)fcell(a, C, x, y) * a.ndf + df], k, a.nent_f);
   };
-  auto CO = [&](int df) { return coarse[a.mapc[(size_t)C * a.ndf + df] + k]; };
+  auto CO = [&](int df) { return coarse[dof_at(a.mapc[(size_t)C * a.ndf + df], k, a.nent_c)]; };
   if (k < a.nl) {
     for (int x = 0; x < nx; ++x) {
       fine[F(DN, x, 0)] = w[F(DN, x, 0)] * CO(DN);
@@ -156,22 +165,11 @@ __global__ void k_w2_prolong(W2Args a, double* __restrict__ fine,
 
 }  // namespace
 
-struct lfg_w2map_s {
-  lfg_ctx ctx = nullptr;
-  lfg_intergrid ig = nullptr;
-  int nl = 0, ndf = 0, undf_c = 0, undf_f = 0;
-  bool has_sel = false;
-  int* mapc = nullptr;
-  int* mapf = nullptr;
-  int* sel_ew = nullptr;
-  int* sel_ns = nullptr;
-};
-
 namespace {
 
 W2Args args_of(lfg_w2map m) {
   return W2Args{m->ig->ncoarse, m->nl, m->ig->nx, m->ig->ny, m->ndf, m->ig->child,
-                m->mapc,        m->mapf, m->sel_ew, m->sel_ns};
+                m->mapc,        m->mapf, m->sel_ew, m->sel_ns, m->nent_c, m->nent_f};
 }
 
 void w2_release(lfg_w2map m) {
@@ -198,9 +196,15 @@ void check_map(const int* map, int ncell, int ndf, int nl, int undf, const char*
 
 extern "C" {
 
-int lfg_w2map_create(lfg_intergrid ig, int nlayers, int ndf, const int* map_coarse,
-                     int undf_coarse, const int* map_fine, int undf_fine,
-                     const int* face_selector_ew, const int* face_selector_ns, lfg_w2map* out) {
+}  // extern "C"
+
+namespace {
+
+// lfg_w2map_create (nent_c = nent_f = 0) and lfg_w2map_create_columns
+int w2map_create(lfg_intergrid ig, int nlayers, int ndf, const int* map_coarse,
+                 int undf_coarse, const int* map_fine, int undf_fine,
+                 const int* face_selector_ew, const int* face_selector_ns, int nent_c,
+                 int nent_f, lfg_w2map* out) {
   if (!ig || !out || !map_coarse || !map_fine) return LFG_ERR_ARG;
   lfg_ctx c = ig->ctx;
   lfg_w2map m = new lfg_w2map_s;
@@ -215,8 +219,19 @@ int lfg_w2map_create(lfg_intergrid ig, int nlayers, int ndf, const int* map_coar
     m->ndf = ndf;
     m->undf_c = undf_coarse;
     m->undf_f = undf_fine;
-    check_map(map_coarse, ig->ncoarse, ndf, nlayers, undf_coarse, "w2map_create (coarse)");
-    check_map(map_fine, ig->nfine, ndf, nlayers, undf_fine, "w2map_create (fine)");
+    m->nent_c = nent_c;
+    m->nent_f = nent_f;
+    if (nent_c) {  // column ids of level-major fields with nlayers+1 levels
+      for (size_t i = 0; i < (size_t)ig->ncoarse * ndf; ++i)
+        LFG_REQUIRE(map_coarse[i] >= 0 && map_coarse[i] < nent_c,
+                    "w2map_create_columns: coarse column id out of range");
+      for (size_t i = 0; i < (size_t)ig->nfine * ndf; ++i)
+        LFG_REQUIRE(map_fine[i] >= 0 && map_fine[i] < nent_f,
+                    "w2map_create_columns: fine column id out of range");
+    } else {
+      check_map(map_coarse, ig->ncoarse, ndf, nlayers, undf_coarse, "w2map_create (coarse)");
+      check_map(map_fine, ig->nfine, ndf, nlayers, undf_fine, "w2map_create (fine)");
+    }
     m->mapc = (int*)dmalloc(sizeof(int) * (size_t)ig->ncoarse * ndf);
     m->mapf = (int*)dmalloc(sizeof(int) * (size_t)ig->nfine * ndf);
     upload(m->mapc, map_coarse, sizeof(int) * (size_t)ig->ncoarse * ndf);
@@ -240,6 +255,27 @@ int lfg_w2map_create(lfg_intergrid ig, int nlayers, int ndf, const int* map_coar
   }
   *out = m;
   return LFG_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int lfg_w2map_create(lfg_intergrid ig, int nlayers, int ndf, const int* map_coarse,
+                     int undf_coarse, const int* map_fine, int undf_fine,
+                     const int* face_selector_ew, const int* face_selector_ns, lfg_w2map* out) {
+  return w2map_create(ig, nlayers, ndf, map_coarse, undf_coarse, map_fine, undf_fine,
+                      face_selector_ew, face_selector_ns, 0, 0, out);
+}
+
+int lfg_w2map_create_columns(lfg_intergrid ig, int nlayers, int ndf, const int* col_coarse,
+                             int ncol_coarse, const int* col_fine, int ncol_fine,
+                             const int* face_selector_ew, const int* face_selector_ns,
+                             lfg_w2map* out) {
+  if (ncol_coarse <= 0 || ncol_fine <= 0) return LFG_ERR_ARG;
+  return w2map_create(ig, nlayers, ndf, col_coarse, ncol_coarse * (nlayers + 1), col_fine,
+                      ncol_fine * (nlayers + 1), face_selector_ew, face_selector_ns,
+                      ncol_coarse, ncol_fine, out);
 }
 
 int lfg_w2map_destroy(lfg_w2map m) {

@@ -285,3 +285,168 @@ def w0_problem(n: int, nlayers: int, seed: int, top: float, kappa_sigma: float =
     rhs = rng.standard_normal(mesh.w0_ndof())
     return W0Problem(ncell=ncell, nlayers=nlayers, nvert=mesh.surface.nvert,
                      map=mesh.w0_dofmap(), mass=mass, stiff=stiff, kappa=kappa, rhs=rhs)
+
+
+# ------------------------------------------------------------------ W2 LMA
+# Lowest-order Raviart-Thomas (W2) basis on the unit cube, one function per
+# face W, S, E, N, B, T with unit flux through its own face in the positive
+# direction of its axis (as the W2 transfers assume: a coarse cell's W and E
+# values are fluxes in the same direction): phi_W = (1 - xi1, 0, 0),
+# phi_E = (xi1, 0, 0), and likewise in xi2 (S, N) and xi3 (B, T); the
+# reference divergences are -1 (W, S, B) and +1 (E, N, T).
+_RT_AXIS = (0, 1, 0, 1, 2, 2)
+_RT_UP = (False, False, True, True, False, True)     # xi or 1 - xi
+_RT_DIV = np.array([-1.0, -1.0, 1.0, 1.0, -1.0, 1.0])
+
+
+def w2_element_matrices(mesh, tau: float) -> np.ndarray:
+    """Per cell-layer 6x6 matrices of M + tau D on the extruded mesh, with
+    M the W2 mass matrix and D the divergence-divergence form, both through
+    the contravariant Piola map of the trilinear hexahedron (2x2x2 Gauss),
+    in the cell's local positive directions.  Returns (ncell*nl, 6, 6)."""
+    surf, nl = mesh.surface, mesh.nlayers
+    ncell = surf.ncell
+    r = mesh.radius + mesh.heights
+    base = surf.vertex_xyz[surf.cell_vertices]
+    bot = base[:, None, :, :] * r[None, :-1, None, None]
+    top = base[:, None, :, :] * r[None, 1:, None, None]
+    X = np.concatenate([bot, top], axis=2).reshape(ncell * nl, 8, 3)
+    g = np.array([0.5 - 0.5 / np.sqrt(3.0), 0.5 + 0.5 / np.sqrt(3.0)])
+    dd = np.outer(_RT_DIV, _RT_DIV)
+    A = np.zeros((ncell * nl, 6, 6))
+    for a in g:
+        for b in g:
+            for c in g:
+                xi = np.array([a, b, c])
+                _, dphi = _q1(xi)
+                J = np.einsum("nia,ib->nab", X, dphi)           # dx_a / dxi_b
+                detJ = np.abs(np.linalg.det(J))
+                ref = np.zeros((6, 3))
+                for f in range(6):
+                    t = xi[_RT_AXIS[f]]
+                    ref[f, _RT_AXIS[f]] = t if _RT_UP[f] else 1.0 - t
+                Jphi = np.einsum("nab,fb->nfa", J, ref)          # J phi_hat
+                w = 0.125
+                A += (w / detJ)[:, None, None] * np.einsum("nfa,nga->nfg", Jphi, Jphi)
+                A += (tau * w / detJ)[:, None, None] * dd[None, :, :]
+    return A
+
+
+@dataclass
+class W2Level:
+    """One level of a W2 multigrid hierarchy in the device layout the
+    library's LMA operators use: entities are the side-face columns
+    (nlayers dofs) followed by one vertical column per cell (nlayers+1 dofs,
+    B at offset 0 and T at offset 1); a field is (nent, nlayers+1) columns,
+    the top level of every side face unused (zero).
+
+    ent / off (ncell, 6): entity and level offset of each cell dof W, S, E,
+    N, B, T.  matrix: local_stencil (ncell*nl, 6, 6) in Fortran order with
+    the global orientation signs applied.  A field on the host is
+    column-contiguous, column e holding its nlayers+1 levels (to_columns /
+    from_columns convert from / to the flat order).  flat_map (ncell, 6) and
+    flat_ndof: the same space in the reference's flat dof order
+    (ExtrudedMesh.w2_dofmap).  ew / ns: face selectors of restrictions onto
+    this level."""
+
+    n: int
+    nlayers: int
+    ncell: int
+    nent: int
+    ent: np.ndarray
+    off: np.ndarray
+    matrix: np.ndarray
+    flat_map: np.ndarray
+    flat_ndof: int
+    links: np.ndarray
+    ew: np.ndarray
+    ns: np.ndarray
+
+    @property
+    def nlev(self) -> int:
+        return self.nlayers + 1
+
+    def to_columns(self, v: np.ndarray) -> np.ndarray:
+        """Flat reference-order W2 vector -> (nent, nlev) column-contiguous
+        (the order Field.import_ takes; padding levels zero)."""
+        out = np.zeros((self.nent, self.nlev))
+        for df in range(5):
+            ncol = self.nlayers + (1 if df == 4 else 0)
+            for k in range(ncol):
+                out[self.ent[:, df], k] = v[self.flat_map[:, df] + k]
+        return out.ravel()
+
+    def from_columns(self, d: np.ndarray) -> np.ndarray:
+        d = np.asarray(d).reshape(self.nent, self.nlev)
+        v = np.zeros(self.flat_ndof)
+        for df in range(5):
+            ncol = self.nlayers + (1 if df == 4 else 0)
+            for k in range(ncol):
+                v[self.flat_map[:, df] + k] = d[self.ent[:, df], k]
+        return v
+
+
+def w2_level(n: int, nlayers: int, top: float, tau: float,
+             radius: float = EARTH_RADIUS_DEFAULT) -> W2Level:
+    from .mesh import extruded_mesh
+    mesh = extruded_mesh(n, nlayers, top, radius=radius)
+    fmap, ndof = mesh.w2_dofmap()
+    ncell = mesh.ncell
+    # entities: side-face columns in dof order, then one vertical column per cell
+    side = np.unique(fmap[:, :4])
+    nside = side.size
+    face_ent = {int(d): i for i, d in enumerate(side)}
+    ent = np.zeros((ncell, 6), dtype=np.int32)
+    off = np.zeros((ncell, 6), dtype=np.int32)
+    for c in range(ncell):
+        for df in range(4):
+            ent[c, df] = face_ent[int(fmap[c, df])]
+        ent[c, 4] = ent[c, 5] = nside + c
+        off[c, 5] = 1
+    # global orientation: the two cells of a face agree on its direction
+    # when one reaches it as E or N and the other as W or S (inside a panel
+    # always); where a panel edge pairs E/N with E/N or W/S with W/S, the
+    # cell that did not number the face (the later one) flips its function
+    links = mesh.surface.face_links
+    sign = np.ones((ncell, 6))
+    for c in range(ncell):
+        for df in range(4):
+            nb = int(links[c, df])
+            g = [q for q in range(4) if links[nb, q] == c][0]
+            if (df >= 2) != (g < 2) and c > nb:
+                sign[c, df] = -1.0
+    Ae = w2_element_matrices(mesh, tau)
+    nl = nlayers
+    s = np.repeat(sign, nl, axis=0)                     # (ncell*nl, 6), ik = c*nl + layer
+    Ae = Ae * s[:, :, None] * s[:, None, :]
+    # local_stencil(ik, df, df2) in Fortran order: ik fastest, then df, then df2
+    matrix = np.ascontiguousarray(Ae.transpose(2, 1, 0)).ravel()
+    ew, ns = mesh.w2_face_selectors()
+    return W2Level(n=n, nlayers=nlayers, ncell=ncell, nent=nside + ncell, ent=ent, off=off,
+                   matrix=matrix, flat_map=fmap.astype(np.int32), flat_ndof=int(ndof),
+                   links=mesh.surface.face_links, ew=ew, ns=ns)
+
+
+@dataclass
+class W2Hierarchy:
+    """W2 operators A = M + tau D on C_n, C_{n/2}, ... (rediscretised on every
+    level) with the 2x2 cell maps between consecutive levels and a seeded
+    right-hand side on the finest level (flat reference order)."""
+
+    levels: list
+    cell_maps: list
+    rhs: np.ndarray
+
+
+def w2_hierarchy(n: int, nlayers: int, nlevels: int, seed: int, top: float = 10e3,
+                 tau: float = 1.0, radius: float = EARTH_RADIUS_DEFAULT) -> W2Hierarchy:
+    from .mesh import coarsen_map
+    levels, maps = [], []
+    m = n
+    for l in range(nlevels):
+        levels.append(w2_level(m, nlayers, top, tau, radius))
+        if l + 1 < nlevels:
+            maps.append(coarsen_map(m))
+            m //= 2
+    rhs = np.random.default_rng(seed).standard_normal(levels[0].flat_ndof)
+    return W2Hierarchy(levels=levels, cell_maps=maps, rhs=rhs)

@@ -264,6 +264,32 @@ void ora_lma_apply_cb(void* op, const double* x, double* y);
 void ora_lma_apply_transpose(const ora_lma* op, const double* x, double* y);
 void ora_lma_diagonal(const ora_lma* op, double* diag);
 
+/* Multigrid V-cycle over W2 LMA operators (project-defined set-up of the
+ * reference's abstract_hierarchical_preconditioner_type,
+ * components/science/source/solver/sci_hierarchical_preconditioner_mod.f90:22-38):
+ * flat W2 fields in the reference's dof order, level 0 finest.  Each level
+ * smooths with weighted Jacobi, x = x + omega (b - A x) / diag with diag
+ * the mm_diagonal of its operator (entries no cell reaches count as 1);
+ * the residual goes down with restrict_w2, the coarse correction comes up
+ * with prolong_w2 (weights_prolong_w2 weights) and is added; n_coarse sweeps
+ * from zero on the coarsest level.  cell_map[l] holds, for each cell of
+ * level l+1, its 2x2 cells of level l as Fortran cell_map(2, 2), 1-based;
+ * sel_ew / sel_ns[l] are the face selectors of the cells of level l+1. */
+#define ORA_W2MG_MAXLEV 8
+typedef struct {
+  int nlevels, n_pre, n_post, n_coarse;
+  double omega;
+  ora_lma op[ORA_W2MG_MAXLEV];
+  int ncoarse[ORA_W2MG_MAXLEV];
+  const int* cell_map[ORA_W2MG_MAXLEV];
+  const int* sel_ew[ORA_W2MG_MAXLEV];
+  const int* sel_ns[ORA_W2MG_MAXLEV];
+  double* work;  /* ora_w2mg_work_size doubles, filled by ora_w2mg_setup */
+} ora_w2mg;
+long ora_w2mg_work_size(const ora_w2mg* mg);
+void ora_w2mg_setup(ora_w2mg* mg);
+void ora_w2mg_apply_cb(void* mg, const double* b, double* x);
+
 /* Mixed-precision iterative refinement: FP64 outer residual and update,
  * FP32 inner GCR(k) preconditioned by an FP32 multigrid V-cycle with FP64
  * inner products.  Returns a status; x starts from zero. */

@@ -221,3 +221,81 @@ int ora_threads(int n) {
   return 1;
 #endif
 }
+
+/* ------------------------------------------------ W2 multigrid V-cycle
+ * Work per level l (undf_l doubles each): diag, r, y, bc, xc, t, w. */
+enum { W2_DIAG, W2_R, W2_Y, W2_BC, W2_XC, W2_T, W2_W, W2_NARR };
+
+static double* w2_arr(const ora_w2mg* mg, int l, int which) {
+  long off = 0;
+  for (int i = 0; i < l; ++i) off += (long)W2_NARR * mg->op[i].undf;
+  return mg->work + off + (long)which * mg->op[l].undf;
+}
+
+long ora_w2mg_work_size(const ora_w2mg* mg) {
+  long n = 0;
+  for (int l = 0; l < mg->nlevels; ++l) n += (long)W2_NARR * mg->op[l].undf;
+  return n;
+}
+
+void ora_w2mg_setup(ora_w2mg* mg) {
+  for (int l = 0; l < mg->nlevels; ++l) {
+    double* d = w2_arr(mg, l, W2_DIAG);
+    ora_lma_diagonal(&mg->op[l], d);
+    for (int i = 0; i < mg->op[l].undf; ++i)
+      if (d[i] == 0.0) d[i] = 1.0;
+    if (l + 1 < mg->nlevels) {
+      double* w = w2_arr(mg, l, W2_W);
+      memset(w, 0, sizeof(double) * mg->op[l].undf);
+      for (int C = 0; C < mg->ncoarse[l]; ++C)
+        ora_weights_prolong_w2_code(mg->op[l].nlayers, mg->cell_map[l] + 4 * C, 2, 2, 4, w, 6,
+                                    mg->op[l].map);
+    }
+  }
+}
+
+/* x = x + omega (b - A x) / diag */
+static void w2_sweep(ora_w2mg* mg, int l, const double* b, double* x) {
+  const long n = mg->op[l].undf;
+  double *r = w2_arr(mg, l, W2_R), *y = w2_arr(mg, l, W2_Y);
+  const double* d = w2_arr(mg, l, W2_DIAG);
+  ora_lma_apply_cb(&mg->op[l], x, y);
+  for (long i = 0; i < n; ++i) r[i] = b[i] + (-1.0) * y[i];
+  for (long i = 0; i < n; ++i) r[i] = r[i] / d[i];
+  for (long i = 0; i < n; ++i) x[i] = x[i] + mg->omega * r[i];
+}
+
+static void w2_vcycle(ora_w2mg* mg, int l, const double* b, double* x) {
+  const long n = mg->op[l].undf;
+  const int nl = mg->op[l].nlayers;
+  memset(x, 0, sizeof(double) * n);
+  if (l == mg->nlevels - 1) {
+    for (int i = 0; i < mg->n_coarse; ++i) w2_sweep(mg, l, b, x);
+    return;
+  }
+  for (int i = 0; i < mg->n_pre; ++i) w2_sweep(mg, l, b, x);
+  double *r = w2_arr(mg, l, W2_R), *y = w2_arr(mg, l, W2_Y);
+  ora_lma_apply_cb(&mg->op[l], x, y);
+  for (long i = 0; i < n; ++i) r[i] = b[i] + (-1.0) * y[i];
+  double* bc = w2_arr(mg, l + 1, W2_BC);
+  double* xc = w2_arr(mg, l + 1, W2_XC);
+  double work[ORA_MAX_NL + 1];
+  for (int C = 0; C < mg->ncoarse[l]; ++C) {
+    const int sel_idx[1] = {C + 1};
+    ora_restrict_w2_code_r_double(nl, mg->cell_map[l] + 4 * C, 2, 2, 4, bc, r, mg->sel_ew[l],
+                                  mg->sel_ns[l], mg->op[l + 1].map + 6 * C, 6, mg->op[l].map,
+                                  sel_idx, 1, work);
+  }
+  w2_vcycle(mg, l + 1, bc, xc);
+  double* t = w2_arr(mg, l, W2_T);
+  const double* w = w2_arr(mg, l, W2_W);
+  for (int C = 0; C < mg->ncoarse[l]; ++C)
+    ora_prolong_w2_code(nl, mg->cell_map[l] + 4 * C, 2, 2, 4, t, xc, w, 6, mg->op[l].map,
+                        mg->op[l + 1].map + 6 * C);
+  for (long i = 0; i < n; ++i) x[i] = x[i] + 1.0 * t[i];
+  for (int i = 0; i < mg->n_post; ++i) w2_sweep(mg, l, b, x);
+}
+
+void ora_w2mg_apply_cb(void* vmg, const double* b, double* x) {
+  w2_vcycle((ora_w2mg*)vmg, 0, b, x);
+}

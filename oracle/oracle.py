@@ -312,3 +312,113 @@ def _setup_signatures(L):
                                  C.c_double, C.c_double, C.c_int, C.c_int, _dp, _dp, _dp,
                                  C.c_void_p]
 
+
+
+MAX_W2_LEVELS = 8
+
+
+class W2MgStruct(C.Structure):
+    _fields_ = [("nlevels", C.c_int), ("n_pre", C.c_int), ("n_post", C.c_int),
+                ("n_coarse", C.c_int), ("omega", C.c_double),
+                ("op", Lma * MAX_W2_LEVELS), ("ncoarse", C.c_int * MAX_W2_LEVELS),
+                ("cell_map", C.c_void_p * MAX_W2_LEVELS),
+                ("sel_ew", C.c_void_p * MAX_W2_LEVELS), ("sel_ns", C.c_void_p * MAX_W2_LEVELS),
+                ("work", C.c_void_p)]
+
+
+class W2Multigrid:
+    """Oracle view of a W2 hierarchy (problems.W2Hierarchy): flat W2 fields
+    in the reference's dof order, each level's LMA operator with 1-based
+    dofmaps, and the V-cycle of ora_w2mg_apply_cb as a preconditioner of
+    the reference's cg_solve."""
+
+    def __init__(self, hier, n_pre=2, n_post=2, n_coarse=8, omega=0.6, native: bool = False):
+        L = lib(native)
+        self.L, self.hier = L, hier
+        self.keep = []
+        s = W2MgStruct()
+        nlev = len(hier.levels)
+        s.nlevels, s.n_pre, s.n_post, s.n_coarse, s.omega = nlev, n_pre, n_post, n_coarse, omega
+        for l, lev in enumerate(hier.levels):
+            A = self._flat_matrix(lev)
+            m1 = np.ascontiguousarray(lev.flat_map + 1, dtype=np.int32)
+            self.keep += [A, m1]
+            s.op[l] = Lma(lev.ncell, lev.nlayers, 6, lev.flat_ndof, A.ctypes.data, m1.ctypes.data)
+        for l, cm in enumerate(hier.cell_maps):
+            cmf = np.ascontiguousarray(np.asarray(cm).reshape(cm.shape[0], 4) + 1, dtype=np.int32)
+            coarse = hier.levels[l + 1]
+            ew = np.ascontiguousarray(coarse.ew, dtype=np.int32)
+            ns = np.ascontiguousarray(coarse.ns, dtype=np.int32)
+            self.keep += [cmf, ew, ns]
+            s.ncoarse[l] = cm.shape[0]
+            s.cell_map[l], s.sel_ew[l], s.sel_ns[l] = cmf.ctypes.data, ew.ctypes.data, ns.ctypes.data
+        L.ora_w2mg_work_size.restype = C.c_long
+        work = np.zeros(L.ora_w2mg_work_size(C.byref(s)))
+        self.keep.append(work)
+        s.work = work.ctypes.data
+        L.ora_w2mg_setup(C.byref(s))
+        self.s = s
+        self.op0 = s.op[0]
+
+    @staticmethod
+    def _flat_matrix(lev):
+        # local_stencil as stored: Fortran (ncell*nl, 6, 6) flattened
+        return np.ascontiguousarray(lev.matrix, dtype=np.float64)
+
+    def apply(self, x: np.ndarray) -> np.ndarray:
+        y = np.zeros(self.hier.levels[0].flat_ndof)
+        self.L.ora_lma_apply_cb(C.byref(self.op0), ptr(np.ascontiguousarray(x)), ptr(y))
+        return y
+
+    def vcycle(self, b: np.ndarray) -> np.ndarray:
+        x = np.zeros_like(b)
+        self.L.ora_w2mg_apply_cb(C.byref(self.s), ptr(np.ascontiguousarray(b)), ptr(x))
+        return x
+
+    def cg_solve(self, b, r_tol=1e-8, max_iter=500, multigrid=True):
+        """cg_solve preconditioned by the V-cycle (or by the diagonal)."""
+        L = self.L
+        n = b.size
+        x = np.zeros(n)
+        work = np.zeros(3 * n)
+        info = SolveInfo()
+        if multigrid:
+            prec, pctx = C.cast(L.ora_w2mg_apply_cb, C.c_void_p), C.byref(self.s)
+        else:
+            d = np.zeros(n)
+            L.ora_lma_diagonal(C.byref(self.op0), ptr(d))
+            self.keep.append(d)
+            dp = DiagPrec(n, d.ctypes.data)
+            self.keep.append(dp)
+            prec, pctx = C.cast(L.ora_diag_prec_apply, C.c_void_p), C.byref(dp)
+        st = L.ora_cg_solve_d(C.c_long(n), C.cast(L.ora_lma_apply_cb, C.c_void_p),
+                              C.byref(self.op0), prec, pctx, C.c_double(r_tol), C.c_double(0.0),
+                              max_iter, 1, ptr(x), ptr(np.ascontiguousarray(b, dtype=np.float64)),
+                              ptr(work), C.byref(info))
+        return x, st, info
+
+
+def _w2_gcr(self, b, gcrk=10, r_tol=1e-8, max_iter=100, multigrid=True):
+    """gcr_solve (right-preconditioned GCR(k)) with the V-cycle or the diagonal."""
+    L = self.L
+    n = b.size
+    x = np.zeros(n)
+    work = np.zeros((2 * gcrk + 3) * n)
+    info = SolveInfo()
+    if multigrid:
+        prec, pctx = C.cast(L.ora_w2mg_apply_cb, C.c_void_p), C.byref(self.s)
+    else:
+        d = np.zeros(n)
+        L.ora_lma_diagonal(C.byref(self.op0), ptr(d))
+        dp = DiagPrec(n, d.ctypes.data)
+        self.keep += [d, dp]
+        prec, pctx = C.cast(L.ora_diag_prec_apply, C.c_void_p), C.byref(dp)
+    st = L.ora_gcr_solve_d(C.c_long(n), C.cast(L.ora_lma_apply_cb, C.c_void_p),
+                           C.byref(self.op0), prec, pctx, gcrk, C.c_double(r_tol),
+                           C.c_double(0.0), max_iter, 1, ptr(x),
+                           ptr(np.ascontiguousarray(b, dtype=np.float64)), ptr(work),
+                           C.byref(info))
+    return x, st, info
+
+
+W2Multigrid.gcr_solve = _w2_gcr
