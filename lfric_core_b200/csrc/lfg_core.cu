@@ -14,6 +14,7 @@
 #include <map>
 #include <utility>
 
+#include <cstdlib>
 #include <cstring>
 
 using namespace lfg;
@@ -91,6 +92,8 @@ __device__ __forceinline__ void for_each_pack(const Op& op, size_t n, bool vec, 
 
 template <class T, class Op>
 __global__ void k_ew(Op op, size_t n, bool vec) {
+  grid_dep_launch();
+  grid_dep_wait();
   double acc = 0.0;
   const auto b = op.bind();
   for_each_pack<T>(b, n, vec, acc);
@@ -98,6 +101,8 @@ __global__ void k_ew(Op op, size_t n, bool vec) {
 
 template <class T, class Op>
 __global__ void k_ewr(Op op, size_t n, bool vec, Red r) {
+  grid_dep_launch();
+  grid_dep_wait();
   double acc = 0.0;
   const auto b = op.bind();
   for_each_pack<T>(b, n, vec, acc);
@@ -126,6 +131,8 @@ struct SetOp {
 
 template <class TO, class TI>
 __global__ void k_copy(TO* __restrict__ y, const TI* __restrict__ x, size_t n) {
+  grid_dep_launch();
+  grid_dep_wait();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
     y[i] = (TO)x[i];
@@ -150,6 +157,8 @@ struct CopyOp {
 // sci_psykal_light_mod.f90:218-265), the product is then formed in X's kind.
 template <class T, class TY>
 __global__ void k_axpy(T* __restrict__ x, const TY* __restrict__ y, size_t n, Sc b) {
+  grid_dep_launch();
+  grid_dep_wait();
   const T bv = (T)sc_eval(b);
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
@@ -246,6 +255,8 @@ struct ScaleOp {
 template <class T>
 __global__ void k_divide(T* __restrict__ z, const T* __restrict__ x, const T* __restrict__ y,
                          size_t n) {
+  grid_dep_launch();
+  grid_dep_wait();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
     z[i] = x[i] / y[i];
@@ -485,8 +496,8 @@ static void same_kind(lfg_field a, lfg_field b, const char* what) {
 template <class T, class Op>
 void launch_ew(lfg_ctx c, const Op& op, size_t n, bool vec, const char* what, int words) {
   const size_t work = vec ? n / kVec<T> + n % kVec<T> : n;
-  k_ew<T, Op><<<occ_grid(c, (const void*)k_ew<T, Op>, kThreads, work), kThreads, 0, c->stream>>>(
-      op, n, vec);
+  launch_pdl(c, k_ew<T, Op>, occ_grid(c, (const void*)k_ew<T, Op>, kThreads, work), kThreads, 0,
+             op, n, vec);
   after_launch(c, what, (uint64_t)words * n * sizeof(T));
 }
 
@@ -499,7 +510,7 @@ void launch_ewr(lfg_ctx c, const Op& op, size_t n, bool vec, int slot, const cha
   const int g = std::min(occ_grid(c, (const void*)k_ewr<T, Op>, kThreads, work), kMaxRedBlocks);
   Red r = c->red(slot);
   if (out) r.result = out;
-  k_ewr<T, Op><<<g, kThreads, 0, c->stream>>>(op, n, vec, r);
+  launch_pdl(c, k_ewr<T, Op>, g, kThreads, 0, op, n, vec, r);
   after_launch(c, what, (uint64_t)words * n * sizeof(T));
 }
 
@@ -524,9 +535,11 @@ void vec_copy(lfg_field dst, lfg_field src) {
   }
   const int g = c->stream_grid(dst->n());
   if (dst->kind == LFG_R_DOUBLE)
-    k_copy<double, float><<<g, kThreads, 0, c->stream>>>((double*)dst->d, (const float*)src->d, dst->n());
+    launch_pdl(c, k_copy<double, float>, g, kThreads, 0, (double*)dst->d, (const float*)src->d,
+               dst->n());
   else
-    k_copy<float, double><<<g, kThreads, 0, c->stream>>>((float*)dst->d, (const double*)src->d, dst->n());
+    launch_pdl(c, k_copy<float, double>, g, kThreads, 0, (float*)dst->d, (const double*)src->d,
+               dst->n());
   after_launch(c, "copy", (uint64_t)dst->n() * (dst->kind + src->kind));
 }
 
@@ -541,9 +554,11 @@ void vec_axpy(lfg_field x, Sc b, lfg_field y) {
   }
   const int g = c->stream_grid(x->n());
   if (x->kind == LFG_R_DOUBLE)
-    k_axpy<double, float><<<g, kThreads, 0, c->stream>>>((double*)x->d, (const float*)y->d, x->n(), b);
+    launch_pdl(c, k_axpy<double, float>, g, kThreads, 0, (double*)x->d, (const float*)y->d,
+               x->n(), b);
   else
-    k_axpy<float, double><<<g, kThreads, 0, c->stream>>>((float*)x->d, (const double*)y->d, x->n(), b);
+    launch_pdl(c, k_axpy<float, double>, g, kThreads, 0, (float*)x->d, (const double*)y->d,
+               x->n(), b);
   after_launch(c, "axpy", (uint64_t)x->n() * (2 * x->kind + y->kind));
 }
 
@@ -575,8 +590,8 @@ void vec_divide(lfg_field z, lfg_field x, lfg_field y) {
   same_kind(z, y, "X_divideby_Y");
   lfg_ctx c = z->ctx;
   DISPATCH_KIND(z->kind, T,
-                k_divide<T><<<c->stream_grid(z->n()), kThreads, 0, c->stream>>>(
-                    (T*)z->d, (const T*)x->d, (const T*)y->d, z->n()));
+                launch_pdl(c, k_divide<T>, c->stream_grid(z->n()), kThreads, 0, (T*)z->d,
+                           (const T*)x->d, (const T*)y->d, z->n()));
   after_launch(c, "divide", (uint64_t)3 * z->n() * z->kind);
 }
 
@@ -732,6 +747,7 @@ int lfg_ctx_create(int device, lfg_ctx* out) {
   int st = guard(c, [&] {
     LFG_CUDA(cudaSetDevice(device));
     c->device = device;
+    c->pdl = std::getenv("LFG_NO_PDL") == nullptr;
     LFG_CUDA(cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device));
     LFG_CUDA(cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking));
     c->stream = c->own_stream;

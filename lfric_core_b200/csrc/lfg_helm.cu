@@ -172,6 +172,8 @@ template <class T, bool RESID, bool DOT, bool HASW, bool CF>
 __global__ void __launch_bounds__(256) k_helm_apply(HelmArgs<T> A, const T* __restrict__ x,
                                                     const T* __restrict__ b, T* __restrict__ y,
                                                     const T* __restrict__ w, Red r) {
+  grid_dep_launch();
+  grid_dep_wait();
   const unsigned N = A.ncol;
   const int nchunk = (A.nl + KC - 1) / KC;
   const unsigned total = N * (unsigned)nchunk;
@@ -213,6 +215,8 @@ __global__ void k_helm_factor(const T* __restrict__ sub, const T* __restrict__ d
 template <class T, bool CF>
 __global__ void __launch_bounds__(256) k_helm_rhs(HelmArgs<T> A, const T* __restrict__ xin,
                                                   const T* __restrict__ b, T* __restrict__ r) {
+  grid_dep_launch();
+  grid_dep_wait();
   const unsigned N = A.ncol;
   const int nchunk = (A.nl + KC - 1) / KC;
   const unsigned total = N * (unsigned)nchunk;
@@ -239,6 +243,8 @@ __global__ void __launch_bounds__(128) k_helm_subst(
     int ncol, int nl, const T* __restrict__ r, const T* __restrict__ sub,
     const T* __restrict__ inv, const T* __restrict__ cp, const T* __restrict__ xin, T omega,
     T* __restrict__ xout) {
+  grid_dep_launch();
+  grid_dep_wait();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* sd = reinterpret_cast<T*>(smem_raw);     // [nl][blockDim]
   const int t = threadIdx.x, bs = blockDim.x;
@@ -376,6 +382,8 @@ __global__ void __launch_bounds__(256) k_helm_resid_restrict(HelmArgs<T> A,
                                                              T* __restrict__ bc,
                                                              const int* __restrict__ child,
                                                              int ncoarse, int nq) {
+  grid_dep_launch();
+  grid_dep_wait();
   const unsigned NC = ncoarse;
   const int nchunk = (A.nl + KR - 1) / KR;
   const unsigned total = NC * (unsigned)nchunk;
@@ -605,6 +613,8 @@ __global__ void __launch_bounds__(256) k_helm_panel(HelmArgs<T> A, PanelArgs P,
                                                     const T* __restrict__ x,
                                                     const T* __restrict__ b, T* __restrict__ y,
                                                     const T* __restrict__ w, Red r) {
+  grid_dep_launch();
+  grid_dep_wait();
   constexpr int V = PanelShape<T>::V, KL = PanelShape<T>::KL;
   constexpr unsigned SPLIT = kPanelMargin / V;
   const unsigned n = P.n;
@@ -643,6 +653,8 @@ __global__ void __launch_bounds__(256) k_helm_resid_restrict_panel(
     HelmArgs<T> A, PanelArgs P, const T* __restrict__ x, const T* __restrict__ b,
     T* __restrict__ bc, const int* __restrict__ child, int ncoarse, unsigned long long qpos,
     const int* __restrict__ cedge, int ncedge) {
+  grid_dep_launch();
+  grid_dep_wait();
   const unsigned N = A.ncol, nf = P.n, nc = nf / 2, NC = ncoarse;
   const int nl = A.nl;
   const size_t plane = (size_t)nl * N;
@@ -721,6 +733,8 @@ constexpr int KP = 4;
 template <class T>
 __global__ void k_prolong_add(T* __restrict__ fine, const T* __restrict__ coarse,
                               const int* __restrict__ parent, int nfine, int ncoarse, int nl) {
+  grid_dep_launch();
+  grid_dep_wait();
   const size_t nblk = (size_t)nfine * ((nl + KP - 1) / KP);
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < nblk;
        t += (size_t)gridDim.x * blockDim.x) {
@@ -800,6 +814,8 @@ template <class T, bool XIN, int S, bool CF>
 __global__ void __launch_bounds__(128) k_helm_sweep_seg(HelmArgs<T> A, const T* __restrict__ b,
                                                         const T* __restrict__ xin, T omega,
                                                         T* __restrict__ xout) {
+  grid_dep_launch();
+  grid_dep_wait();
   constexpr int LMAX = kSegLevels;
   const int tid = threadIdx.x, j = tid % S;
   const unsigned c = blockIdx.x * (128 / S) + tid / S;
@@ -916,10 +932,10 @@ void launch_sweep_seg(lfg_ctx c, int S, HelmArgs<T> A, const T* b, const T* xin,
   auto go = [&](auto cf) {
     constexpr bool CF = decltype(cf)::value;
     switch (S) {
-      case 4: k_helm_sweep_seg<T, XIN, 4, CF><<<grid, 128, 0, c->stream>>>(A, b, xin, omega, xout); break;
-      case 8: k_helm_sweep_seg<T, XIN, 8, CF><<<grid, 128, 0, c->stream>>>(A, b, xin, omega, xout); break;
-      case 16: k_helm_sweep_seg<T, XIN, 16, CF><<<grid, 128, 0, c->stream>>>(A, b, xin, omega, xout); break;
-      default: k_helm_sweep_seg<T, XIN, 32, CF><<<grid, 128, 0, c->stream>>>(A, b, xin, omega, xout); break;
+      case 4: launch_pdl(c, k_helm_sweep_seg<T, XIN, 4, CF>, grid, 128, 0, A, b, xin, omega, xout); break;
+      case 8: launch_pdl(c, k_helm_sweep_seg<T, XIN, 8, CF>, grid, 128, 0, A, b, xin, omega, xout); break;
+      case 16: launch_pdl(c, k_helm_sweep_seg<T, XIN, 16, CF>, grid, 128, 0, A, b, xin, omega, xout); break;
+      default: launch_pdl(c, k_helm_sweep_seg<T, XIN, 32, CF>, grid, 128, 0, A, b, xin, omega, xout); break;
     }
   };
   if (XIN && hwords < 4.0) go(std::true_type{});
@@ -946,8 +962,8 @@ void launch_subst(lfg_ctx c, int ncol, int nl, const T* r, const T* sub, const T
   while ((size_t)nl * bs * sizeof(T) > cap) bs /= 2;
   auto kern = k_helm_subst<T, XIN>;
   ensure_smem_attr((const void*)kern, (int)cap);
-  kern<<<(ncol + bs - 1) / bs, bs, (size_t)nl * bs * sizeof(T), c->stream>>>(
-      ncol, nl, r, sub, inv, cp, xin, omega, xout);
+  launch_pdl(c, kern, (ncol + bs - 1) / bs, bs, (size_t)nl * bs * sizeof(T), ncol, nl, r, sub,
+             inv, cp, xin, omega, xout);
   // r, inv, sub, c' read and x written; x_in with XIN
   after_launch(c, "helm_subst", sizeof(T) * (XIN ? 6 : 5) * (uint64_t)ncol * nl);
 }
@@ -988,8 +1004,8 @@ void launch_panel(lfg_helm op, const T* x, const T* b, T* y, const T* w, Red r) 
   lfg_ctx c = op->ctx;
   auto k = op->hsym ? k_helm_panel<T, MODE, DOT, HASW, true>
                     : k_helm_panel<T, MODE, DOT, HASW, false>;
-  k<<<occ_grid(c, (const void*)k, 256, panel_work<T>(op)), 256, 0, c->stream>>>(
-      args_of<T>(op), panel_args(op), x, b, y, w, r);
+  launch_pdl(c, k, occ_grid(c, (const void*)k, 256, panel_work<T>(op)), 256, 0, args_of<T>(op),
+             panel_args(op), x, b, y, w, r);
 }
 
 // r = b + H_off x (k_helm_rhs, or the panel kernel)
@@ -1001,7 +1017,7 @@ void launch_rhs(lfg_helm op, const T* x, const T* b, T* r) {
     launch_panel<T, M_RHS, false, false>(op, x, b, r, nullptr, Red{nullptr, nullptr, nullptr});
   else {
     auto rk = op->hsym ? k_helm_rhs<T, true> : k_helm_rhs<T, false>;
-    rk<<<occ_grid(c, (const void*)rk, 256, work), 256, 0, c->stream>>>(args_of<T>(op), x, b, r);
+    launch_pdl(c, rk, occ_grid(c, (const void*)rk, 256, work), 256, 0, args_of<T>(op), x, b, r);
   }
   // x, b and the couplings read, r written
   after_launch(c, "helm_rhs",
@@ -1048,7 +1064,7 @@ void launch_apply(lfg_helm op, const T* x, const T* b, T* y, const T* w, Red r) 
   const size_t work = (size_t)op->ncol * ((op->nl + KC - 1) / KC);
   auto k = op->hsym ? k_helm_apply<T, RESID, DOT, HASW, true>
                     : k_helm_apply<T, RESID, DOT, HASW, false>;
-  k<<<occ_grid(c, (const void*)k, bs, work), bs, 0, c->stream>>>(args_of<T>(op), x, b, y, w, r);
+  launch_pdl(c, k, occ_grid(c, (const void*)k, bs, work), bs, 0, args_of<T>(op), x, b, y, w, r);
 }
 
 void check_field(lfg_helm op, lfg_field f, const char* what) {
@@ -1144,15 +1160,16 @@ void helm_residual_restrict(lfg_helm op, lfg_intergrid ig, lfg_field x, lfg_fiel
       auto k = op->hsym ? k_helm_resid_restrict_panel<T, true>
                         : k_helm_resid_restrict_panel<T, false>;
       const lfg_mesh m = op->mesh;
-      k<<<occ_grid(c, (const void*)k, bs, pwork), bs, 0, c->stream>>>(
-          args_of<T>(op), PanelArgs{m->pn, m->proll, nullptr, 0}, (const T*)x->d,
-          (const T*)b->d, (T*)bc->d, ig->child, ig->ncoarse, ig->qpos, ig->cedge, ig->ncedge);
+      launch_pdl(c, k, occ_grid(c, (const void*)k, bs, pwork), bs, 0, args_of<T>(op),
+                 PanelArgs{m->pn, m->proll, nullptr, 0}, (const T*)x->d, (const T*)b->d,
+                 (T*)bc->d, (const int*)ig->child, ig->ncoarse, ig->qpos,
+                 (const int*)ig->cedge, ig->ncedge);
       return;
     }
     auto k = op->hsym ? k_helm_resid_restrict<T, true> : k_helm_resid_restrict<T, false>;
-    k<<<occ_grid(c, (const void*)k, bs, work), bs, 0, c->stream>>>(
-        args_of<T>(op), (const T*)x->d, (const T*)b->d, (T*)bc->d, ig->child, ig->ncoarse,
-        ig->nx * ig->ny);
+    launch_pdl(c, k, occ_grid(c, (const void*)k, bs, work), bs, 0, args_of<T>(op),
+               (const T*)x->d, (const T*)b->d, (T*)bc->d, (const int*)ig->child, ig->ncoarse,
+               ig->nx * ig->ny);
   };
   if (op->kind == LFG_R_DOUBLE) go(double{});
   else go(float{});
@@ -1169,9 +1186,13 @@ void prolong_add(lfg_intergrid ig, lfg_field fine, lfg_field coarse) {
   lfg_ctx c = fine->ctx;
   const size_t work = (size_t)ig->nfine * ((fine->nlev + KP - 1) / KP);
   if (fine->kind == LFG_R_DOUBLE)
-    k_prolong_add<double><<<occ_grid(c, (const void*)k_prolong_add<double>, 256, work), 256, 0, c->stream>>>((double*)fine->d, (const double*)coarse->d, ig->parent, ig->nfine, ig->ncoarse, fine->nlev);
+    launch_pdl(c, k_prolong_add<double>, occ_grid(c, (const void*)k_prolong_add<double>, 256, work),
+               256, 0, (double*)fine->d, (const double*)coarse->d, (const int*)ig->parent,
+               ig->nfine, ig->ncoarse, fine->nlev);
   else
-    k_prolong_add<float><<<occ_grid(c, (const void*)k_prolong_add<float>, 256, work), 256, 0, c->stream>>>((float*)fine->d, (const float*)coarse->d, ig->parent, ig->nfine, ig->ncoarse, fine->nlev);
+    launch_pdl(c, k_prolong_add<float>, occ_grid(c, (const void*)k_prolong_add<float>, 256, work),
+               256, 0, (float*)fine->d, (const float*)coarse->d, (const int*)ig->parent,
+               ig->nfine, ig->ncoarse, fine->nlev);
   after_launch(c, "prolong_add",
                (uint64_t)fine->kind * fine->nlev * (2 * (uint64_t)ig->nfine + ig->ncoarse));
 }

@@ -17,6 +17,7 @@
 #include <stdexcept>
 #include <string>
 #include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "../../include/lfg.h"
@@ -155,6 +156,9 @@ struct lfg_ctx_s {
   // polls of a TMA stage wait before the substitution kernels give up
   // (< 0: their built-in limit); lfg_ctx_test_tma_spin_limit sets it
   long long tma_stage_spins = -1;
+  // launch the multigrid and Helmholtz kernels with programmatic dependent
+  // launch (off when LFG_NO_PDL is set in the environment: a debugging aid)
+  bool pdl = true;
 
   lfg::Red red(int slot) {
     return lfg::Red{red_partials + (size_t)slot * lfg::kMaxRedBlocks, red_counters + slot,
@@ -392,10 +396,10 @@ struct Vec {
 };
 
 // V consecutive values from a V*sizeof(T)-aligned address (8 or 16 bytes:
-// one load); STREAM: evict-first, for arrays read once.  Four-wide FP32
-// loads ignore STREAM: the FP32 panel kernels measured faster with plain
-// loads (C192x70: sweep right-hand side 76 against 83 us, apply 104
-// against 107 us).
+// one load); STREAM: evict-first, for arrays read once.  FP32 vectors
+// ignore STREAM: the FP32 panel kernels measured faster with plain loads
+// (C192x70: sweep right-hand side 76 against 83 us, apply 104 against 107
+// us, residual + restriction 114 against 127 us).
 template <bool STREAM, class T, int V>
 __device__ __forceinline__ Vec<T, V> vld(const T* p) {
   Vec<T, V> r;
@@ -403,8 +407,7 @@ __device__ __forceinline__ Vec<T, V> vld(const T* p) {
     const float4 q = *reinterpret_cast<const float4*>(p);
     r.e[0] = q.x; r.e[1] = q.y; r.e[2] = q.z; r.e[3] = q.w;
   } else if constexpr (std::is_same_v<T, float> && V == 2) {
-    const float2 q = STREAM ? __ldcs(reinterpret_cast<const float2*>(p))
-                            : *reinterpret_cast<const float2*>(p);
+    const float2 q = *reinterpret_cast<const float2*>(p);
     r.e[0] = q.x; r.e[1] = q.y;
   } else if constexpr (std::is_same_v<T, double> && V == 2) {
     const double2 q = STREAM ? __ldcs(reinterpret_cast<const double2*>(p))
@@ -433,6 +436,37 @@ __device__ __forceinline__ void vst(T* p, const Vec<T, V>& v) {
     *reinterpret_cast<double2*>(p) = make_double2(v.e[0], v.e[1]);
   else
     p[0] = v.e[0];
+}
+
+// ------------------------------------------- programmatic dependent launch
+// A kernel launched by launch_pdl may begin launching while the kernel
+// before it in the stream is still running (its blocks take the SM slots
+// the earlier kernel leaves); it must call grid_dep_wait() before its first
+// access to global memory, which returns once the earlier kernel has
+// finished and its writes are visible.  grid_dep_launch() lets the next
+// such kernel start launching.  Only kernels that call grid_dep_wait() at
+// their top are launched this way.
+__device__ __forceinline__ void grid_dep_wait() {
+  asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+__device__ __forceinline__ void grid_dep_launch() {
+  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
+template <class... KArgs, class... Args>
+void launch_pdl(lfg_ctx c, void (*kern)(KArgs...), dim3 grid, dim3 block, size_t smem,
+                Args&&... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = c->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = c->pdl ? 1 : 0;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  LFG_CUDA(cudaLaunchKernelEx(&cfg, kern, std::forward<Args>(args)...));
 }
 
 // Columns at each end of a panel row that the element-parallel panel

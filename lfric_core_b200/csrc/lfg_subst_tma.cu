@@ -102,6 +102,8 @@ template <bool XIN>
 __global__ void __launch_bounds__(TC) k_subst_tma(const __grid_constant__ TmaMaps maps, int ncol,
                                                   int nl, float omega, float* __restrict__ xout,
                                                   unsigned* err, long long stage_spins) {
+  grid_dep_launch();
+  grid_dep_wait();
   extern __shared__ __align__(128) unsigned char smem[];
   float* stage = reinterpret_cast<float*>(smem);                       // [NST][NARR][KCH][TC]
   float* sd = stage + NST * NARR * KCH * TC;                           // [nl][TC]
@@ -212,6 +214,8 @@ template <class T, bool XIN, int NCH>
 __global__ void __launch_bounds__(tile_cols<T>(), 3)
     k_subst_tma_reg(const __grid_constant__ TmaMaps maps, int ncol, int nl, T omega,
                     T* __restrict__ xout, unsigned* err, long long stage_spins) {
+  grid_dep_launch();
+  grid_dep_wait();
   constexpr int TCT = tile_cols<T>();
   extern __shared__ __align__(128) unsigned char smem[];
   T* stage = reinterpret_cast<T*>(smem);  // [NST][NARR][KCH][TCT]
@@ -405,7 +409,17 @@ void launch_reg(lfg_ctx c, const TmaMaps& maps, int ncol, int nl, bool xin, T om
   unsigned* err = c->dev_err;
   long long spins = stage_spins(c);
   void* args[] = {&m, &nc, &nlv, &om, &xo, &err, &spins};
-  LFG_CUDA(cudaLaunchKernel(kern, dim3(grid), dim3(TCT), args, smem, c->stream));
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(grid);
+  cfg.blockDim = dim3(TCT);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = c->stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  attr[0].val.programmaticStreamSerializationAllowed = c->pdl ? 1 : 0;
+  cfg.attrs = attr;
+  cfg.numAttrs = 1;
+  LFG_CUDA(cudaLaunchKernelExC(&cfg, kern, args));
   // r, inv, sub, c' read and x written, x_in read when given
   after_launch(c, "helm_subst_tma", sizeof(T) * (uint64_t)ncol * nl * (xin ? 6 : 5));
 }
@@ -441,11 +455,11 @@ void subst_tma(lfg_ctx c, int ncol, int nl, const float* r, const float* sub, co
   const int ntile = (ncol + TC - 1) / TC;
   const int grid = std::max(1, std::min(ntile, c->num_sms * std::max(per_sm, 1)));
   if (xin)
-    k_subst_tma<true><<<grid, TC, smem, c->stream>>>(maps, ncol, nl, omega, xout, c->dev_err,
-                                                     stage_spins(c));
+    launch_pdl(c, k_subst_tma<true>, grid, TC, smem, maps, ncol, nl, omega, xout, c->dev_err,
+               stage_spins(c));
   else
-    k_subst_tma<false><<<grid, TC, smem, c->stream>>>(maps, ncol, nl, omega, xout, c->dev_err,
-                                                      stage_spins(c));
+    launch_pdl(c, k_subst_tma<false>, grid, TC, smem, maps, ncol, nl, omega, xout, c->dev_err,
+               stage_spins(c));
   after_launch(c, "helm_subst_tma", sizeof(float) * (uint64_t)ncol * nl * (xin ? 6 : 5));
 }
 

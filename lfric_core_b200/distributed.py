@@ -250,27 +250,28 @@ class LibrarySpace:
         def pack(f, c):
             buf = torch.empty(len(c) * self.nl, dtype=torch.float64, device=dev)
             ctx.check(ctx.lib.lfg_field_pack_columns(
-                f.h, api.C.c_void_p(self._dev_cols(c).data_ptr()), len(c),
-                api.C.c_void_p(buf.data_ptr())), "pack_columns")
+                f.h, self._cols_ptr(c), len(c), api.C.c_void_p(buf.data_ptr())), "pack_columns")
             return buf
 
         def unpack(f, c, buf):
             ctx.check(ctx.lib.lfg_field_unpack_columns(
-                f.h, api.C.c_void_p(self._dev_cols(c).data_ptr()), len(c),
-                api.C.c_void_p(buf.data_ptr())), "unpack_columns")
+                f.h, self._cols_ptr(c), len(c), api.C.c_void_p(buf.data_ptr())),
+                "unpack_columns")
 
         def new_buffer(f, c):
             return torch.empty(len(c) * self.nl, dtype=torch.float64, device=dev)
 
         self.exchange = HaloExchange(self.plan, pack, unpack, new_buffer, group)
 
-    def _dev_cols(self, c):
-        """The plan's column list c on the device (made once per list)."""
+    def _cols_ptr(self, c):
+        """The plan's column list c on the device (made once per list), as
+        the int pointer the C ABI takes."""
         import torch
         key = c.ctypes.data
         if key not in self._devcols:
             self._devcols[key] = torch.tensor(c, dtype=torch.int32, device=self.device)
-        return self._devcols[key]
+        C = self.api.C
+        return C.cast(self._devcols[key].data_ptr(), C.POINTER(C.c_int))
 
     # vector space ---------------------------------------------------------
     def new(self):

@@ -24,13 +24,14 @@ def test_halo_pack_unpack_zero(ctx):
     cols = np.array([5, 0, 299, 17, 18], dtype=np.int32)
     dcols = torch.tensor(cols, device="cuda")
     buf = torch.empty(cols.size * nl, dtype=torch.float64, device="cuda")
-    ctx.check(ctx.lib.lfg_field_pack_columns(F.h, C.c_void_p(dcols.data_ptr()), cols.size,
+    ip = C.cast(dcols.data_ptr(), C.POINTER(C.c_int))
+    ctx.check(ctx.lib.lfg_field_pack_columns(F.h, ip, int(cols.size),
                                              C.c_void_p(buf.data_ptr())))
     ctx.synchronize()
     vv = v.reshape(ncol, nl)
     assert np.array_equal(buf.cpu().numpy().reshape(nl, cols.size), vv[cols].T)
     G = Field(ctx, R_DOUBLE, ncol, nl)
-    ctx.check(ctx.lib.lfg_field_unpack_columns(G.h, C.c_void_p(dcols.data_ptr()), cols.size,
+    ctx.check(ctx.lib.lfg_field_unpack_columns(G.h, ip, int(cols.size),
                                                C.c_void_p(buf.data_ptr())))
     g = G.export().reshape(ncol, nl)
     assert np.array_equal(g[cols], vv[cols])
