@@ -390,7 +390,10 @@ __global__ void k_cma_app(const T* __restrict__ bands, const int* __restrict__ i
 // The same with V adjacent columns per thread (16-byte loads and stores of
 // the bands, x and lhs), for fields whose rows start on 16-byte boundaries;
 // the same operations in the same order as k_cma_app.
-template <class T, int V>
+// TRI: the W3 -> W3 tridiagonal with identity row and column maps
+// (alpha = beta = gamma_m = gamma_p = 1, bandwidth 3), whose band columns
+// i-1, i, i+1 and rows follow from i without reading the index maps.
+template <class T, int V, bool TRI>
 __global__ void k_cma_app_v(const T* __restrict__ bands, const int* __restrict__ ind_to,
                             const int* __restrict__ ind_from, const int* __restrict__ jminus,
                             const int* __restrict__ jplus, int ncol, int nrow, int ncolumn,
@@ -399,13 +402,13 @@ __global__ void k_cma_app_v(const T* __restrict__ bands, const int* __restrict__
   const int i = blockIdx.y;
   if (c >= ncol) return;
   const size_t N = ncol, plane = (size_t)nrow * N;
-  const int jm = jminus[i];
-  const int jlo = max(0, jm), jhi = min(ncolumn - 1, jplus[i]);
-  const size_t o = (size_t)ind_to[i] * N + c;
+  const int jm = TRI ? i - 1 : jminus[i];
+  const int jlo = max(0, jm), jhi = min(ncolumn - 1, TRI ? i + 1 : jplus[i]);
+  const size_t o = (size_t)(TRI ? i : ind_to[i]) * N + c;
   Vec<T, V> acc = vld<false, T, V>(lhs + o);
   for (int j = jlo; j <= jhi; ++j) {
     const Vec<T, V> a = vld<true, T, V>(bands + (size_t)(j - jm) * plane + (size_t)i * N + c);
-    const Vec<T, V> xv = vld<false, T, V>(x + (size_t)ind_from[j] * N + c);
+    const Vec<T, V> xv = vld<false, T, V>(x + (size_t)(TRI ? j : ind_from[j]) * N + c);
 #pragma unroll
     for (int v = 0; v < V; ++v) acc.e[v] = acc.e[v] + a.e[v] * xv.e[v];
   }
@@ -653,6 +656,8 @@ int lfg_cma_create(lfg_ctx c, int kind, int ncol, int nrow, int ncolumn, int bw,
     m->max_ind_from = max_from;
     m->ind_identity = true;
     for (int i = 0; i < nrow; ++i) m->ind_identity &= ind_to[i] == i + 1;
+    m->ind_from_identity = true;
+    for (int j = 0; j < ncolumn; ++j) m->ind_from_identity &= ind_from[j] == j + 1;
     const size_t n = (size_t)bw * nrow * ncol;
     std::vector<double> dev(n);
     for (int col = 0; col < ncol; ++col)
@@ -720,14 +725,17 @@ int lfg_cma_apply(lfg_cma m, lfg_field lhs, lfg_field x) {
     const int V = 16 / m->kind;
     const bool vec = m->ncol % V == 0 && reinterpret_cast<uintptr_t>(x->d) % 16 == 0 &&
                      reinterpret_cast<uintptr_t>(lhs->d) % 16 == 0;
+    bool tri = m->bw == 3 && m->alpha == 1 && m->beta == 1 && m->gm == 1 && m->gp == 1 &&
+               m->nrow == m->ncolumn && m->ind_identity && m->ind_from_identity;
     dispatch(m->kind, [&](auto tag) {
       using T = decltype(tag);
       if (vec) {
         constexpr int VT = 16 / sizeof(T);
         dim3 grid((m->ncol / VT + 127) / 128, m->nrow);
-        k_cma_app_v<T, VT><<<grid, 128, 0, c->stream>>>(
-            (const T*)m->bands, m->ind_to, m->ind_from, m->jminus, m->jplus, m->ncol, m->nrow,
-            m->ncolumn, (const T*)x->d, (T*)lhs->d);
+        auto k = tri ? k_cma_app_v<T, VT, true> : k_cma_app_v<T, VT, false>;
+        k<<<grid, 128, 0, c->stream>>>((const T*)m->bands, m->ind_to, m->ind_from, m->jminus,
+                                       m->jplus, m->ncol, m->nrow, m->ncolumn, (const T*)x->d,
+                                       (T*)lhs->d);
       } else {
         dim3 grid((m->ncol + 127) / 128, m->nrow);
         k_cma_app<T><<<grid, 128, 0, c->stream>>>((const T*)m->bands, m->ind_to, m->ind_from,

@@ -92,7 +92,6 @@ __device__ __forceinline__ void for_each_pack(const Op& op, size_t n, bool vec, 
 
 template <class T, class Op>
 __global__ void k_ew(Op op, size_t n, bool vec) {
-  grid_dep_launch();
   grid_dep_wait();
   double acc = 0.0;
   const auto b = op.bind();
@@ -101,7 +100,6 @@ __global__ void k_ew(Op op, size_t n, bool vec) {
 
 template <class T, class Op>
 __global__ void k_ewr(Op op, size_t n, bool vec, Red r) {
-  grid_dep_launch();
   grid_dep_wait();
   double acc = 0.0;
   const auto b = op.bind();
@@ -131,7 +129,6 @@ struct SetOp {
 
 template <class TO, class TI>
 __global__ void k_copy(TO* __restrict__ y, const TI* __restrict__ x, size_t n) {
-  grid_dep_launch();
   grid_dep_wait();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)
@@ -157,7 +154,6 @@ struct CopyOp {
 // sci_psykal_light_mod.f90:218-265), the product is then formed in X's kind.
 template <class T, class TY>
 __global__ void k_axpy(T* __restrict__ x, const TY* __restrict__ y, size_t n, Sc b) {
-  grid_dep_launch();
   grid_dep_wait();
   const T bv = (T)sc_eval(b);
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
@@ -255,7 +251,6 @@ struct ScaleOp {
 template <class T>
 __global__ void k_divide(T* __restrict__ z, const T* __restrict__ x, const T* __restrict__ y,
                          size_t n) {
-  grid_dep_launch();
   grid_dep_wait();
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < n;
        i += (size_t)gridDim.x * blockDim.x)

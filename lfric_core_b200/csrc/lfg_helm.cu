@@ -172,7 +172,6 @@ template <class T, bool RESID, bool DOT, bool HASW, bool CF>
 __global__ void __launch_bounds__(256) k_helm_apply(HelmArgs<T> A, const T* __restrict__ x,
                                                     const T* __restrict__ b, T* __restrict__ y,
                                                     const T* __restrict__ w, Red r) {
-  grid_dep_launch();
   grid_dep_wait();
   const unsigned N = A.ncol;
   const int nchunk = (A.nl + KC - 1) / KC;
@@ -215,7 +214,6 @@ __global__ void k_helm_factor(const T* __restrict__ sub, const T* __restrict__ d
 template <class T, bool CF>
 __global__ void __launch_bounds__(256) k_helm_rhs(HelmArgs<T> A, const T* __restrict__ xin,
                                                   const T* __restrict__ b, T* __restrict__ r) {
-  grid_dep_launch();
   grid_dep_wait();
   const unsigned N = A.ncol;
   const int nchunk = (A.nl + KC - 1) / KC;
@@ -243,7 +241,6 @@ __global__ void __launch_bounds__(128) k_helm_subst(
     int ncol, int nl, const T* __restrict__ r, const T* __restrict__ sub,
     const T* __restrict__ inv, const T* __restrict__ cp, const T* __restrict__ xin, T omega,
     T* __restrict__ xout) {
-  grid_dep_launch();
   grid_dep_wait();
   extern __shared__ __align__(16) unsigned char smem_raw[];
   T* sd = reinterpret_cast<T*>(smem_raw);     // [nl][blockDim]
@@ -382,7 +379,6 @@ __global__ void __launch_bounds__(256) k_helm_resid_restrict(HelmArgs<T> A,
                                                              T* __restrict__ bc,
                                                              const int* __restrict__ child,
                                                              int ncoarse, int nq) {
-  grid_dep_launch();
   grid_dep_wait();
   const unsigned NC = ncoarse;
   const int nchunk = (A.nl + KR - 1) / KR;
@@ -613,7 +609,6 @@ __global__ void __launch_bounds__(256) k_helm_panel(HelmArgs<T> A, PanelArgs P,
                                                     const T* __restrict__ x,
                                                     const T* __restrict__ b, T* __restrict__ y,
                                                     const T* __restrict__ w, Red r) {
-  grid_dep_launch();
   grid_dep_wait();
   constexpr int V = PanelShape<T>::V, KL = PanelShape<T>::KL;
   constexpr unsigned SPLIT = kPanelMargin / V;
@@ -653,7 +648,6 @@ __global__ void __launch_bounds__(256) k_helm_resid_restrict_panel(
     HelmArgs<T> A, PanelArgs P, const T* __restrict__ x, const T* __restrict__ b,
     T* __restrict__ bc, const int* __restrict__ child, int ncoarse, unsigned long long qpos,
     const int* __restrict__ cedge, int ncedge) {
-  grid_dep_launch();
   grid_dep_wait();
   const unsigned N = A.ncol, nf = P.n, nc = nf / 2, NC = ncoarse;
   const int nl = A.nl;
@@ -733,7 +727,6 @@ constexpr int KP = 4;
 template <class T>
 __global__ void k_prolong_add(T* __restrict__ fine, const T* __restrict__ coarse,
                               const int* __restrict__ parent, int nfine, int ncoarse, int nl) {
-  grid_dep_launch();
   grid_dep_wait();
   const size_t nblk = (size_t)nfine * ((nl + KP - 1) / KP);
   for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < nblk;
@@ -814,7 +807,6 @@ template <class T, bool XIN, int S, bool CF>
 __global__ void __launch_bounds__(128) k_helm_sweep_seg(HelmArgs<T> A, const T* __restrict__ b,
                                                         const T* __restrict__ xin, T omega,
                                                         T* __restrict__ xout) {
-  grid_dep_launch();
   grid_dep_wait();
   constexpr int LMAX = kSegLevels;
   const int tid = threadIdx.x, j = tid % S;

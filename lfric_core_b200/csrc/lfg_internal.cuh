@@ -260,7 +260,8 @@ struct lfg_cma_s {
   int* jminus = nullptr;      // [nrow] first band column of each row (0-based)
   int* jplus = nullptr;       // [nrow] last band column of each row
   int max_ind_to = 0, max_ind_from = 0;  // largest 1-based column offsets
-  bool ind_identity = false;  // ind_to(i) = i for every row (W3 -> W3 style maps)
+  bool ind_identity = false;       // ind_to(i) = i for every row (W3 -> W3 style maps)
+  bool ind_from_identity = false;  // ind_from(j) = j for every column
   int* tptr = nullptr;        // [ncolumn+1] rows reaching each column (transpose)
   int* trow = nullptr;
   // Thomas factors of a square tridiagonal operator (columnwise_op_appinv's
@@ -439,18 +440,17 @@ __device__ __forceinline__ void vst(T* p, const Vec<T, V>& v) {
 }
 
 // ------------------------------------------- programmatic dependent launch
-// A kernel launched by launch_pdl may begin launching while the kernel
-// before it in the stream is still running (its blocks take the SM slots
-// the earlier kernel leaves); it must call grid_dep_wait() before its first
-// access to global memory, which returns once the earlier kernel has
-// finished and its writes are visible.  grid_dep_launch() lets the next
-// such kernel start launching.  Only kernels that call grid_dep_wait() at
-// their top are launched this way.
+// A kernel launched by launch_pdl may begin launching as soon as every block
+// of the kernel before it in the stream has exited, before that kernel's
+// completion has been signalled; it must call grid_dep_wait() before its
+// first access to global memory, which returns once the earlier kernel has
+// finished and its writes are visible.  Only kernels that call
+// grid_dep_wait() at their top are launched this way.  (No kernel here
+// signals its dependents early: letting a kernel's successor launch while
+// the kernel itself still waited on its own predecessor filled the SMs with
+// waiting blocks and halved the solve rate.)
 __device__ __forceinline__ void grid_dep_wait() {
   asm volatile("griddepcontrol.wait;" ::: "memory");
-}
-__device__ __forceinline__ void grid_dep_launch() {
-  asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
 }
 
 template <class... KArgs, class... Args>

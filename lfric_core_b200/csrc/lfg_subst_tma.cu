@@ -102,7 +102,6 @@ template <bool XIN>
 __global__ void __launch_bounds__(TC) k_subst_tma(const __grid_constant__ TmaMaps maps, int ncol,
                                                   int nl, float omega, float* __restrict__ xout,
                                                   unsigned* err, long long stage_spins) {
-  grid_dep_launch();
   grid_dep_wait();
   extern __shared__ __align__(128) unsigned char smem[];
   float* stage = reinterpret_cast<float*>(smem);                       // [NST][NARR][KCH][TC]
@@ -214,7 +213,6 @@ template <class T, bool XIN, int NCH>
 __global__ void __launch_bounds__(tile_cols<T>(), 3)
     k_subst_tma_reg(const __grid_constant__ TmaMaps maps, int ncol, int nl, T omega,
                     T* __restrict__ xout, unsigned* err, long long stage_spins) {
-  grid_dep_launch();
   grid_dep_wait();
   constexpr int TCT = tile_cols<T>();
   extern __shared__ __align__(128) unsigned char smem[];
