@@ -339,12 +339,14 @@ def measure_configs(ctx, stream, steps: int, peak: float, cpu: bool) -> dict:
     flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
 
     def gpu_ms_cold(fn, n):
-        """Each launch timed alone after a 256 MB write has replaced L2
-        (for inputs smaller than L2)."""
+        """Each launch timed alone after a 256 MB read has replaced L2 (for
+        inputs smaller than L2; a read leaves no dirty lines for the timed
+        launch to write back)."""
         ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
               for _ in range(n)]
+        sink = torch.empty(1, dtype=torch.int64, device="cuda")
         for a, b in ev:
-            flush_buf.zero_()
+            torch.sum(flush_buf, dtype=torch.int64, out=sink)
             a.record(stream)
             fn()
             b.record(stream)
@@ -424,7 +426,7 @@ def measure_configs(ctx, stream, steps: int, peak: float, cpu: bool) -> dict:
     msref = gpu_ms(refine, 10)
     x64, xr = X.export(), X2.export()
     c2 = {"workload": "C96x70 W3 tridiagonal (diagonal ratio U(1.5,3)), seeded rhs; solves "
-                      "timed alone after an L2-replacing write",
+                      "timed alone after an L2-replacing read",
           "ndof": n,
           "fp64_solve": {"us": ms64 * 1e3, "algorithmic_bytes": 5 * n * 8,
                          "GB/s": 5 * n * 8 / (ms64 * 1e-3) / 1e9,
@@ -558,25 +560,10 @@ def measure_kernels(ctx, stream, peak: float) -> list:
     from lfric_core_b200.problems import helmholtz_problem, w0_problem
     rows = []
 
-    flush_buf = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
-
-    def time(fn, n=20, flush=False):
-        """Mean launch time over n launches.  flush: the inputs fit in L2
-        (126 MB), so L2 is overwritten (a 256 MB write) before every launch
-        and each launch is timed alone between its own events."""
+    def time(fn, n=20):
         for _ in range(3):
             fn()
         torch.cuda.synchronize()
-        if flush:
-            ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
-                  for _ in range(n)]
-            for a, b in ev:
-                flush_buf.zero_()
-                a.record(stream)
-                fn()
-                b.record(stream)
-            torch.cuda.synchronize()
-            return sum(a.elapsed_time(b) for a, b in ev) / n
         e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         e0.record(stream)
         for _ in range(n):
@@ -630,25 +617,27 @@ def measure_kernels(ctx, stream, peak: float) -> list:
         (N + nc * NLAYERS) * 8, time(lambda: ig.restrict(api.RESTRICT_MASS_W3, Cc, F)))
     add("k_prolong (prolong_scalar_unweighted)", f"C{N_FINE // 2}->C{N_FINE}x{NLAYERS} FP64",
         (2 * N + nc * NLAYERS) * 8, time(lambda: ig.prolong(F, Cc)))
-    # CMA tridiagonal on C96 x 70 (W3 -> W3): app and appinv
-    n96 = 6 * 96 * 96
+    # CMA tridiagonal (W3 -> W3) app and appinv on C192 x 70, whose arrays
+    # are larger than L2 (the C96 line solve of config 2 is timed with L2
+    # replaced before each launch in the bench line)
+    ncma = 6 * N_FINE * N_FINE
     rng = np.random.default_rng(2)
-    sub = -rng.random((n96, NLAYERS))
-    sup = -rng.random((n96, NLAYERS))
-    diag = (np.abs(sub) + np.abs(sup)) * (1.5 + 1.5 * rng.random((n96, NLAYERS)))
+    sub = -rng.random((ncma, NLAYERS))
+    sup = -rng.random((ncma, NLAYERS))
+    diag = (np.abs(sub) + np.abs(sup)) * (1.5 + 1.5 * rng.random((ncma, NLAYERS)))
     cm = np.stack([sub, diag, sup], axis=-1).ravel()
     ind = np.arange(1, NLAYERS + 1)
     for kind, w, tag in ((R_DOUBLE, 8, "FP64"), (R_SINGLE, 4, "FP32")):
-        A = api.ColumnwiseOperator(ctx, kind, n96, NLAYERS, NLAYERS, 3, 1, 1, 1, 1, ind, ind, cm)
-        X = Field(ctx, kind, n96, NLAYERS)
-        Y = Field(ctx, kind, n96, NLAYERS)
+        A = api.ColumnwiseOperator(ctx, kind, ncma, NLAYERS, NLAYERS, 3, 1, 1, 1, 1, ind, ind, cm)
+        X = Field(ctx, kind, ncma, NLAYERS)
+        Y = Field(ctx, kind, ncma, NLAYERS)
         X.set_scalar(1.0)
         Y.set_scalar(0.0)
-        n = n96 * NLAYERS
-        add("k_cma_app_v (columnwise_op_app, L2 flushed)", f"C96x{NLAYERS} {tag}", 6 * n * w,
-            time(lambda: A.apply(Y, X), flush=True))
-        add("k_subst_tma_reg (columnwise_op_appinv, L2 flushed)", f"C96x{NLAYERS} {tag}", 5 * n * w,
-            time(lambda: A.apply_inverse(Y, X), flush=True))
+        n = ncma * NLAYERS
+        add("k_cma_app_v (columnwise_op_app)", f"C{N_FINE}x{NLAYERS} {tag}", 6 * n * w,
+            time(lambda: A.apply(Y, X)))
+        add("k_subst_tma_reg (columnwise_op_appinv)", f"C{N_FINE}x{NLAYERS} {tag}", 5 * n * w,
+            time(lambda: A.apply_inverse(Y, X)))
         del A, X, Y
     # LMA W0 apply (matrix_vector, gather form) on the C48 x 30 W0 problem
     wp = w0_problem(48, 30, seed=4, top=30e3)
