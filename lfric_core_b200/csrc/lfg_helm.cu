@@ -642,9 +642,11 @@ __global__ void __launch_bounds__(256) k_helm_panel(HelmArgs<T> A, PanelArgs P,
 // The children's residuals are summed in the cell map's slot order (the
 // per-panel placement qpos), as the per-coarse-column code does; the
 // coarse border columns (cedge) run that code, one level each, in the
-// threads just before the same level's interior ones.
+// threads just before the same level's interior ones.  Four blocks per SM
+// (64 registers a thread): the extra resident warps hide more load latency
+// than the few spilled bytes cost (126 -> 114 us at C192x70).
 template <class T, bool CF>
-__global__ void __launch_bounds__(256) k_helm_resid_restrict_panel(
+__global__ void __launch_bounds__(256, 4) k_helm_resid_restrict_panel(
     HelmArgs<T> A, PanelArgs P, const T* __restrict__ x, const T* __restrict__ b,
     T* __restrict__ bc, const int* __restrict__ child, int ncoarse, unsigned long long qpos,
     const int* __restrict__ cedge, int ncedge) {
@@ -993,11 +995,13 @@ size_t panel_work(lfg_helm op) {
 // y = A x / b - A x / b + H_off x through the panel kernel
 template <class T, int MODE, bool DOT, bool HASW>
 void launch_panel(lfg_helm op, const T* x, const T* b, T* y, const T* w, Red r) {
-  lfg_ctx c = op->ctx;
-  auto k = op->hsym ? k_helm_panel<T, MODE, DOT, HASW, true>
-                    : k_helm_panel<T, MODE, DOT, HASW, false>;
-  launch_pdl(c, k, occ_grid(c, (const void*)k, 256, panel_work<T>(op)), 256, 0, args_of<T>(op),
-             panel_args(op), x, b, y, w, r);
+  if constexpr (PanelShape<T>::on) {  // only the shapes panel_ok admits are built
+    lfg_ctx c = op->ctx;
+    auto k = op->hsym ? k_helm_panel<T, MODE, DOT, HASW, true>
+                      : k_helm_panel<T, MODE, DOT, HASW, false>;
+    launch_pdl(c, k, occ_grid(c, (const void*)k, 256, panel_work<T>(op)), 256, 0,
+               args_of<T>(op), panel_args(op), x, b, y, w, r);
+  }
 }
 
 // r = b + H_off x (k_helm_rhs, or the panel kernel)
@@ -1146,17 +1150,19 @@ void helm_residual_restrict(lfg_helm op, lfg_intergrid ig, lfg_field x, lfg_fiel
                      reinterpret_cast<uintptr_t>(b->d) % 16 == 0;
   auto go = [&](auto tag) {
     using T = decltype(tag);
-    if (panel) {
-      const size_t ni = ig->pnc - 2;
-      const size_t pwork = (6 * ni * ni + (size_t)ig->ncedge) * op->nl;
-      auto k = op->hsym ? k_helm_resid_restrict_panel<T, true>
-                        : k_helm_resid_restrict_panel<T, false>;
-      const lfg_mesh m = op->mesh;
-      launch_pdl(c, k, occ_grid(c, (const void*)k, bs, pwork), bs, 0, args_of<T>(op),
-                 PanelArgs{m->pn, m->proll, nullptr, 0}, (const T*)x->d, (const T*)b->d,
-                 (T*)bc->d, (const int*)ig->child, ig->ncoarse, ig->qpos,
-                 (const int*)ig->cedge, ig->ncedge);
-      return;
+    if constexpr (PanelShape<T>::on) {
+      if (panel) {
+        const size_t ni = ig->pnc - 2;
+        const size_t pwork = (6 * ni * ni + (size_t)ig->ncedge) * op->nl;
+        auto k = op->hsym ? k_helm_resid_restrict_panel<T, true>
+                          : k_helm_resid_restrict_panel<T, false>;
+        const lfg_mesh m = op->mesh;
+        launch_pdl(c, k, occ_grid(c, (const void*)k, bs, pwork), bs, 0, args_of<T>(op),
+                   PanelArgs{m->pn, m->proll, nullptr, 0}, (const T*)x->d, (const T*)b->d,
+                   (T*)bc->d, (const int*)ig->child, ig->ncoarse, ig->qpos,
+                   (const int*)ig->cedge, ig->ncedge);
+        return;
+      }
     }
     auto k = op->hsym ? k_helm_resid_restrict<T, true> : k_helm_resid_restrict<T, false>;
     launch_pdl(c, k, occ_grid(c, (const void*)k, bs, work), bs, 0, args_of<T>(op),
