@@ -40,7 +40,7 @@ FALLBACK_HBM_GBS = 6650.0
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="lfg", choices=["lfg", "reference"])
     ap.add_argument("--n", type=int, default=N_FINE, help=argparse.SUPPRESS)
@@ -85,10 +85,15 @@ class ClockSampler:
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--id={self.idx}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", "50"],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._read, daemon=True)
             self.thread.start()
+            # nvidia-smi takes a few hundred ms to start: wait for its first
+            # row so that the samples cover the timed region from its start
+            t0 = time.perf_counter()
+            while not self.rows and time.perf_counter() - t0 < 5.0:
+                time.sleep(0.01)
         except (FileNotFoundError, OSError):
             self.proc = None
         return self
@@ -753,19 +758,6 @@ def main():
         system.solve_mixed()
         system.solve_fp64()
 
-    # ---- mixed (headline, device-resident inputs)
-    with ClockSampler(dev) as clk:
-        torch.cuda.nvtx.range_push("timed_mixed")
-        ms_mixed, launches, res_m = timed(system.solve_mixed, args.steps)
-        bytes_mixed = timed.bytes
-        torch.cuda.nvtx.range_pop()
-    # ---- plain FP64 drop-in
-    torch.cuda.nvtx.range_push("timed_fp64")
-    ms_fp64, launches64, res_64 = timed(system.solve_fp64, args.steps)
-    bytes_fp64 = timed.bytes
-    torch.cuda.nvtx.range_pop()
-
-    # ---- e2e through the ABI with host buffers (pinned)
     b_host = torch.from_numpy(prob.rhs.astype(np.float64)).pin_memory()
     x_host = torch.empty(N, dtype=torch.float64).pin_memory()
     b_np, x_np = b_host.numpy(), x_host.numpy()
@@ -776,9 +768,21 @@ def main():
         system.x64.export_into(x_np)
         return r
 
-    for _ in range(1):
-        e2e_step()
-    ms_e2e, _, _ = timed(e2e_step, args.steps)
+    e2e_step()
+    # the clocks are sampled over the three timed regions
+    with ClockSampler(dev) as clk:
+        # ---- mixed (headline, device-resident inputs)
+        torch.cuda.nvtx.range_push("timed_mixed")
+        ms_mixed, launches, res_m = timed(system.solve_mixed, args.steps)
+        bytes_mixed = timed.bytes
+        torch.cuda.nvtx.range_pop()
+        # ---- plain FP64 drop-in
+        torch.cuda.nvtx.range_push("timed_fp64")
+        ms_fp64, launches64, res_64 = timed(system.solve_fp64, args.steps)
+        bytes_fp64 = timed.bytes
+        torch.cuda.nvtx.range_pop()
+        # ---- e2e through the ABI with host buffers (pinned)
+        ms_e2e, _, _ = timed(e2e_step, args.steps)
 
     # true residual of the last mixed solve, in FP64 on the device
     system.solve_mixed()

@@ -82,8 +82,14 @@ __device__ __forceinline__ void load_faces(const HelmArgs<T>& A, unsigned c, int
 // loads are all independent.
 constexpr int KC = 2;
 
-// Levels a thread keeps in registers in the segmented coarse-level sweep.
-constexpr int kSegLevels = 12;
+// Shapes of the segmented coarse-level sweep: S threads per column, each
+// keeping at most LM levels in registers (the register arrays are sized LM,
+// so a shape fits its segments tightly: 70 levels are 4 x 18, 8 x 9,
+// 16 x 5 or 32 x 3).  The last shape takes columns up to 384 levels.
+struct SegShape {
+  int S, LM;
+};
+constexpr SegShape kSegShapes[] = {{4, 18}, {8, 9}, {16, 5}, {32, 3}, {32, 12}};
 
 // (A x)(c,k) from values already in registers: the T' row (sub, diag,
 // super, in the columnwise_op_app order) then minus the four couplings.
@@ -324,54 +330,71 @@ __global__ void __launch_bounds__(128) k_helm_subst(
 
 // bc(C,k) = sum over the children q (y outer, x inner) of (b - A x)(child,k):
 // residual fused with restrict_mass_w3 (sci_restrict_mass_w3_kernel_mod.F90:126-179).
-// Levels k0 .. k0+KR-1 of coarse column C through the child map and the
-// links table (every mesh), loads issued before use.
+// child_resid: (b - A x) at levels k0 .. k0+NLV-1 of fine column c through
+// the links table (every mesh), loads issued before use.
 constexpr int KR = 2;
+template <class T, bool CF, int NLV>
+__device__ __forceinline__ void child_resid(const HelmArgs<T>& A, const T* __restrict__ x,
+                                            const T* __restrict__ b, unsigned c, int k0,
+                                            T (&r)[NLV]) {
+  const unsigned N = A.ncol;
+  const int nl = A.nl;
+  int nb[4], fc[4];
+#pragma unroll
+  for (int f = 0; f < 4; ++f) nb[f] = A.links[f * N + c];
+  load_faces<CF>(A, c, fc);
+  T xv[NLV + 2];
+#pragma unroll
+  for (int u = 0; u < NLV + 2; ++u) {
+    const int k = min(max(k0 - 1 + u, 0), nl - 1);
+    xv[u] = x[(size_t)k * N + c];
+  }
+#pragma unroll
+  for (int kk = 0; kk < NLV; ++kk) {
+    const int k = min(k0 + kk, nl - 1);
+    const size_t i = (size_t)k * N + c;
+    T xn[4], hv[4];
+#pragma unroll
+    for (int f = 0; f < 4; ++f) {
+      xn[f] = x[(size_t)k * N + nb[f]];
+      hv[f] = h_side<CF>(A, f, k, i, fc);
+    }
+    const T v = helm_row_v(A.sub[i], A.diag[i], A.sup[i], hv, xv[kk], xv[kk + 1], xv[kk + 2],
+                           xn, k > 0, k < nl - 1);
+    r[kk] = b[i] - v;
+  }
+}
+
+// One thread sums all nq children of coarse column C (the panel kernel's
+// border columns).
 template <class T, bool CF, int NLV = KR>
 __device__ __forceinline__ void resid_restrict_col(const HelmArgs<T>& A,
                                                    const T* __restrict__ x,
                                                    const T* __restrict__ b, T* __restrict__ bc,
                                                    const int* __restrict__ child, unsigned NC,
                                                    int nq, unsigned C, int k0) {
-  const unsigned N = A.ncol;
-  const int nl = A.nl;
-  const int kn = min(NLV, nl - k0);
+  const int kn = min(NLV, A.nl - k0);
   T acc[NLV];
 #pragma unroll
   for (int kk = 0; kk < NLV; ++kk) acc[kk] = (T)0;
   for (int q = 0; q < nq; ++q) {
-    const unsigned c = child[q * NC + C];
-    int nb[4], fc[4];
+    T r[NLV];
+    child_resid<T, CF, NLV>(A, x, b, (unsigned)child[q * NC + C], k0, r);
 #pragma unroll
-    for (int f = 0; f < 4; ++f) nb[f] = A.links[f * N + c];
-    load_faces<CF>(A, c, fc);
-    T xv[NLV + 2];
-#pragma unroll
-    for (int u = 0; u < NLV + 2; ++u) {
-      const int k = min(max(k0 - 1 + u, 0), nl - 1);
-      xv[u] = x[(size_t)k * N + c];
-    }
-#pragma unroll
-    for (int kk = 0; kk < NLV; ++kk) {
-      const int k = min(k0 + kk, nl - 1);
-      const size_t i = (size_t)k * N + c;
-      T xn[4], hv[4];
-#pragma unroll
-      for (int f = 0; f < 4; ++f) {
-        xn[f] = x[(size_t)k * N + nb[f]];
-        hv[f] = h_side<CF>(A, f, k, i, fc);
-      }
-      const T v = helm_row_v(A.sub[i], A.diag[i], A.sup[i], hv, xv[kk], xv[kk + 1],
-                             xv[kk + 2], xn, k > 0, k < nl - 1);
-      acc[kk] = acc[kk] + (b[i] - v);
-    }
+    for (int kk = 0; kk < NLV; ++kk) acc[kk] = acc[kk] + r[kk];
   }
 #pragma unroll
   for (int kk = 0; kk < NLV; ++kk)
     if (kk < kn) bc[(size_t)(k0 + kk) * NC + C] = acc[kk];
 }
 
-// Thread = (coarse column, chunk of KR levels).
+// Thread = (child slot q, coarse column C, chunk of KR levels): the four
+// slots of a coarse column are adjacent lanes, so a warp reads its eight
+// coarse columns' children (two rows of fine columns on a structured mesh)
+// with every child's load chain in flight at once; lane q = 0 gathers the
+// other slots' residuals by shuffle and sums them in slot order.  Every
+// lane of a warp runs the same trips (the loop bound is rounded up to the
+// warp), so the shuffles see all 32 lanes.
 template <class T, bool CF>
 __global__ void __launch_bounds__(256) k_helm_resid_restrict(HelmArgs<T> A,
                                                              const T* __restrict__ x,
@@ -382,10 +405,31 @@ __global__ void __launch_bounds__(256) k_helm_resid_restrict(HelmArgs<T> A,
   grid_dep_wait();
   const unsigned NC = ncoarse;
   const int nchunk = (A.nl + KR - 1) / KR;
-  const unsigned total = NC * (unsigned)nchunk;
-  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
-    const unsigned kc = t / NC, C = t - kc * NC;
-    resid_restrict_col<T, CF>(A, x, b, bc, child, NC, nq, C, (int)kc * KR);
+  const unsigned total = NC * (unsigned)nchunk * 4u;
+  const unsigned trips = (total + 31u) & ~31u;
+  for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < trips; t += gridDim.x * blockDim.x) {
+    const unsigned g = t >> 2, q = t & 3u;
+    const unsigned kc = g / NC, C = g - kc * NC;
+    const int k0 = (int)kc * KR;
+    T r[KR];
+#pragma unroll
+    for (int kk = 0; kk < KR; ++kk) r[kk] = (T)0;
+    if (t < total && q < (unsigned)nq)
+      child_resid<T, CF, KR>(A, x, b, (unsigned)child[q * NC + C], k0, r);
+#pragma unroll
+    for (int kk = 0; kk < KR; ++kk) {
+      const T r1 = __shfl_down_sync(0xffffffffu, r[kk], 1);
+      const T r2 = __shfl_down_sync(0xffffffffu, r[kk], 2);
+      const T r3 = __shfl_down_sync(0xffffffffu, r[kk], 3);
+      if (q == 0 && t < total && kk < A.nl - k0) {
+        T acc = (T)0;
+        acc = acc + r[kk];
+        if (nq > 1) acc = acc + r1;
+        if (nq > 2) acc = acc + r2;
+        if (nq > 3) acc = acc + r3;
+        bc[(size_t)(k0 + kk) * NC + C] = acc;
+      }
+    }
   }
 }
 
@@ -805,12 +849,11 @@ __global__ void k_convert(TO* __restrict__ y, const TI* __restrict__ x, size_t n
 // an inclusive scan of the maps over the S segments (shuffles of width S)
 // gives every segment its incoming value, and each segment then replays
 // its levels with exactly the sequential formulas from that value.
-template <class T, bool XIN, int S, bool CF>
+template <class T, bool XIN, int S, int LMAX, bool CF>
 __global__ void __launch_bounds__(128) k_helm_sweep_seg(HelmArgs<T> A, const T* __restrict__ b,
                                                         const T* __restrict__ xin, T omega,
                                                         T* __restrict__ xout) {
   grid_dep_wait();
-  constexpr int LMAX = kSegLevels;
   const int tid = threadIdx.x, j = tid % S;
   const unsigned c = blockIdx.x * (128 / S) + tid / S;
   const size_t N = A.ncol;
@@ -902,16 +945,21 @@ __global__ void __launch_bounds__(128) k_helm_sweep_seg(HelmArgs<T> A, const T* 
     }
 }
 
-// Threads per column for the segmented sweep (0: use the per-column kernels):
-// enough threads to cover the GPU, and segments of at most kSegLevels.
-inline int seg_threads(lfg_ctx c, int ncol, int nl) {
-  const long want = 2L * c->num_sms * 128;
-  if ((long)ncol >= want) return 0;
-  int S = 1;
-  while ((long)ncol * S < want && S < 32) S *= 2;
-  while ((nl + S - 1) / S > kSegLevels && S < 32) S *= 2;
-  if ((nl + S - 1) / S > kSegLevels || S < 4) return 0;
-  return S;
+// Shape of the segmented sweep (S = 0: use the per-column kernels).  Meshes
+// with fewer than two columns per resident thread slot of 128-thread blocks
+// are segmented; the first shape whose threads cover one such slot per
+// column-thread and whose segments fit is taken: fewer threads per column
+// and longer segments measured faster than more of both (C48 x 70 FP32
+// sweep 13.9 us at 4 x 18 against 16.0 at 8 x 12 registers; C24 x 70 8.1 us
+// at 8 x 9 against 9.4 at 16 x 12).
+inline SegShape seg_shape(lfg_ctx c, int ncol, int nl) {
+  const long slots = (long)c->num_sms * 128;
+  if ((long)ncol >= 2 * slots) return {0, 0};
+  for (const SegShape& s : kSegShapes)
+    if ((long)ncol * s.S >= slots && (nl + s.S - 1) / s.S <= s.LM) return s;
+  for (const SegShape& s : kSegShapes)
+    if ((nl + s.S - 1) / s.S <= s.LM) return s;
+  return {0, 0};
 }
 
 // Coupling words per dof the kernels read: 4 per side, 2 through the
@@ -919,18 +967,19 @@ inline int seg_threads(lfg_ctx c, int ncol, int nl) {
 inline double coupling_words(lfg_helm op) { return op->hsym ? 2.0 : 4.0; }
 
 template <class T, bool XIN>
-void launch_sweep_seg(lfg_ctx c, int S, HelmArgs<T> A, const T* b, const T* xin, T omega,
+void launch_sweep_seg(lfg_ctx c, SegShape sh, HelmArgs<T> A, const T* b, const T* xin, T omega,
                       T* xout, double hwords) {
-  const int cols = 128 / S;
+  const int cols = 128 / sh.S;
   const unsigned grid = (unsigned)((A.ncol + cols - 1) / cols);
   auto go = [&](auto cf) {
     constexpr bool CF = decltype(cf)::value;
-    switch (S) {
-      case 4: launch_pdl(c, k_helm_sweep_seg<T, XIN, 4, CF>, grid, 128, 0, A, b, xin, omega, xout); break;
-      case 8: launch_pdl(c, k_helm_sweep_seg<T, XIN, 8, CF>, grid, 128, 0, A, b, xin, omega, xout); break;
-      case 16: launch_pdl(c, k_helm_sweep_seg<T, XIN, 16, CF>, grid, 128, 0, A, b, xin, omega, xout); break;
-      default: launch_pdl(c, k_helm_sweep_seg<T, XIN, 32, CF>, grid, 128, 0, A, b, xin, omega, xout); break;
-    }
+    auto run = [&](auto k) { launch_pdl(c, k, grid, 128, 0, A, b, xin, omega, xout); };
+    static_assert(sizeof(kSegShapes) / sizeof(SegShape) == 5, "one case per shape");
+    if (sh.S == 4) run(k_helm_sweep_seg<T, XIN, kSegShapes[0].S, kSegShapes[0].LM, CF>);
+    else if (sh.S == 8) run(k_helm_sweep_seg<T, XIN, kSegShapes[1].S, kSegShapes[1].LM, CF>);
+    else if (sh.S == 16) run(k_helm_sweep_seg<T, XIN, kSegShapes[2].S, kSegShapes[2].LM, CF>);
+    else if (sh.LM == 3) run(k_helm_sweep_seg<T, XIN, kSegShapes[3].S, kSegShapes[3].LM, CF>);
+    else run(k_helm_sweep_seg<T, XIN, kSegShapes[4].S, kSegShapes[4].LM, CF>);
   };
   if (XIN && hwords < 4.0) go(std::true_type{});
   else go(std::false_type{});
@@ -1028,12 +1077,12 @@ void smooth_t(lfg_helm op, double omega, lfg_field x_in, lfg_field b, lfg_field 
   const T* sub = (const T*)op->sub;
   const T* inv = (const T*)op->inv;
   const T* cp = (const T*)op->cp;
-  if (const int S = seg_threads(c, op->ncol, op->nl)) {
+  if (const SegShape sh = seg_shape(c, op->ncol, op->nl); sh.S) {
     const HelmArgs<T> A = args_of<T>(op);
     if (!x_in)
-      launch_sweep_seg<T, false>(c, S, A, (const T*)b->d, nullptr, om, (T*)x_out->d, 4.0);
+      launch_sweep_seg<T, false>(c, sh, A, (const T*)b->d, nullptr, om, (T*)x_out->d, 4.0);
     else
-      launch_sweep_seg<T, true>(c, S, A, (const T*)b->d, (const T*)x_in->d, om, (T*)x_out->d,
+      launch_sweep_seg<T, true>(c, sh, A, (const T*)b->d, (const T*)x_in->d, om, (T*)x_out->d,
                                 coupling_words(op));
     return;
   }
@@ -1141,10 +1190,15 @@ void helm_residual_restrict(lfg_helm op, lfg_intergrid ig, lfg_field x, lfg_fiel
   lfg_ctx c = op->ctx;
   const int bs = 256;
   const size_t work = (size_t)ig->ncoarse * ((op->nl + KR - 1) / KR);
-  // the panel form: structured fine mesh and 2x2 map, 16-byte aligned fields
+  // the panel form: structured fine mesh and 2x2 map, 16-byte aligned
+  // fields, and at least 8 waves of coarse columns x levels (its thread runs
+  // four children's load chains; on fewer waves the lane-per-child kernel
+  // hides the latency better: 30 against 42 us at C96 -> C48, 7 against
+  // 24 us at C48 -> C24, 117 against 113 us at C192 -> C96)
   const bool panel = (op->kind == LFG_R_SINGLE ? PanelShape<float>::on
                                                : PanelShape<double>::on) &&
                      ig->pnc > 0 && op->mesh->pn == 2 * ig->pnc &&
+                     6.0 * ig->pnc * ig->pnc * op->nl >= 8.0 * c->num_sms * 2048 &&
                      !(op->hsym && !op->mesh->pcf) &&
                      reinterpret_cast<uintptr_t>(x->d) % 16 == 0 &&
                      reinterpret_cast<uintptr_t>(b->d) % 16 == 0;
@@ -1165,7 +1219,7 @@ void helm_residual_restrict(lfg_helm op, lfg_intergrid ig, lfg_field x, lfg_fiel
       }
     }
     auto k = op->hsym ? k_helm_resid_restrict<T, true> : k_helm_resid_restrict<T, false>;
-    launch_pdl(c, k, occ_grid(c, (const void*)k, bs, work), bs, 0, args_of<T>(op),
+    launch_pdl(c, k, occ_grid(c, (const void*)k, bs, 4 * work), bs, 0, args_of<T>(op),
                (const T*)x->d, (const T*)b->d, (T*)bc->d, (const int*)ig->child, ig->ncoarse,
                ig->nx * ig->ny);
   };

@@ -398,12 +398,14 @@ def test_helmholtz_apply_and_smooth(ctx, helm_small, kind):
     assert rel(Y.export(np.float64), ora.smooth(x, b, 0.8)) < tol
 
 
-@pytest.mark.parametrize("n,kind", [(24, R_SINGLE), (48, R_DOUBLE), (96, R_SINGLE),
-                                    (96, R_DOUBLE)])
+@pytest.mark.parametrize("n,kind", [(12, R_SINGLE), (16, R_DOUBLE), (24, R_SINGLE),
+                                    (48, R_DOUBLE), (96, R_SINGLE), (96, R_DOUBLE)])
 def test_helmholtz_smooth_each_launch_path(ctx, n, kind):
     """The sweep runs as the segmented one-kernel sweep on meshes with few
-    columns (C24, C48), and as right-hand side + substitution on C96 (the
-    FP32 substitution through TMA-staged tiles): all against the oracle."""
+    columns (70 levels as 32 x 3 on C12, 16 x 5 on C16, 8 x 9 on C24 and
+    4 x 18 on C48: threads per column x levels per thread), and as
+    right-hand side + substitution on C96 (the FP32 substitution through
+    TMA-staged tiles): all against the oracle."""
     p = helmholtz_problem(n, 70, seed=11, mg_levels=1)
     dt = np.float64 if kind == R_DOUBLE else np.float32
     ora = OraHelm(p)

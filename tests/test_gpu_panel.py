@@ -29,7 +29,10 @@ def _view(ctx, kind, ncol, nl, keep):
 
 
 @pytest.mark.parametrize("kind", [R_SINGLE, R_DOUBLE])
-@pytest.mark.parametrize("n,nl", [(12, 5), (48, 9)])
+# C176 x 64 is large enough for the panel form of the fused residual +
+# restriction (at least 8 waves of coarse columns x levels on 148 SMs); the
+# smaller meshes take the lane-per-child kernel for it in both layouts
+@pytest.mark.parametrize("n,nl", [(12, 5), (48, 9), (176, 64)])
 def test_panel_kernels_equal_per_column_kernels(ctx, kind, n, nl):
     p = helmholtz_problem(n, nl, seed=41, mg_levels=2)
     mesh, cmesh = api.Mesh(ctx, p.links), api.Mesh(ctx, p.mg_links[0])
