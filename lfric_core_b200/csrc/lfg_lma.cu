@@ -193,6 +193,56 @@ __global__ void k_lma_local(LmaArgs<T> L, const T* __restrict__ x, T* __restrict
   }
 }
 
+// Transposed 8 x 8 local products with the input dofs split over a lane
+// pair: lane h = 0 sums df = 0..3 from zero for all eight outputs, hands
+// the partial sums to lane h = 1 by shuffle, and that lane adds df = 4..7
+// and stores, so each output is summed in ascending df as in the unsplit
+// kernel (the same bits).  Each lane gathers 4 inputs and streams 32
+// matrix values, the pair's loads of one plane are two 128-byte runs, and
+// twice as many threads have loads in flight as with one thread per
+// cell-layer (47 -> 40 us for the C48x30 W0 operator's 217 MB).  Every
+// lane runs the same trips (the bound is rounded up to the warp).
+template <class T>
+__global__ void __launch_bounds__(256) k_lma_local_tsplit(LmaArgs<T> L, const T* __restrict__ x,
+                                                          T* __restrict__ loc) {
+  const size_t plane = (size_t)L.ncell * L.nl;
+  const size_t total = 2 * plane, trips = (total + 31) & ~(size_t)31;
+  for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < trips;
+       i += (size_t)gridDim.x * blockDim.x) {
+    const bool on = i < total;
+    const int h = (int)(i & 1);
+    const size_t t = on ? i >> 1 : 0;
+    const int cell = (int)(t % L.ncell), layer = (int)(t / L.ncell);
+    T xv[4], a[4][8];
+#pragma unroll
+    for (int dd = 0; dd < 4; ++dd) {
+      const size_t ti = (size_t)(4 * h + dd) * L.ncell + cell;
+      xv[dd] = x[(size_t)(layer + L.off_to[ti]) * L.nent_to + L.ent_to[ti]];
+#pragma unroll
+      for (int o = 0; o < 8; ++o) a[dd][o] = __ldcs(L.a + (size_t)((4 * h + dd) * 8 + o) * plane + t);
+    }
+    T acc[8];
+#pragma unroll
+    for (int o = 0; o < 8; ++o) acc[o] = (T)0;
+    if (h == 0) {
+#pragma unroll
+      for (int dd = 0; dd < 4; ++dd)
+#pragma unroll
+        for (int o = 0; o < 8; ++o) acc[o] = acc[o] + a[dd][o] * xv[dd];
+    }
+#pragma unroll
+    for (int o = 0; o < 8; ++o) acc[o] = __shfl_up_sync(0xffffffffu, acc[o], 1);
+    if (h == 1 && on) {
+#pragma unroll
+      for (int dd = 0; dd < 4; ++dd)
+#pragma unroll
+        for (int o = 0; o < 8; ++o) acc[o] = acc[o] + a[dd][o] * xv[dd];
+#pragma unroll
+      for (int o = 0; o < 8; ++o) loc[(size_t)o * plane + t] = acc[o];
+    }
+  }
+}
+
 // Padded incidence table: slot m of entity e, [m][e], holds its m-th
 // incidence as (cell, o << 8 | df), o the level offset of local dof df in
 // the cell; level k of e takes layer k - o of the cell when 0 <= k - o < nl.
@@ -358,10 +408,11 @@ void launch_local(lfg_ctx c, lfg_lma m, const T* x, T* loc) {
   auto go = [&](void (*k)(LmaArgs<T>, const T*, T*), int os) {
     k<<<occ_grid(c, (const void*)k, 256, ncl * os), 256, 0, c->stream>>>(args_of<T>(m), x, loc);
   };
-  // forward 8x8: outputs split over 2 threads (48.0 against 53.7 us on the
-  // C48x30 W0 operator); the transposed products measured best unsplit
+  // 8x8: forward outputs split over 2 threads (48.0 against 53.7 us on the
+  // C48x30 W0 operator); the transposed products split their inputs over a
+  // lane pair (splitting their outputs measured slower: 69 us)
   if (m->ndf_to == 8 && m->ndf_from == 8) {
-    if (TR) go(k_lma_local<T, TR, 8, 8, 1>, 1);
+    if (TR) go(k_lma_local_tsplit<T>, 2);
     else go(k_lma_local<T, TR, 8, 8, 2>, 2);
   }
   else if (m->ndf_to == 1 && m->ndf_from == 1) go(k_lma_local<T, TR, 1, 1>, 1);
