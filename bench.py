@@ -47,6 +47,8 @@ def parse():
     # profiling aids: only the batched workload, at a chosen size and launch shape
     ap.add_argument("--batched-only", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--kernels", action="store_true", help=argparse.SUPPRESS)
+    # small cases for ncu captures of one kernel family
+    ap.add_argument("--case", choices=["lma", "coarse"], help=argparse.SUPPRESS)
     ap.add_argument("--batch-rhs", type=int, default=64, help=argparse.SUPPRESS)
     ap.add_argument("--batch-uneven", type=int, default=32, help=argparse.SUPPRESS)
     ap.add_argument("--batch-shape", type=int, nargs=2, default=(0, 0), help=argparse.SUPPRESS)
@@ -678,6 +680,38 @@ def measure_kernels(ctx, stream, peak: float) -> list:
     return rows
 
 
+def profile_case(ctx, case: str):
+    """A small workload for an ncu capture of one kernel family: "lma" makes
+    the C48x30 W0 operator and runs three forward then three transposed
+    applies (k_lma_local, k_lma_local_tsplit, k_lma_gather_tab); "coarse"
+    makes the C96x70 hierarchy (FP32) and runs four sweeps on its C24 level,
+    then four on its C48 level (k_helm_sweep_seg)."""
+    from lfric_core_b200 import api
+    from lfric_core_b200.api import R_DOUBLE, Field
+    from lfric_core_b200.problems import helmholtz_problem, w0_problem
+    if case == "lma":
+        wp = w0_problem(48, 30, seed=4, top=30e3)
+        L = api.LocalOperator(ctx, R_DOUBLE, wp.ncell, wp.nlayers, wp.matrix(), wp.map,
+                              wp.nvert, wp.nlayers + 1)
+        X = Field(ctx, R_DOUBLE, wp.nvert, wp.nlayers + 1)
+        Y = Field(ctx, R_DOUBLE, wp.nvert, wp.nlayers + 1)
+        X.set_scalar(1.0)
+        Y.set_scalar(0.0)
+        for mode in (api.LMA_INC, api.LMA_TRANSPOSE):
+            for _ in range(3):
+                L.apply(mode, Y, X)
+    else:
+        p = helmholtz_problem(96, NLAYERS, seed=SEED, mg_levels=3)
+        S = api.HelmholtzSystem(ctx, p, fp64=False)
+        for lev in (S.levels32[2], S.levels32[1]):
+            x, b, y = lev.field(), lev.field(), lev.field()
+            x.set_scalar(1.0)
+            b.set_scalar(1.0)
+            for _ in range(4):
+                lev.smooth(0.8, x, b, y)
+    ctx.synchronize()
+
+
 def main():
     args = parse()
     rank, world, local = dist_env()
@@ -697,6 +731,12 @@ def main():
 
     from lfric_core_b200 import api
     from lfric_core_b200.problems import helmholtz_problem
+
+    if args.case:
+        ctx = api.Context(dev)
+        profile_case(ctx, args.case)
+        ctx.close()
+        return
 
     if args.kernels:
         ctx = api.Context(dev)
