@@ -398,6 +398,35 @@ def test_helmholtz_apply_and_smooth(ctx, helm_small, kind):
     assert rel(Y.export(np.float64), ora.smooth(x, b, 0.8)) < tol
 
 
+@pytest.mark.parametrize("kind", [R_SINGLE, R_DOUBLE])
+@pytest.mark.parametrize("nx,ny", [(1, 1), (2, 1), (3, 1), (2, 2)])
+def test_residual_restrict_any_child_count(ctx, kind, nx, ny):
+    """The fused residual + restriction on maps of 1 to 4 children per
+    coarse column (the lane-per-child kernel leaves the lanes past the
+    map's children idle): b_c = the sum of the children's b - A x."""
+    p = helmholtz_problem(6, 7, seed=47, mg_levels=1)
+    ncol, nl = p.ncol, p.nlayers
+    H = api.Helmholtz(ctx, kind, api.Mesh(ctx, p.links), nl, p.cm, p.hf)
+    nq = nx * ny
+    nc = ncol // nq
+    child = np.arange(ncol, dtype=np.int32).reshape(nc, ny, nx)   # 216 columns
+    ig = api.Intergrid(ctx, child, ncol)
+    rng = np.random.default_rng(48)
+    dt = np.float64 if kind == R_DOUBLE else np.float32
+    x = rng.standard_normal(p.ndof).astype(dt)
+    b = rng.standard_normal(p.ndof).astype(dt)
+    X, B, Y = H.field(x), H.field(b), H.field()
+    H.apply(Y, X)
+    r = (b.astype(np.float64) - Y.export(np.float64)).reshape(ncol, nl)
+    CB = Field(ctx, kind, nc, nl)
+    H.residual_restrict(ig, X, B, CB)
+    want = np.zeros((nc, nl))
+    for q in range(nq):
+        want += r[child.reshape(nc, nq)[:, q]]
+    tol = 1e-13 if kind == R_DOUBLE else 1e-5
+    assert rel(CB.export(np.float64), want.ravel()) < tol
+
+
 @pytest.mark.parametrize("n,kind", [(12, R_SINGLE), (16, R_DOUBLE), (24, R_SINGLE),
                                     (48, R_DOUBLE), (96, R_SINGLE), (96, R_DOUBLE)])
 def test_helmholtz_smooth_each_launch_path(ctx, n, kind):
