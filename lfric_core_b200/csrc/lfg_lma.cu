@@ -199,9 +199,10 @@ __global__ void k_lma_local(LmaArgs<T> L, const T* __restrict__ x, T* __restrict
 // and stores, so each output is summed in ascending df as in the unsplit
 // kernel (the same bits).  Each lane gathers 4 inputs and streams 32
 // matrix values, the pair's loads of one plane are two 128-byte runs, and
-// twice as many threads have loads in flight as with one thread per
-// cell-layer (47 -> 40 us for the C48x30 W0 operator's 217 MB).  Every
-// lane runs the same trips (the bound is rounded up to the warp).
+// the loads of both halves are in flight at once (C48x30 W0 operator, 217
+// MB of matrices: 47 -> 39 us under ncu; both phases of the apply 53 -> 45
+// us between CUDA events).  Every lane runs the same trips (the bound is
+// rounded up to the warp).
 template <class T>
 __global__ void __launch_bounds__(256) k_lma_local_tsplit(LmaArgs<T> L, const T* __restrict__ x,
                                                           T* __restrict__ loc) {
