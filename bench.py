@@ -400,9 +400,10 @@ def measure_configs(ctx, stream, steps: int, peak: float, cpu: bool) -> dict:
     c1 = {"workload": "C24x20 W0 mass+stiffness (kappa 1), Jacobi-preconditioned CG FP64 to 1e-8",
           "ndof": p.ndof, "iterations": res["r"].iterations, "ms_per_solve": ms,
           "solves_per_s": 1e3 / ms,
-          "note": "each solve reads the monitored residual norm on the host every iteration "
-                  "(the reference's monitor_convergence), so it is launch- and "
-                  "synchronisation-bound at this size"}
+          "note": "the reference's monitor_convergence tests the residual norm after every "
+                  "iteration; the solver reads the norms of 8 iterations at a time and "
+                  "rolls x back to the one that converged (same iterations and bits); "
+                  "about 8 small launches per iteration: launch-bound at this size"}
     if cpu:
         from oracle.oracle import W0 as OraW0
         o = OraW0(p, A, native=True)

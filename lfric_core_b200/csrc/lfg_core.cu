@@ -729,6 +729,13 @@ double lfg_ctx_s::read_result(int slot) {
   return host_results[slot];
 }
 
+void lfg_ctx_s::read_results(int slot, int n, double* out) {
+  LFG_CUDA(cudaMemcpyAsync(host_results + slot, red_results + slot, sizeof(double) * n,
+                           cudaMemcpyDeviceToHost, stream));
+  LFG_CUDA(cudaStreamSynchronize(stream));
+  for (int i = 0; i < n; ++i) out[i] = host_results[slot + i];
+}
+
 // ================================================================ C ABI
 extern "C" {
 

@@ -173,6 +173,8 @@ struct lfg_ctx_s {
   void* staging(size_t bytes);
   void* scratch(size_t bytes);
   double read_result(int slot);   // synchronises the stream
+  // n consecutive slots' results into out[] (one copy; synchronises)
+  void read_results(int slot, int n, double* out);
 };
 
 struct lfg_field_s {

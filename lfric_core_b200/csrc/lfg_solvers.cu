@@ -384,11 +384,30 @@ int take_slots(int n) {
   return s;
 }
 
-// cg_solve, sci_iterative_solver_mod.f90:495-592
+// cg_solve, sci_iterative_solver_mod.f90:495-592.
+//
+// With convergence monitoring the reference tests the residual norm after
+// every iteration; a host read of it stalls the GPU for about 24 us, which
+// is as long as a whole iteration on small meshes.  So on meshes of at most
+// kCgBatchDofs dofs the loop runs kCgBatch iterations between reads: every
+// iteration leaves its norm in its own reduction slot and a copy of x, one
+// read brings the batch's norms, and the host takes the first iteration
+// that met the tolerance and restores x from its copy.  The iteration
+// count, x and the reported error are those of the one-read-per-iteration
+// loop, bit for bit; at most kCgBatch - 1 iterations are computed past the
+// convergence (their results discarded).
+constexpr int kCgBatch = 8;
+constexpr size_t kCgBatchDofs = (size_t)1 << 21;
+
 struct CgSolver : lfg_solver_s {
+  std::vector<FieldPtr> snaps;  // x after each iteration of a batch
   int solve(lfg_field x, lfg_field b, int* iters, double* err_out) override {
     lfg_field r = W(0), p = W(1), z = W(2);
     const int s_r = slot0, s_rz0 = slot0 + 1, s_rz1 = slot0 + 2, s_pz = slot0 + 3;
+    const int s_nb = slot0 + 4;  // the batch's norms: kCgBatch slots
+    const int m = cfg.monitor_convergence && x->n() <= kCgBatchDofs ? kCgBatch : 1;
+    if (m > 1 && snaps.empty())
+      for (int i = 0; i < m; ++i) snaps.push_back(make_field(ctx, kind, ncol, nlev));
     double r_nrm_0, r_nrm = NAN;
     int iter, converged = 0, done = 0;
     vec_set(r, sc_const(0.0));
@@ -412,12 +431,24 @@ struct CgSolver : lfg_solver_s {
       op->apply_dot(p, z, p, s_pz);                                 // z = A p, <p, A p>
       vec_axpy(x, sc_div(1.0, ctx->red_results + rz, ctx->red_results + s_pz), p);
       if (cfg.monitor_convergence) {
-        vec_axpy_norm(r, sc_div(-1.0, ctx->red_results + rz, ctx->red_results + s_pz), z, s_r);
-        r_nrm = std::sqrt(host(s_r));
-        done = iter;
-        if (r_nrm / r_nrm_0 <= cfg.r_tol || r_nrm <= cfg.a_tol) {
-          converged = 1;
-          break;
+        const int j = (iter - 1) % m;  // place in the batch
+        vec_axpy_norm(r, sc_div(-1.0, ctx->red_results + rz, ctx->red_results + s_pz), z,
+                      m > 1 ? s_nb + j : s_r);
+        if (m > 1) vec_copy(snaps[j].get(), x);
+        if (j == m - 1 || iter == cfg.max_iter) {
+          double nrm[kCgBatch];
+          if (m > 1) ctx->read_results(s_nb, j + 1, nrm);
+          else nrm[0] = host(s_r);
+          for (int t = 0; t <= j; ++t) {
+            r_nrm = std::sqrt(nrm[t]);
+            done = iter - j + t;
+            if (r_nrm / r_nrm_0 <= cfg.r_tol || r_nrm <= cfg.a_tol) {
+              converged = 1;
+              if (t < j) vec_copy(x, snaps[t].get());
+              break;
+            }
+          }
+          if (converged) break;
         }
       } else {
         vec_axpy(r, sc_div(-1.0, ctx->red_results + rz, ctx->red_results + s_pz), z);

@@ -112,6 +112,42 @@ def test_cg_jacobi_w0_parity(ctx, n, nl):
     assert rel(X.export(), x) < 1e-12
 
 
+def test_cg_convergence_found_inside_a_read_batch(ctx):
+    """On small meshes monitored CG reads its residual norms once per batch
+    of iterations and rolls x back to the iteration that converged: a solve
+    stopped at that iteration by max_iter gives the same bits, and an
+    iteration limit inside a batch reports that many iterations and the
+    oracle's x after them."""
+    from oracle.oracle import W0 as OraW0
+    p = w0_problem(6, 5, seed=1, top=5e3)
+    A = p.matrix()
+    nent, nlev = p.nvert, p.nlayers + 1
+    lma = api.LocalOperator(ctx, R_DOUBLE, p.ncell, p.nlayers, A, p.map, nent, nlev)
+    diag = Field(ctx, R_DOUBLE, nent, nlev)
+    lma.diagonal(diag)
+    B = field_from(ctx, p.rhs, nent, nlev)
+
+    def solve(max_iter):
+        sol = api.IterativeSolver(api.LinearOperator.from_lma(lma),
+                                  api.Preconditioner.diagonal(diag), diag, "cg", r_tol=1e-8,
+                                  max_iter=max_iter)
+        X = Field(ctx, R_DOUBLE, nent, nlev)
+        return sol.apply(X, B), X.export()
+
+    out, x = solve(2000)
+    k = out.iterations
+    assert out.status == 0 and k > 8
+    out_k, x_k = solve(k)
+    assert out_k.status == 0 and out_k.iterations == k
+    assert np.array_equal(x, x_k)
+    assert out_k.final_err == out.final_err
+    out_s, x_s = solve(k - 3)
+    assert out_s.status == api.NOT_CONVERGED and out_s.iterations == k - 3
+    x_ref, st, info = OraW0(p, A).cg_solve(p.rhs, r_tol=1e-8, max_iter=k - 3)
+    assert info.iterations == k - 3
+    assert rel(x_s, x_ref) < 1e-12
+
+
 @pytest.mark.parametrize("method,iters", [("bicgstab", 6), ("gmres", 2), ("fgmres", 2)])
 def test_krylov_variants_parity(ctx, helm24, method, iters):
     """bicgstab / gmres / fgmres with the multigrid preconditioner against the
