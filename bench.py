@@ -401,9 +401,10 @@ def measure_configs(ctx, stream, steps: int, peak: float, cpu: bool) -> dict:
           "ndof": p.ndof, "iterations": res["r"].iterations, "ms_per_solve": ms,
           "solves_per_s": 1e3 / ms,
           "note": "the reference's monitor_convergence tests the residual norm after every "
-                  "iteration; the solver reads the norms of 8 iterations at a time and "
-                  "rolls x back to the one that converged (same iterations and bits); "
-                  "about 8 small launches per iteration: launch-bound at this size"}
+                  "iteration; the solver reads the norms of 8 iterations at a time (the "
+                  "batch replayed from a CUDA graph) and rolls x back to the one that "
+                  "converged (same iterations and bits); about 8 small kernels per "
+                  "iteration: latency-bound at this size"}
     if cpu:
         from oracle.oracle import W0 as OraW0
         o = OraW0(p, A, native=True)

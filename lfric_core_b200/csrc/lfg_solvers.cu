@@ -398,9 +398,77 @@ int take_slots(int n) {
 // convergence (their results discarded).
 constexpr int kCgBatch = 8;
 constexpr size_t kCgBatchDofs = (size_t)1 << 21;
+static_assert(kCgBatch % 2 == 0, "a batch keeps the parity of the rz slots");
 
 struct CgSolver : lfg_solver_s {
   std::vector<FieldPtr> snaps;  // x after each iteration of a batch
+  // A full batch is a fixed sequence of launches for a given x, so after its
+  // first (eager) run it is captured once as a CUDA graph and replayed.
+  struct Graph {
+    cudaGraphExec_t exec = nullptr;
+    uint64_t nodes = 0, bytes = 0;
+  };
+  std::map<void*, Graph> graphs;
+  std::set<void*> seen;
+  cudaStream_t graph_stream = nullptr;
+  bool use_graphs = std::getenv("LFG_NO_GRAPHS") == nullptr;
+
+  void drop_graphs() {
+    for (auto& kv : graphs)
+      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    graphs.clear();
+    seen.clear();
+  }
+  ~CgSolver() override { drop_graphs(); }
+
+  template <class F>
+  void replay(void* key, F&& enqueue) {
+    cudaStream_t st = ctx->stream;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    LFG_CUDA(cudaStreamIsCapturing(st, &cs));
+    if (!use_graphs || cs != cudaStreamCaptureStatusNone) {
+      enqueue();
+      return;
+    }
+    if (graph_stream != st) {
+      drop_graphs();
+      graph_stream = st;
+    }
+    auto it = graphs.find(key);
+    if (it == graphs.end() && !seen.count(key)) {
+      seen.insert(key);
+      enqueue();
+      return;
+    }
+    if (it == graphs.end()) {
+      Graph g;
+      const uint64_t n0 = ctx->launches, b0 = ctx->bytes;
+      LFG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      try {
+        enqueue();
+      } catch (...) {
+        cudaGraph_t dummy = nullptr;
+        cudaStreamEndCapture(st, &dummy);
+        if (dummy) cudaGraphDestroy(dummy);
+        throw;
+      }
+      cudaGraph_t graph = nullptr;
+      LFG_CUDA(cudaStreamEndCapture(st, &graph));
+      cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess)
+        throw Error(LFG_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+      g.nodes = ctx->launches - n0;
+      g.bytes = ctx->bytes - b0;
+      ctx->launches = n0;
+      ctx->bytes = b0;
+      it = graphs.emplace(key, g).first;
+    }
+    LFG_CUDA(cudaGraphLaunch(it->second.exec, st));
+    ctx->launches += it->second.nodes;
+    ctx->bytes += it->second.bytes;
+  }
+
   int solve(lfg_field x, lfg_field b, int* iters, double* err_out) override {
     lfg_field r = W(0), p = W(1), z = W(2);
     const int s_r = slot0, s_rz0 = slot0 + 1, s_rz1 = slot0 + 2, s_pz = slot0 + 3;
@@ -427,37 +495,61 @@ struct CgSolver : lfg_solver_s {
     vec_dot(r, z, s_rz0);
     int rz = s_rz0, rzn = s_rz1;
     vec_copy(p, z);
-    for (iter = 1; iter <= cfg.max_iter; ++iter) {
-      op->apply_dot(p, z, p, s_pz);                                 // z = A p, <p, A p>
-      vec_axpy(x, sc_div(1.0, ctx->red_results + rz, ctx->red_results + s_pz), p);
-      if (cfg.monitor_convergence) {
-        const int j = (iter - 1) % m;  // place in the batch
-        vec_axpy_norm(r, sc_div(-1.0, ctx->red_results + rz, ctx->red_results + s_pz), z,
-                      m > 1 ? s_nb + j : s_r);
-        if (m > 1) vec_copy(snaps[j].get(), x);
-        if (j == m - 1 || iter == cfg.max_iter) {
-          double nrm[kCgBatch];
-          if (m > 1) ctx->read_results(s_nb, j + 1, nrm);
-          else nrm[0] = host(s_r);
-          for (int t = 0; t <= j; ++t) {
-            r_nrm = std::sqrt(nrm[t]);
-            done = iter - j + t;
-            if (r_nrm / r_nrm_0 <= cfg.r_tol || r_nrm <= cfg.a_tol) {
-              converged = 1;
-              if (t < j) vec_copy(x, snaps[t].get());
-              break;
-            }
+    const double* R = ctx->red_results;
+    if (m > 1) {
+      // iteration j of a batch: its norm to slot s_nb + j, x to snaps[j]
+      auto step = [&](int j) {
+        op->apply_dot(p, z, p, s_pz);                               // z = A p, <p, A p>
+        vec_axpy(x, sc_div(1.0, R + rz, R + s_pz), p);
+        vec_axpy_norm(r, sc_div(-1.0, R + rz, R + s_pz), z, s_nb + j);
+        vec_copy(snaps[j].get(), x);
+        prec->apply(r, z);
+        vec_dot(r, z, rzn);                                          // rz_new
+        vec_aypx(p, sc_div(1.0, R + rzn, R + rz), z);
+        std::swap(rz, rzn);
+      };
+      for (iter = 1; iter <= cfg.max_iter; iter += m) {
+        const int nb = std::min(m, cfg.max_iter - iter + 1);
+        if (nb == m)
+          replay(x->d, [&] {
+            for (int j = 0; j < m; ++j) step(j);
+          });
+        else
+          for (int j = 0; j < nb; ++j) step(j);
+        double nrm[kCgBatch];
+        ctx->read_results(s_nb, nb, nrm);
+        for (int t = 0; t < nb; ++t) {
+          r_nrm = std::sqrt(nrm[t]);
+          done = iter + t;
+          if (r_nrm / r_nrm_0 <= cfg.r_tol || r_nrm <= cfg.a_tol) {
+            converged = 1;
+            if (t < nb - 1) vec_copy(x, snaps[t].get());
+            break;
           }
-          if (converged) break;
         }
-      } else {
-        vec_axpy(r, sc_div(-1.0, ctx->red_results + rz, ctx->red_results + s_pz), z);
-        done = iter;
+        if (converged) break;
       }
-      prec->apply(r, z);
-      vec_dot(r, z, rzn);                                            // rz_new
-      vec_aypx(p, sc_div(1.0, ctx->red_results + rzn, ctx->red_results + rz), z);
-      std::swap(rz, rzn);
+    } else {
+      for (iter = 1; iter <= cfg.max_iter; ++iter) {
+        op->apply_dot(p, z, p, s_pz);                               // z = A p, <p, A p>
+        vec_axpy(x, sc_div(1.0, R + rz, R + s_pz), p);
+        if (cfg.monitor_convergence) {
+          vec_axpy_norm(r, sc_div(-1.0, R + rz, R + s_pz), z, s_r);
+          r_nrm = std::sqrt(host(s_r));
+          done = iter;
+          if (r_nrm / r_nrm_0 <= cfg.r_tol || r_nrm <= cfg.a_tol) {
+            converged = 1;
+            break;
+          }
+        } else {
+          vec_axpy(r, sc_div(-1.0, R + rz, R + s_pz), z);
+          done = iter;
+        }
+        prec->apply(r, z);
+        vec_dot(r, z, rzn);                                          // rz_new
+        vec_aypx(p, sc_div(1.0, R + rzn, R + rz), z);
+        std::swap(rz, rzn);
+      }
     }
     if (iters) *iters = done;
     if (err_out) *err_out = cfg.monitor_convergence ? r_nrm / r_nrm_0 : NAN;
