@@ -469,13 +469,21 @@ struct CgSolver : lfg_solver_s {
     ctx->bytes += it->second.bytes;
   }
 
+  bool batched() const {
+    return cfg.monitor_convergence && (size_t)ncol * nlev <= kCgBatchDofs;
+  }
+  void prepare() {
+    if (batched())
+      for (int i = snaps.size(); i < kCgBatch; ++i)
+        snaps.push_back(make_field(ctx, kind, ncol, nlev));
+  }
+
   int solve(lfg_field x, lfg_field b, int* iters, double* err_out) override {
     lfg_field r = W(0), p = W(1), z = W(2);
     const int s_r = slot0, s_rz0 = slot0 + 1, s_rz1 = slot0 + 2, s_pz = slot0 + 3;
     const int s_nb = slot0 + 4;  // the batch's norms: kCgBatch slots
-    const int m = cfg.monitor_convergence && x->n() <= kCgBatchDofs ? kCgBatch : 1;
-    if (m > 1 && snaps.empty())
-      for (int i = 0; i < m; ++i) snaps.push_back(make_field(ctx, kind, ncol, nlev));
+    const int m = batched() ? kCgBatch : 1;
+    prepare();
     double r_nrm_0, r_nrm = NAN;
     int iter, converged = 0, done = 0;
     vec_set(r, sc_const(0.0));
@@ -1219,6 +1227,9 @@ int lfg_solver_create(lfg_linop op, lfg_prec prec, const lfg_solver_cfg* cfg, lf
     s->slot0 = take_slots((cfg->gcrk + 1) * (cfg->gcrk + 1) + 12);
     try {
       s->alloc(nvec);
+      // the x copies of monitored CG's batched reads, allocated here rather
+      // than in a solve that may run under stream capture
+      if (auto* cg = dynamic_cast<CgSolver*>(s)) cg->prepare();
     } catch (...) {
       delete s;
       throw;
