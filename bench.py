@@ -576,6 +576,161 @@ def measure_configs(ctx, stream, steps: int, peak: float, cpu: bool) -> dict:
     return out
 
 
+def measure_next_rows(ctx, stream, peak: float, cpu: bool) -> dict:
+    """The rows past the hot path (their parity is tested in tests/), timed
+    on the GPU beside the oracle where it runs whole solves: the Krylov
+    variants with the multigrid preconditioner on the C96 x 70 Helmholtz
+    problem (FP64, to 1e-8), GCR(10) with the W2 (vector-space) multigrid on
+    a C48 x 4 W2 hierarchy, and the CMA assembly and product kernels on
+    C96 x 70 columns (GPU only: the oracle restates them one column per
+    call)."""
+    import ctypes as C
+    import torch
+    from lfric_core_b200 import api
+    from lfric_core_b200.api import R_DOUBLE, Field
+    from lfric_core_b200.problems import (banded_dofmap, cma_prod_size, cma_size,
+                                          helmholtz_problem, w2_hierarchy)
+    threads = host_threads()
+    out = {}
+
+    def host_ms(fn, reps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(reps):
+            fn()
+        torch.cuda.synchronize()
+        return (time.perf_counter() - t0) / reps * 1e3
+
+    # ---- Krylov variants (sci_iterative_solver_mod.f90:645-1940)
+    p = helmholtz_problem(96, NLAYERS, seed=SEED, mg_levels=3)
+    S = api.HelmholtzSystem(ctx, p, mixed=False)
+    B, X = S.op64.field(p.rhs), S.op64.field()
+    kry = {"workload": "C96x70 W3 Helmholtz, FP64, 3-level multigrid preconditioner, "
+                       "r_tol 1e-8, restart length 10, x0 = 0", "ndof": p.ndof}
+    for method in ("gcr", "bicgstab", "gmres", "fgmres"):
+        sol = api.IterativeSolver(api.LinearOperator.from_helmholtz(S.op64), S.mg64, S.x64,
+                                  method, r_tol=1e-8, max_iter=60, gcrk=10,
+                                  fail_on_non_converged=False)
+        res = {}
+
+        def run():
+            X.set_scalar(0.0)
+            res["r"] = sol.apply(X, B)
+        run()
+        ms = host_ms(run, 3)
+        kry[method] = {"ms_per_solve": ms, "iterations": res["r"].iterations,
+                       "final_err": res["r"].final_err, "status": res["r"].status}
+    if cpu:
+        from oracle.oracle import Helmholtz as OraHelm, SolveInfo, ptr
+        ora = OraHelm(p, native=True)
+        L = ora.L
+        op, mg = ora.op(0), ora.mg(nlevels=3)
+        n = p.ndof
+        b = np.ascontiguousarray(p.rhs)
+        cb_a = C.cast(L.ora_helm_apply_cb_d, C.c_void_p)
+        cb_p = C.cast(L.ora_mg_apply_cb_d, C.c_void_p)
+        cpu_k = {"cores": threads, "kind": "port",
+                 "sample": "one solve each on all threads (-O3 -march=native -fopenmp build)"}
+        for method in ("bicgstab", "gmres"):
+            x = np.zeros(n)
+            info = SolveInfo()
+            if method == "bicgstab":
+                work = np.zeros(8 * n)
+                fn = lambda: L.ora_bicgstab_solve_d(n, cb_a, C.byref(op), cb_p, C.byref(mg),
+                                                    1e-8, 0.0, 60, 1, ptr(x), ptr(b), ptr(work),
+                                                    C.byref(info))
+            else:
+                work = np.zeros(25 * n)
+                fn = lambda: L.ora_gmres_solve_d(n, cb_a, C.byref(op), cb_p, C.byref(mg), 10,
+                                                 1e-8, 0.0, 60, 1, ptr(x), ptr(b), ptr(work),
+                                                 C.byref(info))
+            sec = _cpu_time(fn, threads, L)
+            cpu_k[method] = {"ms_per_solve": sec * 1e3, "iterations": info.iterations}
+        kry["cpu"] = cpu_k
+    out["krylov_variants"] = kry
+    del S, B, X
+
+    # ---- GCR(10) with the W2 multigrid (sci_hierarchical_preconditioner_mod.f90:22-38)
+    H = w2_hierarchy(48, 4, 3, seed=1, top=4e5, tau=1e9, radius=1.2742e6)
+    W = api.W2System(ctx, H)
+    sol = api.IterativeSolver(api.LinearOperator.from_lma(W.ops[0]), W.prec, W.field(), "gcr",
+                              r_tol=1e-8, max_iter=100, gcrk=10)
+    Bw, Xw = W.field(H.rhs), W.field()
+    res = {}
+
+    def run_w2():
+        Xw.set_scalar(0.0)
+        res["r"] = sol.apply(Xw, Bw)
+    run_w2()
+    w2 = {"workload": "C48x4 W2 (RT0 mass + div-div, tau 1e9, radius 1.2742e6 m), 3-level W2 "
+                      "multigrid (weighted Jacobi 2+2, 8 coarse), GCR(10) to 1e-8",
+          "ndof": int(H.levels[0].flat_ndof), "ms_per_solve": host_ms(run_w2, 3),
+          "iterations": res["r"].iterations}
+    if cpu:
+        from oracle.oracle import W2Multigrid
+        ora2 = W2Multigrid(H, omega=0.6, native=True)
+        info2 = {}
+
+        def cpu_w2():
+            info2["i"] = ora2.gcr_solve(H.rhs, gcrk=10, r_tol=1e-8, max_iter=100)[2]
+        sec = _cpu_time(cpu_w2, threads, ora2.L)
+        w2["cpu"] = {"ms_per_solve": sec * 1e3, "iterations": info2["i"].iterations,
+                     "cores": threads, "kind": "port",
+                     "sample": "one solve on all threads (-O3 -march=native -fopenmp build)"}
+    out["w2_multigrid"] = w2
+    del W, sol, Bw, Xw
+
+    # ---- CMA assembly and product on C96 x 70 columns (columnwise_op_asm,
+    # columnwise_op_mul; components/science/source/kernel/columnwise_operators)
+    ncell, nl, w = 6 * 96 * 96, NLAYERS, 8
+    rng = np.random.default_rng(6)
+    p3t = cma_size(nl, 1, 2, 0, 1, 1, 0)           # W3 <- Wtheta
+    pt3 = cma_size(nl, 2, 1, 1, 0, 0, 1)           # Wtheta <- W3
+    ptt = cma_prod_size(pt3, p3t)                  # Wtheta <- Wtheta
+    ls = rng.standard_normal((ncell * nl, 1, 2))
+    mt = np.array([[c * nl] for c in range(ncell)])            # W3 dofmap, (cell, 1)
+    mf = np.array([[c * (nl + 1), c * (nl + 1) + 1] for c in range(ncell)])  # Wtheta, (cell, 2)
+    lma = api.LocalOperator(ctx, R_DOUBLE, ncell, nl, np.asfortranarray(ls).ravel(order="F"),
+                            mt, ncell, nl, mf, ncell, nl + 1)
+
+    def cma(pp, bands=None):
+        return api.ColumnwiseOperator(ctx, R_DOUBLE, ncell, pp["nrow"], pp["ncol"], pp["bw"],
+                                      pp["alpha"], pp["beta"], pp["gm"], pp["gp"],
+                                      np.arange(1, pp["nrow"] + 1), np.arange(1, pp["ncol"] + 1),
+                                      bands)
+    A = cma(p3t)
+    cb_to, cb_from = banded_dofmap(nl, 1, 1, 0), banded_dofmap(nl, 2, 0, 1)
+
+    def ev_ms(fn, n=10):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(n):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    rows = []
+    ms = ev_ms(lambda: A.assemble(lma, cb_to, cb_from))
+    nb = (ncell * nl * 2 + p3t["bw"] * p3t["nrow"] * ncell) * w
+    rows.append({"kernel": "k_cma_asm_rows (columnwise_op_asm, W3 <- Wtheta)", "us": ms * 1e3,
+                 "algorithmic_bytes": nb, "frac_of_measured_hbm": nb / (ms * 1e-3) / 1e9 / peak})
+    At = cma(pt3, rng.standard_normal((pt3["bw"], pt3["nrow"], ncell)).ravel(order="F"))
+    Bt = cma(p3t, rng.standard_normal((p3t["bw"], p3t["nrow"], ncell)).ravel(order="F"))
+    Ct = cma(ptt, np.zeros((ptt["bw"], ptt["nrow"], ncell)).ravel(order="F"))
+    ms = ev_ms(lambda: Ct.multiply(At, Bt))
+    nb = (pt3["bw"] * pt3["nrow"] + p3t["bw"] * p3t["nrow"] + 2 * ptt["bw"] * ptt["nrow"]) \
+        * ncell * w
+    rows.append({"kernel": "k_cma_mul (columnwise_op_mul, Wtheta <- W3 <- Wtheta, C += A B)",
+                 "us": ms * 1e3, "algorithmic_bytes": nb,
+                 "frac_of_measured_hbm": nb / (ms * 1e-3) / 1e9 / peak})
+    out["cma_assembly"] = {"workload": "C96x70 columns (55,296), FP64", "kernels": rows}
+    return out
+
+
 def measure_kernels(ctx, stream, peak: float) -> list:
     """Every hot-path kernel timed alone (CUDA events on the library's
     stream, 3 warm-up + 20 timed launches, inputs larger than L2 where the
@@ -883,6 +1038,13 @@ def main():
                               cpu=(rank == 0 and world == 1))
     torch.cuda.nvtx.range_pop()
 
+    # ---- the rows past the hot path (rank 0 only; a minute at most)
+    nxt = None
+    if rank == 0:
+        torch.cuda.nvtx.range_push("next_rows")
+        nxt = measure_next_rows(ctx, stream, measured_hbm_peak()[0], cpu=(world == 1))
+        torch.cuda.nvtx.range_pop()
+
     # ---- CPU baseline (rank 0, N=1 only): the oracle on the same workload
     cpu = None
     if rank == 0 and world == 1:
@@ -938,6 +1100,7 @@ def main():
             "batched": dict(batched, problems_Mdof_per_s=batched["ndof"] /
                             (batched["ms_per_batch"] * 1e-3) / 1e6),
             **configs,
+            "next_rows": nxt,
             "cpu_baseline": cpu,
             "clocks": clk.summary(),
         }

@@ -709,6 +709,8 @@ int lfg_cma_destroy(lfg_cma m) {
   dfree(m->trow);
   dfree(m->finv);
   dfree(m->fcp);
+  dfree(m->asm_rowptr);
+  dfree(m->asm_list);
   delete m;
   return LFG_OK;
 }

@@ -57,6 +57,38 @@ __global__ void k_cma_asm(T* __restrict__ bands, const int* __restrict__ jminus,
     }
 }
 
+// The same assembly one thread per (row i, column): the row's
+// contributions, (a plane (d1 ndf_from + d2) nl + k, band b) in the
+// reference's loop order (k, then d1, then d2), are listed on the host; a
+// thread sums them in registers, so every band entry gets its terms in the
+// sequential kernel's order (the same bits), and writes each of the row's
+// bands once, zeros included.  The sequential kernel's read-modify-write
+// chain per level left it latency-bound (C96 x 70 W3 <- Wtheta: 136 us,
+// 0.14 of the HBM copy bandwidth).
+template <class T, class TL, int BW>
+__global__ void __launch_bounds__(128) k_cma_asm_rows(T* __restrict__ bands, int ncol, int nrow,
+                                                      int bw, const TL* __restrict__ a,
+                                                      const int* __restrict__ rowptr,
+                                                      const int2* __restrict__ contrib) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y;
+  if (c >= ncol) return;
+  T acc[BW];
+#pragma unroll
+  for (int b = 0; b < BW; ++b) acc[b] = (T)0;
+  for (int q = rowptr[i]; q < rowptr[i + 1]; ++q) {
+    const int2 e = contrib[q];
+    const T v = (T)a[(size_t)e.x * ncol + c];
+#pragma unroll
+    for (int b = 0; b < BW; ++b)
+      if (b == e.y) acc[b] = acc[b] + v;
+  }
+  const size_t plane = (size_t)nrow * ncol;
+#pragma unroll
+  for (int b = 0; b < BW; ++b)
+    if (b < bw) bands[b * plane + (size_t)i * ncol + c] = acc[b];
+}
+
 // columnwise_op_mul_kernel_code, one thread per (row i of C, column):
 // C(j, i) += sum over ell in A's band of row i of A(ell, i) B(j, ell), for
 // the ell whose B band reaches j.
@@ -235,11 +267,73 @@ int lfg_cma_assemble(lfg_cma m, lfg_lma a, const int* cb_to, const int* cb_from)
   lfg_ctx c = m->ctx;
   return guard(c, [&] {
     LFG_REQUIRE(a->ctx == c && a->ncell == m->ncol, "cma_assemble: LMA and CMA cell counts differ");
+    LFG_REQUIRE(cb_to && cb_from, "cma_assemble: null dofmap");
+    const int grid = (m->ncol + 127) / 128;
+    if (m->bw <= 8) {
+      // row-parallel form; the row lists are rebuilt only when the dofmaps
+      // differ from the last assembly's
+      std::vector<int> key = {a->ndf_to, a->ndf_from, a->nl};
+      key.insert(key.end(), cb_to, cb_to + (size_t)a->ndf_to * a->nl);
+      key.insert(key.end(), cb_from, cb_from + (size_t)a->ndf_from * a->nl);
+      if (key != m->asm_key || !m->asm_rowptr) {
+        DevInts dto, dfrom;  // validation of the dofmaps against the operator
+        dto.p = checked_dofmap(cb_to, a->ndf_to, a->nl, m->nrow, "cma_assemble");
+        dfrom.p = checked_dofmap(cb_from, a->ndf_from, a->nl, m->ncolumn, "cma_assemble");
+        check_bands(m, cb_to, a->ndf_to, cb_from, a->ndf_from, a->nl, "cma_assemble");
+        const auto jm = host_ints(m->jminus, m->nrow);
+        std::vector<std::vector<int2>> rows(m->nrow);
+        for (int k = 0; k < a->nl; ++k)
+          for (int d1 = 0; d1 < a->ndf_to; ++d1) {
+            const int i = cb_to[k * a->ndf_to + d1] - 1;
+            for (int d2 = 0; d2 < a->ndf_from; ++d2)
+              rows[i].push_back(make_int2((d1 * a->ndf_from + d2) * a->nl + k,
+                                          cb_from[k * a->ndf_from + d2] - 1 - jm[i]));
+          }
+        std::vector<int> rowptr(1, 0);
+        std::vector<int2> list;
+        for (const auto& r : rows) {
+          list.insert(list.end(), r.begin(), r.end());
+          rowptr.push_back((int)list.size());
+        }
+        LFG_CUDA(cudaStreamSynchronize(c->stream));  // earlier assemblies may read the lists
+        dfree(m->asm_rowptr);
+        dfree(m->asm_list);
+        m->asm_rowptr = nullptr;
+        m->asm_list = nullptr;
+        m->asm_key.clear();
+        m->asm_rowptr = (int*)dmalloc(rowptr.size() * sizeof(int));
+        upload(m->asm_rowptr, rowptr.data(), rowptr.size() * sizeof(int));
+        m->asm_list = (int*)dmalloc(std::max<size_t>(1, list.size()) * sizeof(int2));
+        if (!list.empty()) upload(m->asm_list, list.data(), list.size() * sizeof(int2));
+        m->asm_key = std::move(key);
+        LFG_CUDA(cudaStreamSynchronize(c->stream));  // the dofmap copies are freed on return
+      }
+      const dim3 g2(grid, m->nrow);
+      dispatch_kind(m->kind, [&](auto t) {
+        using T = decltype(t);
+        dispatch_kind(a->kind, [&](auto tl) {
+          using TL = decltype(tl);
+          auto go = [&](auto k) {
+            k<<<g2, 128, 0, c->stream>>>((T*)m->bands, m->ncol, m->nrow, m->bw,
+                                         (const TL*)a->a, m->asm_rowptr,
+                                         (const int2*)m->asm_list);
+          };
+          if (m->bw <= 2) go(k_cma_asm_rows<T, TL, 2>);
+          else if (m->bw <= 4) go(k_cma_asm_rows<T, TL, 4>);
+          else go(k_cma_asm_rows<T, TL, 8>);
+        });
+      });
+      // the element matrices read, every band written once
+      after_launch(c, "cma_asm",
+                   (uint64_t)a->kind * a->ncell * a->nl * a->ndf_to * a->ndf_from +
+                       (uint64_t)m->kind * m->bw * m->nrow * m->ncol);
+      m->fvalid = false;  // the bands changed
+      return;
+    }
     DevInts dto, dfrom;
     dto.p = checked_dofmap(cb_to, a->ndf_to, a->nl, m->nrow, "cma_assemble");
     dfrom.p = checked_dofmap(cb_from, a->ndf_from, a->nl, m->ncolumn, "cma_assemble");
     check_bands(m, cb_to, a->ndf_to, cb_from, a->ndf_from, a->nl, "cma_assemble");
-    const int grid = (m->ncol + 127) / 128;
     dispatch_kind(m->kind, [&](auto t) {
       using T = decltype(t);
       dispatch_kind(a->kind, [&](auto tl) {

@@ -272,6 +272,13 @@ struct lfg_cma_s {
   void* finv = nullptr;
   void* fcp = nullptr;
   bool fvalid = false;
+  // The row lists of the last assembly (lfg_cma_assemble: per row, the
+  // element-matrix planes and bands it sums), kept with the dofmaps they
+  // came from: re-assembling with new element matrices and the same
+  // dofmaps, as every timestep does, reuses them and stays asynchronous.
+  std::vector<int> asm_key;
+  int* asm_rowptr = nullptr;  // device [nrow+1]
+  int* asm_list = nullptr;    // device int2 [rowptr[nrow]]
 };
 
 struct lfg_lma_s {

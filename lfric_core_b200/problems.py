@@ -450,3 +450,38 @@ def w2_hierarchy(n: int, nlayers: int, nlevels: int, seed: int, top: float = 10e
             m //= 2
     rhs = np.random.default_rng(seed).standard_normal(levels[0].flat_ndof)
     return W2Hierarchy(levels=levels, cell_maps=maps, rhs=rhs)
+
+
+# ------------------------------------------------------------ CMA shapes
+def cma_size(nlayers, ndf_to, ndf_from, nface_to, nint_to, nface_from, nint_from):
+    """The columnwise-operator parameters of a to-space / from-space pair
+    (rows, columns, alpha, beta, gamma-, gamma+, bandwidth), as get_cma_size
+    computes them (components/science/unit-test/support/
+    get_unit_test_m3x3_cma_data_mod.f90:130-159); nface / nint are a space's
+    dofs per cell on layer faces / inside the cell."""
+    nrow = nlayers * nint_to + (nlayers + 1) * nface_to
+    ncol = nlayers * nint_from + (nlayers + 1) * nface_from
+    alpha = nface_from + nint_from
+    beta = nface_to + nint_to
+    g_m = (ndf_from - 1) * (nint_to + nface_to)
+    g_p = (ndf_to - 1) * (nint_from + nface_from)
+    bw = 1 + int(np.ceil((g_m + g_p) / beta))
+    return dict(alpha=alpha, beta=beta, gm=g_m, gp=g_p, bw=bw, ncol=ncol, nrow=nrow)
+
+
+def cma_prod_size(a, b):
+    """Parameters of the product A B (get_cma_prod_size, same file)."""
+    alpha, beta = a["alpha"] * b["alpha"], a["beta"] * b["beta"]
+    gm = b["alpha"] * a["gm"] + a["beta"] * b["gm"]
+    gp = b["alpha"] * a["gp"] + a["beta"] * b["gp"]
+    bw = 1 + int(np.ceil((gm + gp) / beta))
+    return dict(alpha=alpha, beta=beta, gm=gm, gp=gp, bw=bw, ncol=b["ncol"], nrow=a["nrow"])
+
+
+def banded_dofmap(nlayers, ndf, nint, nface):
+    """column_banded_dofmap(ndf, nlayers), 1-based
+    (infrastructure/source/operator/columnwise_operator_mod.f90:377-393)."""
+    k = np.arange(nlayers)[None, :]
+    df = np.arange(1, ndf + 1)[:, None]
+    return np.asfortranarray(k * (nint + nface) + df, dtype=np.int32)
+
