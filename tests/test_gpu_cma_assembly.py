@@ -66,6 +66,21 @@ def test_assemble_against_oracle(ctx, kind):
         assert rel(C.get(), ref) < TOL[kind], size
 
 
+def test_reassembly_reuses_the_row_lists(ctx):
+    """Assembling one operator again from new element matrices on the same
+    dofmaps (what every timestep does) reuses the operator's row lists and
+    still matches the oracle, as does the first assembly."""
+    rng = np.random.default_rng(24)
+    p = oh.cma_size(NL, 1, 2, 0, 1, 1, 0)                       # W3 <- Wtheta
+    cb_to, cb_from = oh.banded_dofmap(NL, 1, 1, 0), oh.banded_dofmap(NL, 2, 0, 1)
+    C = cma(ctx, R_DOUBLE, p)
+    for _ in range(3):
+        ls = rng.standard_normal((NCELL * NL, 1, 2))
+        C.assemble(lma(ctx, R_DOUBLE, ls, (1, 0), (2, 1)), cb_to, cb_from)
+        ref = oh.cma_asm(ls, p, NCELL, NL, cb_to, cb_from)
+        assert rel(C.get(), ref) < TOL[R_DOUBLE]
+
+
 @pytest.mark.parametrize("kind", [R_DOUBLE, R_SINGLE])
 def test_multiply_and_scaled_add_against_oracle(ctx, kind):
     rng = np.random.default_rng(22)
