@@ -727,6 +727,38 @@ def measure_next_rows(ctx, stream, peak: float, cpu: bool) -> dict:
     rows.append({"kernel": "k_cma_mul (columnwise_op_mul, Wtheta <- W3 <- Wtheta, C += A B)",
                  "us": ms * 1e3, "algorithmic_bytes": nb,
                  "frac_of_measured_hbm": nb / (ms * 1e-3) / 1e9 / peak})
+    # diag(Dh M2h^-1 Dh^T) on W3 (columnwise_op_asm_diag_hmht) and the lumped
+    # inverse of a W2v mass matrix (columnwise_op_asm_m2v_lumped_inv)
+    p33 = cma_size(nl, 1, 1, 0, 1, 0, 1)
+    dh_ls = rng.standard_normal((ncell * nl, 1, 4))
+    m2h_ls = rng.standard_normal((ncell * nl, 4, 4))
+    for d in range(4):
+        m2h_ls[:, d, d] = 1.0 + rng.random(ncell * nl)
+    m3 = np.array([[c * nl] for c in range(ncell)])
+    m2h_map = np.array([[(c * 4 + d) * nl for d in range(4)] for c in range(ncell)])
+    Dh = api.LocalOperator(ctx, R_DOUBLE, ncell, nl, np.asfortranarray(dh_ls).ravel(order="F"),
+                           m3, ncell, nl, m2h_map, ncell * 4, nl)
+    M2h = api.LocalOperator(ctx, R_DOUBLE, ncell, nl,
+                            np.asfortranarray(m2h_ls).ravel(order="F"), m2h_map, ncell * 4, nl,
+                            m2h_map, ncell * 4, nl)
+    Hc = cma(p33)
+    cb3 = banded_dofmap(nl, 1, 1, 0)
+    ms = ev_ms(lambda: Hc.assemble_diag_hmht(Dh, M2h, cb3))
+    nb = (ncell * nl * (4 + 4) + p33["bw"] * p33["nrow"] * ncell) * w
+    rows.append({"kernel": "k_cma_hmht_rows (columnwise_op_asm_diag_hmht, W3)", "us": ms * 1e3,
+                 "algorithmic_bytes": nb, "frac_of_measured_hbm": nb / (ms * 1e-3) / 1e9 / peak})
+    pvv = cma_size(nl, 2, 2, 1, 0, 1, 0)
+    mv_ls = np.abs(rng.standard_normal((ncell * nl, 2, 2))) + 0.1
+    mvm = np.array([[c * (nl + 1), c * (nl + 1) + 1] for c in range(ncell)])
+    Mv = api.LocalOperator(ctx, R_DOUBLE, ncell, nl, np.asfortranarray(mv_ls).ravel(order="F"),
+                           mvm, ncell, nl + 1, mvm, ncell, nl + 1)
+    Lc = cma(pvv)
+    cbv = banded_dofmap(nl, 2, 0, 1)
+    ms = ev_ms(lambda: Lc.assemble_m2v_lumped_inv(Mv, cbv))
+    nb = (ncell * nl * 2 + pvv["bw"] * pvv["nrow"] * ncell) * w
+    rows.append({"kernel": "k_cma_asm_rows<inverse> (columnwise_op_asm_m2v_lumped_inv, W2v)",
+                 "us": ms * 1e3, "algorithmic_bytes": nb,
+                 "frac_of_measured_hbm": nb / (ms * 1e-3) / 1e9 / peak})
     out["cma_assembly"] = {"workload": "C96x70 columns (55,296), FP64", "kernels": rows}
     return out
 

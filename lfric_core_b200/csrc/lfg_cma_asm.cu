@@ -65,7 +65,10 @@ __global__ void k_cma_asm(T* __restrict__ bands, const int* __restrict__ jminus,
 // bands once, zeros included.  The sequential kernel's read-modify-write
 // chain per level left it latency-bound (C96 x 70 W3 <- Wtheta: 136 us,
 // 0.14 of the HBM copy bandwidth).
-template <class T, class TL, int BW>
+// INV: every non-zero entry then inverted (the lumped inverse of
+// columnwise_op_asm_m2v_lumped_inv, whose contributions are the diagonal
+// entries M(d, d) on band 0).
+template <class T, class TL, int BW, bool INV = false>
 __global__ void __launch_bounds__(128) k_cma_asm_rows(T* __restrict__ bands, int ncol, int nrow,
                                                       int bw, const TL* __restrict__ a,
                                                       const int* __restrict__ rowptr,
@@ -82,6 +85,42 @@ __global__ void __launch_bounds__(128) k_cma_asm_rows(T* __restrict__ bands, int
 #pragma unroll
     for (int b = 0; b < BW; ++b)
       if (b == e.y) acc[b] = acc[b] + v;
+  }
+  const size_t plane = (size_t)nrow * ncol;
+#pragma unroll
+  for (int b = 0; b < BW; ++b) {
+    if (INV && acc[b] != (T)0) acc[b] = (T)1 / acc[b];
+    if (b < bw) bands[b * plane + (size_t)i * ncol + c] = acc[b];
+  }
+}
+
+// columnwise_op_asm_diag_hmht one thread per (row i, column): the row's
+// entries (layer k, dofs d1, d2 of W3, band b) in the reference's loop
+// order, each adding sum over d3 of Dh(d1, d3) Dh(d2, d3) / M2h(d3, d3) at
+// layer k, formed in the element matrices' precision as in k_cma_asm_hmht.
+template <class T, class TL, int BW>
+__global__ void __launch_bounds__(128) k_cma_hmht_rows(T* __restrict__ bands, int ncol, int nrow,
+                                                       int bw, const TL* __restrict__ dh,
+                                                       const TL* __restrict__ m2h, int ndf2h,
+                                                       int nl, const int* __restrict__ rowptr,
+                                                       const int2* __restrict__ contrib) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y;
+  if (c >= ncol) return;
+  T acc[BW];
+#pragma unroll
+  for (int b = 0; b < BW; ++b) acc[b] = (T)0;
+  for (int q = rowptr[i]; q < rowptr[i + 1]; ++q) {
+    const int2 e = contrib[q];
+    const int k = e.x & 0xffff, d1 = (e.x >> 16) & 0xff, d2 = (int)((unsigned)e.x >> 24);
+    TL tmp = (TL)0;
+    for (int d3 = 0; d3 < ndf2h; ++d3)
+      tmp = tmp + dh[(((size_t)d1 * ndf2h + d3) * nl + k) * ncol + c] *
+                      dh[(((size_t)d2 * ndf2h + d3) * nl + k) * ncol + c] /
+                      m2h[(((size_t)d3 * ndf2h + d3) * nl + k) * ncol + c];
+#pragma unroll
+    for (int b = 0; b < BW; ++b)
+      if (b == e.y) acc[b] = acc[b] + (T)tmp;
   }
   const size_t plane = (size_t)nrow * ncol;
 #pragma unroll
@@ -236,6 +275,40 @@ struct DevInts {
   ~DevInts() { dfree(p); }
 };
 
+// The operator's row lists for an assembly identified by `key` (the kind of
+// assembly, the shapes and the dofmaps): rebuilt by build(rows), which
+// lists each row's entries in the reference's loop order, only when the key
+// differs from the last assembly's.
+template <class F>
+void cached_rows(lfg_cma m, std::vector<int> key, F&& build) {
+  if (key == m->asm_key && m->asm_rowptr) return;
+  std::vector<std::vector<int2>> rows(m->nrow);
+  build(rows);
+  std::vector<int> rowptr(1, 0);
+  std::vector<int2> list;
+  for (const auto& r : rows) {
+    list.insert(list.end(), r.begin(), r.end());
+    rowptr.push_back((int)list.size());
+  }
+  LFG_CUDA(cudaStreamSynchronize(m->ctx->stream));  // earlier assemblies may read the lists
+  dfree(m->asm_rowptr);
+  dfree(m->asm_list);
+  m->asm_rowptr = nullptr;
+  m->asm_list = nullptr;
+  m->asm_key.clear();
+  m->asm_rowptr = (int*)dmalloc(rowptr.size() * sizeof(int));
+  upload(m->asm_rowptr, rowptr.data(), rowptr.size() * sizeof(int));
+  m->asm_list = (int*)dmalloc(std::max<size_t>(1, list.size()) * sizeof(int2));
+  if (!list.empty()) upload(m->asm_list, list.data(), list.size() * sizeof(int2));
+  m->asm_key = std::move(key);
+}
+
+// the dofmap's values as a key tail
+std::vector<int> with_map(std::vector<int> key, const int* cb, size_t n) {
+  key.insert(key.end(), cb, cb + n);
+  return key;
+}
+
 }  // namespace
 
 extern "C" {
@@ -272,40 +345,24 @@ int lfg_cma_assemble(lfg_cma m, lfg_lma a, const int* cb_to, const int* cb_from)
     if (m->bw <= 8) {
       // row-parallel form; the row lists are rebuilt only when the dofmaps
       // differ from the last assembly's
-      std::vector<int> key = {a->ndf_to, a->ndf_from, a->nl};
-      key.insert(key.end(), cb_to, cb_to + (size_t)a->ndf_to * a->nl);
-      key.insert(key.end(), cb_from, cb_from + (size_t)a->ndf_from * a->nl);
+      std::vector<int> key = {0, a->ndf_to, a->ndf_from, a->nl};
+      key = with_map(with_map(std::move(key), cb_to, (size_t)a->ndf_to * a->nl), cb_from,
+                     (size_t)a->ndf_from * a->nl);
       if (key != m->asm_key || !m->asm_rowptr) {
         DevInts dto, dfrom;  // validation of the dofmaps against the operator
         dto.p = checked_dofmap(cb_to, a->ndf_to, a->nl, m->nrow, "cma_assemble");
         dfrom.p = checked_dofmap(cb_from, a->ndf_from, a->nl, m->ncolumn, "cma_assemble");
         check_bands(m, cb_to, a->ndf_to, cb_from, a->ndf_from, a->nl, "cma_assemble");
         const auto jm = host_ints(m->jminus, m->nrow);
-        std::vector<std::vector<int2>> rows(m->nrow);
-        for (int k = 0; k < a->nl; ++k)
-          for (int d1 = 0; d1 < a->ndf_to; ++d1) {
-            const int i = cb_to[k * a->ndf_to + d1] - 1;
-            for (int d2 = 0; d2 < a->ndf_from; ++d2)
-              rows[i].push_back(make_int2((d1 * a->ndf_from + d2) * a->nl + k,
-                                          cb_from[k * a->ndf_from + d2] - 1 - jm[i]));
-          }
-        std::vector<int> rowptr(1, 0);
-        std::vector<int2> list;
-        for (const auto& r : rows) {
-          list.insert(list.end(), r.begin(), r.end());
-          rowptr.push_back((int)list.size());
-        }
-        LFG_CUDA(cudaStreamSynchronize(c->stream));  // earlier assemblies may read the lists
-        dfree(m->asm_rowptr);
-        dfree(m->asm_list);
-        m->asm_rowptr = nullptr;
-        m->asm_list = nullptr;
-        m->asm_key.clear();
-        m->asm_rowptr = (int*)dmalloc(rowptr.size() * sizeof(int));
-        upload(m->asm_rowptr, rowptr.data(), rowptr.size() * sizeof(int));
-        m->asm_list = (int*)dmalloc(std::max<size_t>(1, list.size()) * sizeof(int2));
-        if (!list.empty()) upload(m->asm_list, list.data(), list.size() * sizeof(int2));
-        m->asm_key = std::move(key);
+        cached_rows(m, std::move(key), [&](std::vector<std::vector<int2>>& rows) {
+          for (int k = 0; k < a->nl; ++k)
+            for (int d1 = 0; d1 < a->ndf_to; ++d1) {
+              const int i = cb_to[k * a->ndf_to + d1] - 1;
+              for (int d2 = 0; d2 < a->ndf_from; ++d2)
+                rows[i].push_back(make_int2((d1 * a->ndf_from + d2) * a->nl + k,
+                                            cb_from[k * a->ndf_from + d2] - 1 - jm[i]));
+            }
+        });
         LFG_CUDA(cudaStreamSynchronize(c->stream));  // the dofmap copies are freed on return
       }
       const dim3 g2(grid, m->nrow);
@@ -429,10 +486,48 @@ int lfg_cma_assemble_diag_hmht(lfg_cma m, lfg_lma dh, lfg_lma m2h, const int* cb
     LFG_REQUIRE(dh->ndf_from == m2h->ndf_to && m2h->ndf_to == m2h->ndf_from,
                 "cma_assemble_diag_hmht: Dh must map W2h -> W3 and M2h be W2h x W2h");
     LFG_REQUIRE(dh->kind == m2h->kind, "cma_assemble_diag_hmht: LMA kinds differ");
+    const int grid = (m->ncol + 127) / 128;
+    if (m->bw <= 8 && dh->nl < (1 << 16) && dh->ndf_to < 128) {
+      std::vector<int> key = {1, dh->ndf_to, dh->ndf_from, dh->nl};
+      key = with_map(std::move(key), cbm, (size_t)dh->ndf_to * dh->nl);
+      if (key != m->asm_key || !m->asm_rowptr) {
+        DevInts d;
+        d.p = checked_dofmap(cbm, dh->ndf_to, dh->nl, m->nrow, "cma_assemble_diag_hmht");
+        check_bands(m, cbm, dh->ndf_to, cbm, dh->ndf_to, dh->nl, "cma_assemble_diag_hmht");
+        const auto jm = host_ints(m->jminus, m->nrow);
+        const int n3 = dh->ndf_to;
+        cached_rows(m, std::move(key), [&](std::vector<std::vector<int2>>& rows) {
+          for (int k = 0; k < dh->nl; ++k)
+            for (int d1 = 0; d1 < n3; ++d1) {
+              const int i = cbm[k * n3 + d1] - 1;
+              for (int d2 = 0; d2 < n3; ++d2)
+                rows[i].push_back(make_int2(k | d1 << 16 | d2 << 24, cbm[k * n3 + d2] - 1 - jm[i]));
+            }
+        });
+        LFG_CUDA(cudaStreamSynchronize(c->stream));
+      }
+      const dim3 g2(grid, m->nrow);
+      dispatch_kind(m->kind, [&](auto t) {
+        using T = decltype(t);
+        dispatch_kind(dh->kind, [&](auto tl) {
+          using TL = decltype(tl);
+          auto go = [&](auto k) {
+            k<<<g2, 128, 0, c->stream>>>((T*)m->bands, m->ncol, m->nrow, m->bw,
+                                         (const TL*)dh->a, (const TL*)m2h->a, dh->ndf_from,
+                                         dh->nl, m->asm_rowptr, (const int2*)m->asm_list);
+          };
+          if (m->bw <= 2) go(k_cma_hmht_rows<T, TL, 2>);
+          else if (m->bw <= 4) go(k_cma_hmht_rows<T, TL, 4>);
+          else go(k_cma_hmht_rows<T, TL, 8>);
+        });
+      });
+      after_launch(c, "cma_asm_diag_hmht");
+      m->fvalid = false;
+      return;
+    }
     DevInts d;
     d.p = checked_dofmap(cbm, dh->ndf_to, dh->nl, m->nrow, "cma_assemble_diag_hmht");
     check_bands(m, cbm, dh->ndf_to, cbm, dh->ndf_to, dh->nl, "cma_assemble_diag_hmht");
-    const int grid = (m->ncol + 127) / 128;
     dispatch_kind(m->kind, [&](auto t) {
       using T = decltype(t);
       dispatch_kind(dh->kind, [&](auto tl) {
@@ -454,9 +549,42 @@ int lfg_cma_assemble_m2v_lumped_inv(lfg_cma m, lfg_lma mm, const int* cbm) {
   return guard(c, [&] {
     LFG_REQUIRE(mm->ctx == c && mm->ncell == m->ncol && mm->ndf_to == mm->ndf_from,
                 "cma_assemble_m2v_lumped_inv: LMA must be square with the CMA's cells");
+    const int grid = (m->ncol + 127) / 128;
+    if (m->bw <= 8) {
+      std::vector<int> key = {2, mm->ndf_to, mm->nl};
+      key = with_map(std::move(key), cbm, (size_t)mm->ndf_to * mm->nl);
+      if (key != m->asm_key || !m->asm_rowptr) {
+        DevInts d;
+        d.p = checked_dofmap(cbm, mm->ndf_to, mm->nl, m->nrow, "cma_assemble_m2v_lumped_inv");
+        const int nd = mm->ndf_to;
+        cached_rows(m, std::move(key), [&](std::vector<std::vector<int2>>& rows) {
+          for (int k = 0; k < mm->nl; ++k)
+            for (int dd = 0; dd < nd; ++dd)
+              rows[cbm[k * nd + dd] - 1].push_back(make_int2((dd * nd + dd) * mm->nl + k, 0));
+        });
+        LFG_CUDA(cudaStreamSynchronize(c->stream));
+      }
+      const dim3 g2(grid, m->nrow);
+      dispatch_kind(m->kind, [&](auto t) {
+        using T = decltype(t);
+        dispatch_kind(mm->kind, [&](auto tl) {
+          using TL = decltype(tl);
+          auto go = [&](auto k) {
+            k<<<g2, 128, 0, c->stream>>>((T*)m->bands, m->ncol, m->nrow, m->bw,
+                                         (const TL*)mm->a, m->asm_rowptr,
+                                         (const int2*)m->asm_list);
+          };
+          if (m->bw <= 2) go(k_cma_asm_rows<T, TL, 2, true>);
+          else if (m->bw <= 4) go(k_cma_asm_rows<T, TL, 4, true>);
+          else go(k_cma_asm_rows<T, TL, 8, true>);
+        });
+      });
+      after_launch(c, "cma_asm_m2v_lumped_inv");
+      m->fvalid = false;
+      return;
+    }
     DevInts d;
     d.p = checked_dofmap(cbm, mm->ndf_to, mm->nl, m->nrow, "cma_assemble_m2v_lumped_inv");
-    const int grid = (m->ncol + 127) / 128;
     dispatch_kind(m->kind, [&](auto t) {
       using T = decltype(t);
       dispatch_kind(mm->kind, [&](auto tl) {
