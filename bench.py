@@ -676,7 +676,8 @@ def measure_next_rows(ctx, stream, peak: float, cpu: bool) -> dict:
         sec = _cpu_time(cpu_w2, threads, ora2.L)
         w2["cpu"] = {"ms_per_solve": sec * 1e3, "iterations": info2["i"].iterations,
                      "cores": threads, "kind": "port",
-                     "sample": "one solve on all threads (-O3 -march=native -fopenmp build)"}
+                     "sample": "one solve on all threads (-O3 -march=native -fopenmp build; "
+                               "its LMA applies, GH_INC scatters, run serially)"}
     out["w2_multigrid"] = w2
     del W, sol, Bw, Xw
 
