@@ -718,6 +718,7 @@ void* lfg_ctx_s::scratch(size_t bytes) {
     scratch_bytes = 0;
     scratch_buf = dmalloc(bytes);
     scratch_bytes = bytes;
+    ++scratch_gen;
   }
   return scratch_buf;
 }

@@ -150,6 +150,10 @@ struct lfg_ctx_s {
   // device scratch of the kernels that need one (grown on demand)
   void* scratch_buf = nullptr;
   size_t scratch_bytes = 0;
+  // counts reallocations of scratch_buf: a captured CUDA graph whose kernels
+  // use the scratch buffer is replayed only under the generation it was
+  // captured in
+  uint64_t scratch_gen = 0;
   // device error word: kernels whose bounded waits ran out record a code
   // here (0 = none); read by check_device_error
   unsigned* dev_err = nullptr;

@@ -124,6 +124,94 @@ FieldPtr make_field(lfg_ctx c, int kind, int ncol, int nlev) {
 // n_pre block-Jacobi column sweeps from zero, residual fused with
 // restrict_mass_w3, the coarse-level cycle, prolong_scalar_unweighted added
 // in place, n_post sweeps; n_coarse sweeps from zero on the coarsest level.
+// Captured CUDA graphs of fixed launch sequences, one per key (the buffers
+// the sequence reads and writes): the first run of a key is eager (kernel
+// set-up such as shared-memory attributes and the scratch buffer's size
+// happen outside any capture), the second is captured, later ones replay.
+// A graph is replayed only on the stream and under the scratch generation
+// it was captured with (its kernels may hold the scratch buffer's address);
+// otherwise the sequence runs eagerly and is captured again.  The launch
+// and byte counts of a capture are added at every replay.
+struct GraphCache {
+  struct Graph {
+    cudaGraphExec_t exec = nullptr;
+    uint64_t nodes = 0, bytes = 0, gen = 0;
+  };
+  using Key = std::pair<const void*, const void*>;
+  lfg_ctx ctx = nullptr;
+  std::map<Key, Graph> graphs;
+  std::set<Key> seen;
+  cudaStream_t stream = nullptr;
+  bool enabled = std::getenv("LFG_NO_GRAPHS") == nullptr;
+
+  void drop() {
+    for (auto& kv : graphs)
+      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
+    graphs.clear();
+    seen.clear();
+  }
+  ~GraphCache() { drop(); }
+
+  template <class F>
+  void run(Key key, F&& enqueue) {
+    cudaStream_t st = ctx->stream;
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    LFG_CUDA(cudaStreamIsCapturing(st, &cs));
+    if (!enabled || cs != cudaStreamCaptureStatusNone) {
+      enqueue();
+      return;
+    }
+    if (stream != st) {  // graphs are replayed on the stream they target
+      drop();
+      stream = st;
+    }
+    auto it = graphs.find(key);
+    if (it != graphs.end() && it->second.gen != ctx->scratch_gen) {
+      cudaGraphExecDestroy(it->second.exec);
+      graphs.erase(it);
+      seen.erase(key);
+      it = graphs.end();
+    }
+    if (it == graphs.end() && !seen.count(key)) {
+      seen.insert(key);
+      enqueue();
+      return;
+    }
+    if (it == graphs.end()) {
+      Graph g;
+      g.gen = ctx->scratch_gen;
+      const uint64_t n0 = ctx->launches, b0 = ctx->bytes;
+      LFG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+      try {
+        enqueue();
+      } catch (...) {
+        cudaGraph_t dummy = nullptr;
+        cudaStreamEndCapture(st, &dummy);
+        if (dummy) cudaGraphDestroy(dummy);
+        throw;
+      }
+      cudaGraph_t graph = nullptr;
+      LFG_CUDA(cudaStreamEndCapture(st, &graph));
+      if (g.gen != ctx->scratch_gen) {  // the scratch buffer moved while capturing
+        cudaGraphDestroy(graph);
+        throw Error(LFG_ERR_CUDA, "graph capture: the scratch buffer was reallocated");
+      }
+      cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess)
+        throw Error(LFG_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+      g.nodes = ctx->launches - n0;
+      g.bytes = ctx->bytes - b0;
+      ctx->launches = n0;
+      ctx->bytes = b0;
+      it = graphs.emplace(key, g).first;
+    }
+    LFG_CUDA(cudaGraphLaunch(it->second.exec, st));
+    ctx->launches += it->second.nodes;
+    ctx->bytes += it->second.bytes;
+  }
+};
+
 struct MgPrec : lfg_prec_s {
   std::vector<lfg_helm> ops;
   std::vector<lfg_intergrid> maps;
@@ -181,26 +269,11 @@ struct MgPrec : lfg_prec_s {
     if (n_post > 0) sweeps(l, n_post, P, b, X, T);
   }
 
-  // One captured CUDA graph per (input, output) buffer pair: the V-cycle is
-  // a fixed sequence of ~20 launches per level, and the Krylov solvers
-  // apply the preconditioner to a small fixed set of vectors, so replaying
-  // a graph removes the per-kernel launch gaps.
-  struct Graph {
-    cudaGraphExec_t exec = nullptr;
-    uint64_t nodes = 0, bytes = 0;
-  };
-  std::map<std::pair<void*, void*>, Graph> graphs;
-  std::set<std::pair<void*, void*>> seen;
-  cudaStream_t graph_stream = nullptr;
-  bool use_graphs = std::getenv("LFG_NO_GRAPHS") == nullptr;
-
-  void drop_graphs() {
-    for (auto& kv : graphs)
-      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
-    graphs.clear();
-    seen.clear();
-  }
-  ~MgPrec() override { drop_graphs(); }
+  // The V-cycle is a fixed sequence of ~20 launches per level and the
+  // Krylov solvers apply the preconditioner to a small fixed set of
+  // vectors, so each (input, output) pair's V-cycle is replayed from a
+  // captured graph, without the per-kernel launch gaps.
+  GraphCache graphs;
 
   void apply(lfg_field x, lfg_field y) override {
     const lfg_helm h = ops[0];
@@ -208,53 +281,8 @@ struct MgPrec : lfg_prec_s {
                     y->ncol == h->ncol && y->nlev == h->nl && y->kind == h->kind,
                 "multigrid apply: fields do not match the finest operator");
     LFG_REQUIRE(x->d != y->d, "multigrid apply: x and y may not alias");
-    cudaStream_t st = ctx->stream;
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    LFG_CUDA(cudaStreamIsCapturing(st, &cs));
-    if (!use_graphs || cs != cudaStreamCaptureStatusNone) {
-      vcycle(0, x, y);
-      return;
-    }
-    if (graph_stream != st) {  // graphs are replayed on the stream they target
-      drop_graphs();
-      graph_stream = st;
-    }
-    auto key = std::make_pair(x->d, y->d);
-    auto it = graphs.find(key);
-    if (it == graphs.end() && !seen.count(key)) {
-      // first use of this pair runs eagerly (one-time kernel set-up such as
-      // shared-memory attributes happens outside any capture)
-      seen.insert(key);
-      vcycle(0, x, y);
-      return;
-    }
-    if (it == graphs.end()) {
-      Graph g;
-      const uint64_t n0 = ctx->launches, b0 = ctx->bytes;
-      LFG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-      try {
-        vcycle(0, x, y);
-      } catch (...) {
-        cudaGraph_t dummy = nullptr;
-        cudaStreamEndCapture(st, &dummy);
-        if (dummy) cudaGraphDestroy(dummy);
-        throw;
-      }
-      cudaGraph_t graph = nullptr;
-      LFG_CUDA(cudaStreamEndCapture(st, &graph));
-      cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
-      cudaGraphDestroy(graph);
-      if (e != cudaSuccess)
-        throw Error(LFG_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
-      g.nodes = ctx->launches - n0;
-      g.bytes = ctx->bytes - b0;
-      ctx->launches = n0;
-      ctx->bytes = b0;
-      it = graphs.emplace(key, g).first;
-    }
-    LFG_CUDA(cudaGraphLaunch(it->second.exec, st));
-    ctx->launches += it->second.nodes;
-    ctx->bytes += it->second.bytes;
+    graphs.ctx = ctx;
+    graphs.run({x->d, y->d}, [&] { vcycle(0, x, y); });
   }
 };
 
@@ -345,8 +373,12 @@ struct W2MgPrec : lfg_prec_s {
                     y->ncol == a->nent_to && y->nlev == a->nlev_to && y->kind == LFG_R_DOUBLE,
                 "w2 multigrid apply: fields do not match the finest operator");
     LFG_REQUIRE(x->d != y->d, "w2 multigrid apply: x and y may not alias");
-    vcycle(0, x, y);
+    graphs.ctx = ctx;
+    graphs.run({x->d, y->d}, [&] { vcycle(0, x, y); });
   }
+  // each (input, output) pair's V-cycle replayed from a captured graph (its
+  // LMA applies hold the scratch buffer: GraphCache checks its generation)
+  GraphCache graphs;
 };
 
 }  // namespace
@@ -402,72 +434,9 @@ static_assert(kCgBatch % 2 == 0, "a batch keeps the parity of the rz slots");
 
 struct CgSolver : lfg_solver_s {
   std::vector<FieldPtr> snaps;  // x after each iteration of a batch
-  // A full batch is a fixed sequence of launches for a given x, so after its
-  // first (eager) run it is captured once as a CUDA graph and replayed.
-  struct Graph {
-    cudaGraphExec_t exec = nullptr;
-    uint64_t nodes = 0, bytes = 0;
-  };
-  std::map<void*, Graph> graphs;
-  std::set<void*> seen;
-  cudaStream_t graph_stream = nullptr;
-  bool use_graphs = std::getenv("LFG_NO_GRAPHS") == nullptr;
-
-  void drop_graphs() {
-    for (auto& kv : graphs)
-      if (kv.second.exec) cudaGraphExecDestroy(kv.second.exec);
-    graphs.clear();
-    seen.clear();
-  }
-  ~CgSolver() override { drop_graphs(); }
-
-  template <class F>
-  void replay(void* key, F&& enqueue) {
-    cudaStream_t st = ctx->stream;
-    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
-    LFG_CUDA(cudaStreamIsCapturing(st, &cs));
-    if (!use_graphs || cs != cudaStreamCaptureStatusNone) {
-      enqueue();
-      return;
-    }
-    if (graph_stream != st) {
-      drop_graphs();
-      graph_stream = st;
-    }
-    auto it = graphs.find(key);
-    if (it == graphs.end() && !seen.count(key)) {
-      seen.insert(key);
-      enqueue();
-      return;
-    }
-    if (it == graphs.end()) {
-      Graph g;
-      const uint64_t n0 = ctx->launches, b0 = ctx->bytes;
-      LFG_CUDA(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
-      try {
-        enqueue();
-      } catch (...) {
-        cudaGraph_t dummy = nullptr;
-        cudaStreamEndCapture(st, &dummy);
-        if (dummy) cudaGraphDestroy(dummy);
-        throw;
-      }
-      cudaGraph_t graph = nullptr;
-      LFG_CUDA(cudaStreamEndCapture(st, &graph));
-      cudaError_t e = cudaGraphInstantiate(&g.exec, graph, 0);
-      cudaGraphDestroy(graph);
-      if (e != cudaSuccess)
-        throw Error(LFG_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
-      g.nodes = ctx->launches - n0;
-      g.bytes = ctx->bytes - b0;
-      ctx->launches = n0;
-      ctx->bytes = b0;
-      it = graphs.emplace(key, g).first;
-    }
-    LFG_CUDA(cudaGraphLaunch(it->second.exec, st));
-    ctx->launches += it->second.nodes;
-    ctx->bytes += it->second.bytes;
-  }
+  // A full batch is a fixed sequence of launches for a given x: replayed
+  // from a captured graph (its LMA applies hold the scratch buffer)
+  GraphCache graphs;
 
   bool batched() const {
     return cfg.monitor_convergence && (size_t)ncol * nlev <= kCgBatchDofs;
@@ -518,12 +487,14 @@ struct CgSolver : lfg_solver_s {
       };
       for (iter = 1; iter <= cfg.max_iter; iter += m) {
         const int nb = std::min(m, cfg.max_iter - iter + 1);
-        if (nb == m)
-          replay(x->d, [&] {
+        if (nb == m) {
+          graphs.ctx = ctx;
+          graphs.run({x->d, nullptr}, [&] {
             for (int j = 0; j < m; ++j) step(j);
           });
-        else
+        } else {
           for (int j = 0; j < nb; ++j) step(j);
+        }
         double nrm[kCgBatch];
         ctx->read_results(s_nb, nb, nrm);
         for (int t = 0; t < nb; ++t) {

@@ -1,5 +1,7 @@
 """Solvers through the C ABI against the oracle (FP64 parity 1e-12) and
 size-independent properties at the full C192 x 70 size."""
+import os
+
 import numpy as np
 import pytest
 
@@ -146,6 +148,47 @@ def test_cg_convergence_found_inside_a_read_batch(ctx):
     x_ref, st, info = OraW0(p, A).cg_solve(p.rhs, r_tol=1e-8, max_iter=k - 3)
     assert info.iterations == k - 3
     assert rel(x_s, x_ref) < 1e-12
+
+
+def test_graph_replay_after_the_scratch_buffer_grows():
+    """Monitored CG replays its full batches from a captured graph whose LMA
+    applies hold the context's scratch buffer.  When a larger operator then
+    grows that buffer (freeing the old one), the next solve captures again
+    instead of replaying the freed address: every solve of the same system
+    into the same x gives the same bits."""
+    c = api.Context(int(os.environ.get("LFG_DEVICE", "0")))
+    try:
+        p = w0_problem(6, 5, seed=1, top=5e3)
+        A = p.matrix()
+        nent, nlev = p.nvert, p.nlayers + 1
+        lma = api.LocalOperator(c, R_DOUBLE, p.ncell, p.nlayers, A, p.map, nent, nlev)
+        diag = Field(c, R_DOUBLE, nent, nlev)
+        lma.diagonal(diag)
+        B, X = field_from(c, p.rhs, nent, nlev), Field(c, R_DOUBLE, nent, nlev)
+        sol = api.IterativeSolver(api.LinearOperator.from_lma(lma),
+                                  api.Preconditioner.diagonal(diag), diag, "cg", r_tol=1e-8,
+                                  max_iter=2000)
+
+        def solve():
+            X.set_scalar(0.0)
+            out = sol.apply(X, B)
+            assert out.status == 0 and out.iterations > 8
+            return out.iterations, X.export()
+
+        k0, x0 = solve()           # eager
+        for _ in range(2):         # captured, then replayed
+            k, x = solve()
+            assert k == k0 and np.array_equal(x, x0)
+        big = w0_problem(24, 20, seed=2, top=2e4)
+        lb = api.LocalOperator(c, R_DOUBLE, big.ncell, big.nlayers, big.matrix(), big.map,
+                               big.nvert, big.nlayers + 1)
+        yb = Field(c, R_DOUBLE, big.nvert, big.nlayers + 1)
+        lb.apply(api.LMA_WRITE, yb, field_from(c, big.rhs, big.nvert, big.nlayers + 1))
+        for _ in range(3):         # eager after the growth, captured, replayed
+            k, x = solve()
+            assert k == k0 and np.array_equal(x, x0)
+    finally:
+        c.close()
 
 
 @pytest.mark.parametrize("method,iters", [("bicgstab", 6), ("gmres", 2), ("fgmres", 2)])
