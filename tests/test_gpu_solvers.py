@@ -35,6 +35,44 @@ def test_gcr_multigrid_fp64_parity(ctx, helm24):
     assert abs(res.final_err - info.final_err) / info.final_err < 1e-6
 
 
+def test_gcr_repeated_solves_give_the_same_bits(ctx, helm24):
+    """Monitored GCR with the multigrid preconditioner (whose V-cycles are
+    replayed from captured graphs from their second use on): every solve
+    takes the oracle's iteration count and gives the first solve's bits,
+    with convergence inside a restart, at the last step the iteration
+    limit allows, and a limit that stops it before convergence
+    (NOT_CONVERGED after exactly that many steps)."""
+    p = helm24
+    x_ref, st_ref, info = OraHelm(p).gcr_mg_solve(p.rhs, gcrk=10, r_tol=1e-8, max_iter=20)
+    S = api.HelmholtzSystem(ctx, p, mixed=False)
+    outs = []
+    for _ in range(3):
+        res = S.solve_fp64(p.rhs)
+        outs.append((res.status, res.iterations, res.final_err, S.solution()))
+    assert outs[0][:2] == (st_ref, info.iterations)
+    for o in outs[1:]:
+        assert o[:3] == outs[0][:3]
+        assert np.array_equal(o[3], outs[0][3])
+    assert rel(outs[-1][3], x_ref) < 1e-12
+    K = info.iterations
+    B = S.op64.field(p.rhs)
+    for gcrk, max_iter in ((3, 20), (K, 1), (3, 1)):
+        sol = api.IterativeSolver(api.LinearOperator.from_helmholtz(S.op64), S.mg64, S.x64,
+                                  "gcr", r_tol=1e-8, max_iter=max_iter, gcrk=gcrk)
+        runs = []
+        for _ in range(3):
+            X = S.op64.field()
+            out = sol.apply(X, B)
+            runs.append((out.status, out.iterations, out.final_err, X.export()))
+        for r in runs[1:]:
+            assert r[:3] == runs[0][:3]
+            assert np.array_equal(r[3], runs[0][3])
+        if gcrk * max_iter < K:
+            assert runs[0][0] == api.NOT_CONVERGED and runs[0][1] == gcrk * max_iter
+        else:
+            assert runs[0][0] == 0
+
+
 def test_mixed_refinement_parity(ctx, helm24):
     p = helm24
     ora = OraHelm(p)
