@@ -98,7 +98,11 @@ __global__ void __launch_bounds__(128) k_cma_asm_rows(T* __restrict__ bands, int
 // entries (layer k, dofs d1, d2 of W3, band b) in the reference's loop
 // order, each adding sum over d3 of Dh(d1, d3) Dh(d2, d3) / M2h(d3, d3) at
 // layer k, formed in the element matrices' precision as in k_cma_asm_hmht.
-template <class T, class TL, int BW>
+// Q > 0 and NDF > 0 (rows of at most Q entries, ndf2h = NDF): every load of
+// the row issued before the first product (the loads in flight together; a
+// loop over d3 left each thread one load at a time: 85 -> 58 us on C96 x 70
+// W3); otherwise loops over any number of entries and dofs.
+template <class T, class TL, int BW, int Q, int NDF>
 __global__ void __launch_bounds__(128) k_cma_hmht_rows(T* __restrict__ bands, int ncol, int nrow,
                                                        int bw, const TL* __restrict__ dh,
                                                        const TL* __restrict__ m2h, int ndf2h,
@@ -110,17 +114,46 @@ __global__ void __launch_bounds__(128) k_cma_hmht_rows(T* __restrict__ bands, in
   T acc[BW];
 #pragma unroll
   for (int b = 0; b < BW; ++b) acc[b] = (T)0;
-  for (int q = rowptr[i]; q < rowptr[i + 1]; ++q) {
-    const int2 e = contrib[q];
-    const int k = e.x & 0xffff, d1 = (e.x >> 16) & 0xff, d2 = (int)((unsigned)e.x >> 24);
-    TL tmp = (TL)0;
-    for (int d3 = 0; d3 < ndf2h; ++d3)
-      tmp = tmp + dh[(((size_t)d1 * ndf2h + d3) * nl + k) * ncol + c] *
-                      dh[(((size_t)d2 * ndf2h + d3) * nl + k) * ncol + c] /
-                      m2h[(((size_t)d3 * ndf2h + d3) * nl + k) * ncol + c];
+  const int q0 = rowptr[i], q1 = rowptr[i + 1];
+  if constexpr (Q > 0 && NDF > 0) {
+    int2 e[Q];
+    TL x1[Q][NDF], x2[Q][NDF], mm[Q][NDF];
 #pragma unroll
-    for (int b = 0; b < BW; ++b)
-      if (b == e.y) acc[b] = acc[b] + (T)tmp;
+    for (int u = 0; u < Q; ++u) e[u] = q0 + u < q1 ? contrib[q0 + u] : make_int2(0, -1);
+#pragma unroll
+    for (int u = 0; u < Q; ++u) {
+      const int k = e[u].x & 0xffff, d1 = (e[u].x >> 16) & 0xff,
+                d2 = (int)((unsigned)e[u].x >> 24);
+      const bool on = e[u].y >= 0;
+#pragma unroll
+      for (int d3 = 0; d3 < NDF; ++d3) {
+        x1[u][d3] = on ? dh[(((size_t)d1 * NDF + d3) * nl + k) * ncol + c] : (TL)0;
+        x2[u][d3] = on ? dh[(((size_t)d2 * NDF + d3) * nl + k) * ncol + c] : (TL)0;
+        mm[u][d3] = on ? m2h[(((size_t)d3 * NDF + d3) * nl + k) * ncol + c] : (TL)1;
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < Q; ++u) {
+      TL tmp = (TL)0;
+#pragma unroll
+      for (int d3 = 0; d3 < NDF; ++d3) tmp = tmp + x1[u][d3] * x2[u][d3] / mm[u][d3];
+#pragma unroll
+      for (int b = 0; b < BW; ++b)
+        if (b == e[u].y) acc[b] = acc[b] + (T)tmp;
+    }
+  } else {
+    for (int q = q0; q < q1; ++q) {
+      const int2 e = contrib[q];
+      const int k = e.x & 0xffff, d1 = (e.x >> 16) & 0xff, d2 = (int)((unsigned)e.x >> 24);
+      TL tmp = (TL)0;
+      for (int d3 = 0; d3 < ndf2h; ++d3)
+        tmp = tmp + dh[(((size_t)d1 * ndf2h + d3) * nl + k) * ncol + c] *
+                        dh[(((size_t)d2 * ndf2h + d3) * nl + k) * ncol + c] /
+                        m2h[(((size_t)d3 * ndf2h + d3) * nl + k) * ncol + c];
+#pragma unroll
+      for (int b = 0; b < BW; ++b)
+        if (b == e.y) acc[b] = acc[b] + (T)tmp;
+    }
   }
   const size_t plane = (size_t)nrow * ncol;
 #pragma unroll
@@ -154,6 +187,57 @@ __global__ void k_cma_mul(T* __restrict__ cb, const int* __restrict__ jmC,
     cb[o] = cb[o] + e;
   }
   (void)bwC;
+}
+
+// The same product with A's band span at most MA and C's at most MC: A's and
+// C's entries of the row and every B entry a term needs are loaded before
+// the first product; the terms are added in the same order.
+template <class T, int MA, int MC>
+__global__ void __launch_bounds__(128) k_cma_mul_u(T* __restrict__ cb, const int* __restrict__ jmC,
+                                                   const int* __restrict__ jpC, int ncolC,
+                                                   const T* __restrict__ ab,
+                                                   const int* __restrict__ jmA,
+                                                   const int* __restrict__ jpA, int ncolA,
+                                                   const T* __restrict__ bb,
+                                                   const int* __restrict__ jmB,
+                                                   const int* __restrict__ jpB, int nrowA,
+                                                   int nrowB, int ncol) {
+  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  const int i = blockIdx.y;
+  if (c >= ncol) return;
+  const int jmc = jmC[i], jma = jmA[i];
+  const int j0 = max(0, jmc), j1 = min(ncolC - 1, jpC[i]);
+  const int l0 = max(0, jma), l1 = min(ncolA - 1, jpA[i]);
+  T av[MA], cv[MC], bv[MC][MA];
+  int jmb[MA], jpb[MA];
+#pragma unroll
+  for (int u = 0; u < MA; ++u) {
+    const int l = l0 + u;
+    const bool on = l <= l1;
+    jmb[u] = on ? jmB[l] : 1;
+    jpb[u] = on ? jpB[l] : 0;
+    av[u] = on ? ab[((size_t)(l - jma) * nrowA + i) * ncol + c] : (T)0;
+  }
+#pragma unroll
+  for (int v = 0; v < MC; ++v) {
+    const int j = j0 + v;
+    cv[v] = j <= j1 ? cb[((size_t)(j - jmc) * gridDim.y + i) * ncol + c] : (T)0;
+#pragma unroll
+    for (int u = 0; u < MA; ++u) {
+      const bool on = j <= j1 && jmb[u] <= j && j <= jpb[u];
+      bv[v][u] = on ? bb[((size_t)(j - jmb[u]) * nrowB + l0 + u) * ncol + c] : (T)0;
+    }
+  }
+#pragma unroll
+  for (int v = 0; v < MC; ++v) {
+    const int j = j0 + v;
+    if (j > j1) break;
+    T e = (T)0;
+#pragma unroll
+    for (int u = 0; u < MA; ++u)
+      if (jmb[u] <= j && j <= jpb[u]) e = e + av[u] * bv[v][u];
+    cb[((size_t)(j - jmc) * gridDim.y + i) * ncol + c] = cv[v] + e;
+  }
 }
 
 // columnwise_op_scaledadd_kernel_code, one thread per (row i of C, column):
@@ -286,9 +370,11 @@ void cached_rows(lfg_cma m, std::vector<int> key, F&& build) {
   build(rows);
   std::vector<int> rowptr(1, 0);
   std::vector<int2> list;
+  int maxq = 0;
   for (const auto& r : rows) {
     list.insert(list.end(), r.begin(), r.end());
     rowptr.push_back((int)list.size());
+    maxq = std::max(maxq, (int)r.size());
   }
   LFG_CUDA(cudaStreamSynchronize(m->ctx->stream));  // earlier assemblies may read the lists
   dfree(m->asm_rowptr);
@@ -301,6 +387,7 @@ void cached_rows(lfg_cma m, std::vector<int> key, F&& build) {
   m->asm_list = (int*)dmalloc(std::max<size_t>(1, list.size()) * sizeof(int2));
   if (!list.empty()) upload(m->asm_list, list.data(), list.size() * sizeof(int2));
   m->asm_key = std::move(key);
+  m->asm_maxq = maxq;
 }
 
 // the dofmap's values as a key tail
@@ -365,12 +452,12 @@ int lfg_cma_assemble(lfg_cma m, lfg_lma a, const int* cb_to, const int* cb_from)
         });
         LFG_CUDA(cudaStreamSynchronize(c->stream));  // the dofmap copies are freed on return
       }
-      const dim3 g2(grid, m->nrow);
       dispatch_kind(m->kind, [&](auto t) {
         using T = decltype(t);
         dispatch_kind(a->kind, [&](auto tl) {
           using TL = decltype(tl);
           auto go = [&](auto k) {
+            const dim3 g2(grid, m->nrow);
             k<<<g2, 128, 0, c->stream>>>((T*)m->bands, m->ncol, m->nrow, m->bw,
                                          (const TL*)a->a, m->asm_rowptr,
                                          (const int2*)m->asm_list);
@@ -415,26 +502,51 @@ int lfg_cma_multiply(lfg_cma C, lfg_cma A, lfg_cma B) {
     LFG_REQUIRE(A->ncol == C->ncol && B->ncol == C->ncol, "cma_multiply: cell counts differ");
     LFG_REQUIRE(A->nrow == C->nrow && A->ncolumn == B->nrow && B->ncolumn == C->ncolumn,
                 "cma_multiply: shapes do not chain (C nrow x ncol = A nrow x B ncol)");
-    // every product entry must have a slot in C's band
-    {
+    // every product entry must have a slot in C's band; the widest spans of
+    // A's and C's rows pick the kernel.  Both follow from the three shapes
+    // (the band limits are functions of alpha, beta, gamma), so a product of
+    // the same shapes as the last one skips the host check and stays
+    // asynchronous.
+    std::vector<int> key;
+    for (lfg_cma m : {A, B, C})
+      key.insert(key.end(), {m->nrow, m->ncolumn, m->bw, m->alpha, m->beta, m->gm, m->gp});
+    int span_a = 0, span_c = 0;
+    if (key == C->mul_key) {
+      span_a = C->mul_span_a;
+      span_c = C->mul_span_c;
+    } else {
       const auto jmA = host_ints(A->jminus, A->nrow), jpA = host_ints(A->jplus, A->nrow);
       const auto jmB = host_ints(B->jminus, B->nrow), jpB = host_ints(B->jplus, B->nrow);
       const auto jmC = host_ints(C->jminus, C->nrow), jpC = host_ints(C->jplus, C->nrow);
       for (int i = 0; i < C->nrow; ++i) {
         LFG_REQUIRE(jpC[i] - jmC[i] + 1 <= C->bw, "cma_multiply: C band too narrow");
+        span_a = std::max(span_a, std::min(A->ncolumn - 1, jpA[i]) - std::max(0, jmA[i]) + 1);
+        span_c = std::max(span_c, std::min(C->ncolumn - 1, jpC[i]) - std::max(0, jmC[i]) + 1);
         for (int l = std::max(0, jmA[i]); l <= std::min(A->ncolumn - 1, jpA[i]); ++l)
           for (int j = std::max(jmB[l], std::max(0, jmC[i]));
                j <= std::min(jpB[l], std::min(C->ncolumn - 1, jpC[i])); ++j)
             LFG_REQUIRE(j - jmC[i] >= 0 && j - jmC[i] < C->bw, "cma_multiply: band overflow");
       }
+      C->mul_key = key;
+      C->mul_span_a = span_a;
+      C->mul_span_c = span_c;
     }
     dim3 grid((C->ncol + 127) / 128, C->nrow);
     dispatch_kind(C->kind, [&](auto t) {
       using T = decltype(t);
-      k_cma_mul<T><<<grid, 128, 0, c->stream>>>(
-          (T*)C->bands, C->jminus, C->jplus, C->ncolumn, C->bw, (const T*)A->bands, A->jminus,
-          A->jplus, A->ncolumn, (const T*)B->bands, B->jminus, B->jplus, A->nrow, B->nrow,
-          C->ncol);
+      auto go = [&](auto k) {
+        k<<<grid, 128, 0, c->stream>>>((T*)C->bands, C->jminus, C->jplus, C->ncolumn,
+                                       (const T*)A->bands, A->jminus, A->jplus, A->ncolumn,
+                                       (const T*)B->bands, B->jminus, B->jplus, A->nrow, B->nrow,
+                                       C->ncol);
+      };
+      if (span_a <= 2 && span_c <= 4) go(k_cma_mul_u<T, 2, 4>);
+      else if (span_a <= 4 && span_c <= 8) go(k_cma_mul_u<T, 4, 8>);
+      else
+        k_cma_mul<T><<<grid, 128, 0, c->stream>>>(
+            (T*)C->bands, C->jminus, C->jplus, C->ncolumn, C->bw, (const T*)A->bands, A->jminus,
+            A->jplus, A->ncolumn, (const T*)B->bands, B->jminus, B->jplus, A->nrow, B->nrow,
+            C->ncol);
     });
     after_launch(c, "cma_mul");
     C->fvalid = false;  // the bands changed
@@ -506,19 +618,28 @@ int lfg_cma_assemble_diag_hmht(lfg_cma m, lfg_lma dh, lfg_lma m2h, const int* cb
         });
         LFG_CUDA(cudaStreamSynchronize(c->stream));
       }
-      const dim3 g2(grid, m->nrow);
       dispatch_kind(m->kind, [&](auto t) {
         using T = decltype(t);
         dispatch_kind(dh->kind, [&](auto tl) {
           using TL = decltype(tl);
           auto go = [&](auto k) {
+            const dim3 g2(grid, m->nrow);
             k<<<g2, 128, 0, c->stream>>>((T*)m->bands, m->ncol, m->nrow, m->bw,
                                          (const TL*)dh->a, (const TL*)m2h->a, dh->ndf_from,
                                          dh->nl, m->asm_rowptr, (const int2*)m->asm_list);
           };
-          if (m->bw <= 2) go(k_cma_hmht_rows<T, TL, 2>);
-          else if (m->bw <= 4) go(k_cma_hmht_rows<T, TL, 4>);
-          else go(k_cma_hmht_rows<T, TL, 8>);
+          const int q = m->asm_maxq;
+          const bool n4 = dh->ndf_from == 4;
+          if (m->bw <= 2) {
+            if (n4 && q <= 1) go(k_cma_hmht_rows<T, TL, 2, 1, 4>);
+            else if (n4 && q <= 2) go(k_cma_hmht_rows<T, TL, 2, 2, 4>);
+            else go(k_cma_hmht_rows<T, TL, 2, 0, 0>);
+          } else if (m->bw <= 4) {
+            if (n4 && q <= 4) go(k_cma_hmht_rows<T, TL, 4, 4, 4>);
+            else go(k_cma_hmht_rows<T, TL, 4, 0, 0>);
+          } else {
+            go(k_cma_hmht_rows<T, TL, 8, 0, 0>);
+          }
         });
       });
       after_launch(c, "cma_asm_diag_hmht");
@@ -564,12 +685,12 @@ int lfg_cma_assemble_m2v_lumped_inv(lfg_cma m, lfg_lma mm, const int* cbm) {
         });
         LFG_CUDA(cudaStreamSynchronize(c->stream));
       }
-      const dim3 g2(grid, m->nrow);
       dispatch_kind(m->kind, [&](auto t) {
         using T = decltype(t);
         dispatch_kind(mm->kind, [&](auto tl) {
           using TL = decltype(tl);
           auto go = [&](auto k) {
+            const dim3 g2(grid, m->nrow);
             k<<<g2, 128, 0, c->stream>>>((T*)m->bands, m->ncol, m->nrow, m->bw,
                                          (const TL*)mm->a, m->asm_rowptr,
                                          (const int2*)m->asm_list);

@@ -283,6 +283,11 @@ struct lfg_cma_s {
   std::vector<int> asm_key;
   int* asm_rowptr = nullptr;  // device [nrow+1]
   int* asm_list = nullptr;    // device int2 [rowptr[nrow]]
+  int asm_maxq = 0;           // most contributions of one row
+  // shapes of the last product C = C + A B into this operator, and the
+  // widest spans of A's and C's rows
+  std::vector<int> mul_key;
+  int mul_span_a = 0, mul_span_c = 0;
 };
 
 struct lfg_lma_s {
