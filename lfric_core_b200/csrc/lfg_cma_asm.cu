@@ -73,6 +73,7 @@ __global__ void __launch_bounds__(128) k_cma_asm_rows(T* __restrict__ bands, int
                                                       int bw, const TL* __restrict__ a,
                                                       const int* __restrict__ rowptr,
                                                       const int2* __restrict__ contrib) {
+  grid_dep_wait();
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = blockIdx.y;
   if (c >= ncol) return;
@@ -108,6 +109,7 @@ __global__ void __launch_bounds__(128) k_cma_hmht_rows(T* __restrict__ bands, in
                                                        const TL* __restrict__ m2h, int ndf2h,
                                                        int nl, const int* __restrict__ rowptr,
                                                        const int2* __restrict__ contrib) {
+  grid_dep_wait();
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = blockIdx.y;
   if (c >= ncol) return;
@@ -202,6 +204,7 @@ __global__ void __launch_bounds__(128) k_cma_mul_u(T* __restrict__ cb, const int
                                                    const int* __restrict__ jmB,
                                                    const int* __restrict__ jpB, int nrowA,
                                                    int nrowB, int ncol) {
+  grid_dep_wait();
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   const int i = blockIdx.y;
   if (c >= ncol) return;
@@ -457,10 +460,8 @@ int lfg_cma_assemble(lfg_cma m, lfg_lma a, const int* cb_to, const int* cb_from)
         dispatch_kind(a->kind, [&](auto tl) {
           using TL = decltype(tl);
           auto go = [&](auto k) {
-            const dim3 g2(grid, m->nrow);
-            k<<<g2, 128, 0, c->stream>>>((T*)m->bands, m->ncol, m->nrow, m->bw,
-                                         (const TL*)a->a, m->asm_rowptr,
-                                         (const int2*)m->asm_list);
+            launch_pdl(c, k, dim3(grid, m->nrow), dim3(128), 0, (T*)m->bands, m->ncol, m->nrow,
+                       m->bw, (const TL*)a->a, m->asm_rowptr, (const int2*)m->asm_list);
           };
           if (m->bw <= 2) go(k_cma_asm_rows<T, TL, 2>);
           else if (m->bw <= 4) go(k_cma_asm_rows<T, TL, 4>);
@@ -535,10 +536,9 @@ int lfg_cma_multiply(lfg_cma C, lfg_cma A, lfg_cma B) {
     dispatch_kind(C->kind, [&](auto t) {
       using T = decltype(t);
       auto go = [&](auto k) {
-        k<<<grid, 128, 0, c->stream>>>((T*)C->bands, C->jminus, C->jplus, C->ncolumn,
-                                       (const T*)A->bands, A->jminus, A->jplus, A->ncolumn,
-                                       (const T*)B->bands, B->jminus, B->jplus, A->nrow, B->nrow,
-                                       C->ncol);
+        launch_pdl(c, k, grid, dim3(128), 0, (T*)C->bands, C->jminus, C->jplus, C->ncolumn,
+                   (const T*)A->bands, A->jminus, A->jplus, A->ncolumn, (const T*)B->bands,
+                   B->jminus, B->jplus, A->nrow, B->nrow, C->ncol);
       };
       if (span_a <= 2 && span_c <= 4) go(k_cma_mul_u<T, 2, 4>);
       else if (span_a <= 4 && span_c <= 8) go(k_cma_mul_u<T, 4, 8>);
@@ -623,10 +623,9 @@ int lfg_cma_assemble_diag_hmht(lfg_cma m, lfg_lma dh, lfg_lma m2h, const int* cb
         dispatch_kind(dh->kind, [&](auto tl) {
           using TL = decltype(tl);
           auto go = [&](auto k) {
-            const dim3 g2(grid, m->nrow);
-            k<<<g2, 128, 0, c->stream>>>((T*)m->bands, m->ncol, m->nrow, m->bw,
-                                         (const TL*)dh->a, (const TL*)m2h->a, dh->ndf_from,
-                                         dh->nl, m->asm_rowptr, (const int2*)m->asm_list);
+            launch_pdl(c, k, dim3(grid, m->nrow), dim3(128), 0, (T*)m->bands, m->ncol, m->nrow,
+                       m->bw, (const TL*)dh->a, (const TL*)m2h->a, dh->ndf_from, dh->nl,
+                       m->asm_rowptr, (const int2*)m->asm_list);
           };
           const int q = m->asm_maxq;
           const bool n4 = dh->ndf_from == 4;
@@ -690,10 +689,8 @@ int lfg_cma_assemble_m2v_lumped_inv(lfg_cma m, lfg_lma mm, const int* cbm) {
         dispatch_kind(mm->kind, [&](auto tl) {
           using TL = decltype(tl);
           auto go = [&](auto k) {
-            const dim3 g2(grid, m->nrow);
-            k<<<g2, 128, 0, c->stream>>>((T*)m->bands, m->ncol, m->nrow, m->bw,
-                                         (const TL*)mm->a, m->asm_rowptr,
-                                         (const int2*)m->asm_list);
+            launch_pdl(c, k, dim3(grid, m->nrow), dim3(128), 0, (T*)m->bands, m->ncol, m->nrow,
+                       m->bw, (const TL*)mm->a, m->asm_rowptr, (const int2*)m->asm_list);
           };
           if (m->bw <= 2) go(k_cma_asm_rows<T, TL, 2, true>);
           else if (m->bw <= 4) go(k_cma_asm_rows<T, TL, 4, true>);
