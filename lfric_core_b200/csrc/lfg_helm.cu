@@ -686,11 +686,11 @@ __global__ void __launch_bounds__(256) k_helm_panel(HelmArgs<T> A, PanelArgs P,
 // The children's residuals are summed in the cell map's slot order (the
 // per-panel placement qpos), as the per-coarse-column code does; the
 // coarse border columns (cedge) run that code, one level each, in the
-// threads just before the same level's interior ones.  Four blocks per SM
-// (64 registers a thread): the extra resident warps hide more load latency
-// than the few spilled bytes cost (126 -> 114 us at C192x70).
+// threads just before the same level's interior ones.  No minimum of
+// blocks per SM: a bound of four (64 registers a thread) spilled and
+// measured 113.7 against 112.0 us at C192x70.
 template <class T, bool CF>
-__global__ void __launch_bounds__(256, 4) k_helm_resid_restrict_panel(
+__global__ void __launch_bounds__(256) k_helm_resid_restrict_panel(
     HelmArgs<T> A, PanelArgs P, const T* __restrict__ x, const T* __restrict__ b,
     T* __restrict__ bc, const int* __restrict__ child, int ncoarse, unsigned long long qpos,
     const int* __restrict__ cedge, int ncedge) {
