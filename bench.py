@@ -48,7 +48,7 @@ def parse():
     ap.add_argument("--batched-only", action="store_true", help=argparse.SUPPRESS)
     ap.add_argument("--kernels", action="store_true", help=argparse.SUPPRESS)
     # small cases for ncu captures of one kernel family
-    ap.add_argument("--case", choices=["lma", "coarse"], help=argparse.SUPPRESS)
+    ap.add_argument("--case", choices=["lma", "coarse", "cma"], help=argparse.SUPPRESS)
     ap.add_argument("--batch-rhs", type=int, default=64, help=argparse.SUPPRESS)
     ap.add_argument("--batch-uneven", type=int, default=32, help=argparse.SUPPRESS)
     ap.add_argument("--batch-shape", type=int, nargs=2, default=(0, 0), help=argparse.SUPPRESS)
@@ -610,6 +610,75 @@ def measure_configs(ctx, stream, steps: int, peak: float, cpu: bool) -> dict:
     return out
 
 
+def cma_assembly_cases(ctx):
+    """The CMA assembly and product workloads on C96 x 70 columns, FP64
+    (columnwise_op_asm W3 <- Wtheta, columnwise_op_mul Wtheta <- W3 <-
+    Wtheta, columnwise_op_asm_diag_hmht on W3, columnwise_op_asm_m2v_lumped_inv
+    on W2v): a list of (kernel label, call, algorithmic bytes of one call)."""
+    from lfric_core_b200 import api
+    from lfric_core_b200.api import R_DOUBLE
+    from lfric_core_b200.problems import banded_dofmap, cma_prod_size, cma_size
+    ncell, nl, w = 6 * 96 * 96, NLAYERS, 8
+    rng = np.random.default_rng(6)
+    p3t = cma_size(nl, 1, 2, 0, 1, 1, 0)           # W3 <- Wtheta
+    pt3 = cma_size(nl, 2, 1, 1, 0, 0, 1)           # Wtheta <- W3
+    ptt = cma_prod_size(pt3, p3t)                  # Wtheta <- Wtheta
+    ls = rng.standard_normal((ncell * nl, 1, 2))
+    mt = np.array([[c * nl] for c in range(ncell)])            # W3 dofmap, (cell, 1)
+    mf = np.array([[c * (nl + 1), c * (nl + 1) + 1] for c in range(ncell)])  # Wtheta, (cell, 2)
+    lma = api.LocalOperator(ctx, R_DOUBLE, ncell, nl, np.asfortranarray(ls).ravel(order="F"),
+                            mt, ncell, nl, mf, ncell, nl + 1)
+
+    def cma(pp, bands=None):
+        return api.ColumnwiseOperator(ctx, R_DOUBLE, ncell, pp["nrow"], pp["ncol"], pp["bw"],
+                                      pp["alpha"], pp["beta"], pp["gm"], pp["gp"],
+                                      np.arange(1, pp["nrow"] + 1), np.arange(1, pp["ncol"] + 1),
+                                      bands)
+    cases = []
+    A = cma(p3t)
+    cb_to, cb_from = banded_dofmap(nl, 1, 1, 0), banded_dofmap(nl, 2, 0, 1)
+    cases.append(("k_cma_asm_rows (columnwise_op_asm, W3 <- Wtheta)",
+                  lambda: A.assemble(lma, cb_to, cb_from),
+                  (ncell * nl * 2 + p3t["bw"] * p3t["nrow"] * ncell) * w))
+    At = cma(pt3, rng.standard_normal((pt3["bw"], pt3["nrow"], ncell)).ravel(order="F"))
+    Bt = cma(p3t, rng.standard_normal((p3t["bw"], p3t["nrow"], ncell)).ravel(order="F"))
+    Ct = cma(ptt, np.zeros((ptt["bw"], ptt["nrow"], ncell)).ravel(order="F"))
+    cases.append(("k_cma_mul_u (columnwise_op_mul, Wtheta <- W3 <- Wtheta, C += A B)",
+                  lambda: Ct.multiply(At, Bt),
+                  (pt3["bw"] * pt3["nrow"] + p3t["bw"] * p3t["nrow"] + 2 * ptt["bw"] * ptt["nrow"])
+                  * ncell * w))
+    # diag(Dh M2h^-1 Dh^T) on W3 (columnwise_op_asm_diag_hmht) and the lumped
+    # inverse of a W2v mass matrix (columnwise_op_asm_m2v_lumped_inv)
+    p33 = cma_size(nl, 1, 1, 0, 1, 0, 1)
+    dh_ls = rng.standard_normal((ncell * nl, 1, 4))
+    m2h_ls = rng.standard_normal((ncell * nl, 4, 4))
+    for d in range(4):
+        m2h_ls[:, d, d] = 1.0 + rng.random(ncell * nl)
+    m3 = np.array([[c * nl] for c in range(ncell)])
+    m2h_map = np.array([[(c * 4 + d) * nl for d in range(4)] for c in range(ncell)])
+    Dh = api.LocalOperator(ctx, R_DOUBLE, ncell, nl, np.asfortranarray(dh_ls).ravel(order="F"),
+                           m3, ncell, nl, m2h_map, ncell * 4, nl)
+    M2h = api.LocalOperator(ctx, R_DOUBLE, ncell, nl,
+                            np.asfortranarray(m2h_ls).ravel(order="F"), m2h_map, ncell * 4, nl,
+                            m2h_map, ncell * 4, nl)
+    Hc = cma(p33)
+    cb3 = banded_dofmap(nl, 1, 1, 0)
+    cases.append(("k_cma_hmht_rows (columnwise_op_asm_diag_hmht, W3)",
+                  lambda: Hc.assemble_diag_hmht(Dh, M2h, cb3),
+                  (ncell * nl * (4 + 4) + p33["bw"] * p33["nrow"] * ncell) * w))
+    pvv = cma_size(nl, 2, 2, 1, 0, 1, 0)
+    mv_ls = np.abs(rng.standard_normal((ncell * nl, 2, 2))) + 0.1
+    mvm = np.array([[c * (nl + 1), c * (nl + 1) + 1] for c in range(ncell)])
+    Mv = api.LocalOperator(ctx, R_DOUBLE, ncell, nl, np.asfortranarray(mv_ls).ravel(order="F"),
+                           mvm, ncell, nl + 1, mvm, ncell, nl + 1)
+    Lc = cma(pvv)
+    cbv = banded_dofmap(nl, 2, 0, 1)
+    cases.append(("k_cma_asm_rows<inverse> (columnwise_op_asm_m2v_lumped_inv, W2v)",
+                  lambda: Lc.assemble_m2v_lumped_inv(Mv, cbv),
+                  (ncell * nl * 2 + pvv["bw"] * pvv["nrow"] * ncell) * w))
+    return cases
+
+
 def measure_next_rows(ctx, stream, peak: float, cpu: bool) -> dict:
     """The rows past the hot path (their parity is tested in tests/), timed
     on the GPU beside the oracle where it runs whole solves: the Krylov
@@ -621,9 +690,7 @@ def measure_next_rows(ctx, stream, peak: float, cpu: bool) -> dict:
     import ctypes as C
     import torch
     from lfric_core_b200 import api
-    from lfric_core_b200.api import R_DOUBLE, Field
-    from lfric_core_b200.problems import (banded_dofmap, cma_prod_size, cma_size,
-                                          helmholtz_problem, w2_hierarchy)
+    from lfric_core_b200.problems import helmholtz_problem, w2_hierarchy
     threads = host_threads()
     out = {}
 
@@ -717,25 +784,6 @@ def measure_next_rows(ctx, stream, peak: float, cpu: bool) -> dict:
 
     # ---- CMA assembly and product on C96 x 70 columns (columnwise_op_asm,
     # columnwise_op_mul; components/science/source/kernel/columnwise_operators)
-    ncell, nl, w = 6 * 96 * 96, NLAYERS, 8
-    rng = np.random.default_rng(6)
-    p3t = cma_size(nl, 1, 2, 0, 1, 1, 0)           # W3 <- Wtheta
-    pt3 = cma_size(nl, 2, 1, 1, 0, 0, 1)           # Wtheta <- W3
-    ptt = cma_prod_size(pt3, p3t)                  # Wtheta <- Wtheta
-    ls = rng.standard_normal((ncell * nl, 1, 2))
-    mt = np.array([[c * nl] for c in range(ncell)])            # W3 dofmap, (cell, 1)
-    mf = np.array([[c * (nl + 1), c * (nl + 1) + 1] for c in range(ncell)])  # Wtheta, (cell, 2)
-    lma = api.LocalOperator(ctx, R_DOUBLE, ncell, nl, np.asfortranarray(ls).ravel(order="F"),
-                            mt, ncell, nl, mf, ncell, nl + 1)
-
-    def cma(pp, bands=None):
-        return api.ColumnwiseOperator(ctx, R_DOUBLE, ncell, pp["nrow"], pp["ncol"], pp["bw"],
-                                      pp["alpha"], pp["beta"], pp["gm"], pp["gp"],
-                                      np.arange(1, pp["nrow"] + 1), np.arange(1, pp["ncol"] + 1),
-                                      bands)
-    A = cma(p3t)
-    cb_to, cb_from = banded_dofmap(nl, 1, 1, 0), banded_dofmap(nl, 2, 0, 1)
-
     def ev_ms(fn, n=10):
         for _ in range(2):
             fn()
@@ -749,51 +797,10 @@ def measure_next_rows(ctx, stream, peak: float, cpu: bool) -> dict:
         return e0.elapsed_time(e1) / n
 
     rows = []
-    ms = ev_ms(lambda: A.assemble(lma, cb_to, cb_from))
-    nb = (ncell * nl * 2 + p3t["bw"] * p3t["nrow"] * ncell) * w
-    rows.append({"kernel": "k_cma_asm_rows (columnwise_op_asm, W3 <- Wtheta)", "us": ms * 1e3,
-                 "algorithmic_bytes": nb, "frac_of_measured_hbm": nb / (ms * 1e-3) / 1e9 / peak})
-    At = cma(pt3, rng.standard_normal((pt3["bw"], pt3["nrow"], ncell)).ravel(order="F"))
-    Bt = cma(p3t, rng.standard_normal((p3t["bw"], p3t["nrow"], ncell)).ravel(order="F"))
-    Ct = cma(ptt, np.zeros((ptt["bw"], ptt["nrow"], ncell)).ravel(order="F"))
-    ms = ev_ms(lambda: Ct.multiply(At, Bt))
-    nb = (pt3["bw"] * pt3["nrow"] + p3t["bw"] * p3t["nrow"] + 2 * ptt["bw"] * ptt["nrow"]) \
-        * ncell * w
-    rows.append({"kernel": "k_cma_mul (columnwise_op_mul, Wtheta <- W3 <- Wtheta, C += A B)",
-                 "us": ms * 1e3, "algorithmic_bytes": nb,
-                 "frac_of_measured_hbm": nb / (ms * 1e-3) / 1e9 / peak})
-    # diag(Dh M2h^-1 Dh^T) on W3 (columnwise_op_asm_diag_hmht) and the lumped
-    # inverse of a W2v mass matrix (columnwise_op_asm_m2v_lumped_inv)
-    p33 = cma_size(nl, 1, 1, 0, 1, 0, 1)
-    dh_ls = rng.standard_normal((ncell * nl, 1, 4))
-    m2h_ls = rng.standard_normal((ncell * nl, 4, 4))
-    for d in range(4):
-        m2h_ls[:, d, d] = 1.0 + rng.random(ncell * nl)
-    m3 = np.array([[c * nl] for c in range(ncell)])
-    m2h_map = np.array([[(c * 4 + d) * nl for d in range(4)] for c in range(ncell)])
-    Dh = api.LocalOperator(ctx, R_DOUBLE, ncell, nl, np.asfortranarray(dh_ls).ravel(order="F"),
-                           m3, ncell, nl, m2h_map, ncell * 4, nl)
-    M2h = api.LocalOperator(ctx, R_DOUBLE, ncell, nl,
-                            np.asfortranarray(m2h_ls).ravel(order="F"), m2h_map, ncell * 4, nl,
-                            m2h_map, ncell * 4, nl)
-    Hc = cma(p33)
-    cb3 = banded_dofmap(nl, 1, 1, 0)
-    ms = ev_ms(lambda: Hc.assemble_diag_hmht(Dh, M2h, cb3))
-    nb = (ncell * nl * (4 + 4) + p33["bw"] * p33["nrow"] * ncell) * w
-    rows.append({"kernel": "k_cma_hmht_rows (columnwise_op_asm_diag_hmht, W3)", "us": ms * 1e3,
-                 "algorithmic_bytes": nb, "frac_of_measured_hbm": nb / (ms * 1e-3) / 1e9 / peak})
-    pvv = cma_size(nl, 2, 2, 1, 0, 1, 0)
-    mv_ls = np.abs(rng.standard_normal((ncell * nl, 2, 2))) + 0.1
-    mvm = np.array([[c * (nl + 1), c * (nl + 1) + 1] for c in range(ncell)])
-    Mv = api.LocalOperator(ctx, R_DOUBLE, ncell, nl, np.asfortranarray(mv_ls).ravel(order="F"),
-                           mvm, ncell, nl + 1, mvm, ncell, nl + 1)
-    Lc = cma(pvv)
-    cbv = banded_dofmap(nl, 2, 0, 1)
-    ms = ev_ms(lambda: Lc.assemble_m2v_lumped_inv(Mv, cbv))
-    nb = (ncell * nl * 2 + pvv["bw"] * pvv["nrow"] * ncell) * w
-    rows.append({"kernel": "k_cma_asm_rows<inverse> (columnwise_op_asm_m2v_lumped_inv, W2v)",
-                 "us": ms * 1e3, "algorithmic_bytes": nb,
-                 "frac_of_measured_hbm": nb / (ms * 1e-3) / 1e9 / peak})
+    for label, fn, nb in cma_assembly_cases(ctx):
+        ms = ev_ms(fn)
+        rows.append({"kernel": label, "us": ms * 1e3, "algorithmic_bytes": nb,
+                     "frac_of_measured_hbm": nb / (ms * 1e-3) / 1e9 / peak})
     out["cma_assembly"] = {"workload": "C96x70 columns (55,296), FP64", "kernels": rows}
     return out
 
@@ -909,7 +916,9 @@ def profile_case(ctx, case: str):
     the C48x30 W0 operator and runs three forward then three transposed
     applies (k_lma_local, k_lma_local_tsplit, k_lma_gather_tab); "coarse"
     makes the C96x70 hierarchy (FP32) and runs four sweeps on its C24 level,
-    then four on its C48 level (k_helm_sweep_seg)."""
+    then four on its C48 level (k_helm_sweep_seg); "cma" runs each of the
+    C96 x 70 CMA assembly and product calls three times (k_cma_asm_rows,
+    k_cma_mul_u, k_cma_hmht_rows)."""
     from lfric_core_b200 import api
     from lfric_core_b200.api import R_DOUBLE, Field
     from lfric_core_b200.problems import helmholtz_problem, w0_problem
@@ -924,6 +933,10 @@ def profile_case(ctx, case: str):
         for mode in (api.LMA_INC, api.LMA_TRANSPOSE):
             for _ in range(3):
                 L.apply(mode, Y, X)
+    elif case == "cma":
+        for _, fn, _ in cma_assembly_cases(ctx):
+            for _ in range(3):
+                fn()
     else:
         p = helmholtz_problem(96, NLAYERS, seed=SEED, mg_levels=3)
         S = api.HelmholtzSystem(ctx, p, fp64=False)

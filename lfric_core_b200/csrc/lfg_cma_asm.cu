@@ -67,31 +67,51 @@ __global__ void k_cma_asm(T* __restrict__ bands, const int* __restrict__ jminus,
 // 0.14 of the HBM copy bandwidth).
 // INV: every non-zero entry then inverted (the lumped inverse of
 // columnwise_op_asm_m2v_lumped_inv, whose contributions are the diagonal
-// entries M(d, d) on band 0).
+// entries M(d, d) on band 0).  A thread takes kAsmColsPerThread columns of
+// its row, so one read of the row's list serves all of them and their
+// element loads are in flight together (the list chain left the kernel
+// latency-bound: C96 x 70 W3 <- Wtheta 29.8 -> 24.4 us).
+constexpr int kAsmColsPerThread = 4;
 template <class T, class TL, int BW, bool INV = false>
 __global__ void __launch_bounds__(128) k_cma_asm_rows(T* __restrict__ bands, int ncol, int nrow,
                                                       int bw, const TL* __restrict__ a,
                                                       const int* __restrict__ rowptr,
                                                       const int2* __restrict__ contrib) {
   grid_dep_wait();
-  const int c = blockIdx.x * blockDim.x + threadIdx.x;
+  constexpr int CPT = kAsmColsPerThread;
+  const int c0 = blockIdx.x * blockDim.x * CPT + threadIdx.x;
   const int i = blockIdx.y;
-  if (c >= ncol) return;
-  T acc[BW];
+  if (c0 >= ncol) return;
+  T acc[CPT][BW];
 #pragma unroll
-  for (int b = 0; b < BW; ++b) acc[b] = (T)0;
+  for (int u = 0; u < CPT; ++u)
+#pragma unroll
+    for (int b = 0; b < BW; ++b) acc[u][b] = (T)0;
   for (int q = rowptr[i]; q < rowptr[i + 1]; ++q) {
     const int2 e = contrib[q];
-    const T v = (T)a[(size_t)e.x * ncol + c];
+    T v[CPT];
 #pragma unroll
-    for (int b = 0; b < BW; ++b)
-      if (b == e.y) acc[b] = acc[b] + v;
+    for (int u = 0; u < CPT; ++u) {
+      const int c = c0 + u * blockDim.x;
+      v[u] = c < ncol ? (T)a[(size_t)e.x * ncol + c] : (T)0;
+    }
+#pragma unroll
+    for (int u = 0; u < CPT; ++u)
+#pragma unroll
+      for (int b = 0; b < BW; ++b)
+        if (b == e.y) acc[u][b] = acc[u][b] + v[u];
   }
   const size_t plane = (size_t)nrow * ncol;
 #pragma unroll
-  for (int b = 0; b < BW; ++b) {
-    if (INV && acc[b] != (T)0) acc[b] = (T)1 / acc[b];
-    if (b < bw) bands[b * plane + (size_t)i * ncol + c] = acc[b];
+  for (int u = 0; u < CPT; ++u) {
+    const int c = c0 + u * blockDim.x;
+    if (c >= ncol) break;
+#pragma unroll
+    for (int b = 0; b < BW; ++b) {
+      T v = acc[u][b];
+      if (INV && v != (T)0) v = (T)1 / v;
+      if (b < bw) bands[b * plane + (size_t)i * ncol + c] = v;
+    }
   }
 }
 
@@ -102,9 +122,10 @@ __global__ void __launch_bounds__(128) k_cma_asm_rows(T* __restrict__ bands, int
 // Q > 0 and NDF > 0 (rows of at most Q entries, ndf2h = NDF): every load of
 // the row issued before the first product (the loads in flight together; a
 // loop over d3 left each thread one load at a time: 85 -> 58 us on C96 x 70
-// W3); otherwise loops over any number of entries and dofs.
+// W3); otherwise loops over any number of entries and dofs.  Rows of one
+// entry run 12 blocks per SM (their registers allowed 10: 53.8 -> 51.1 us).
 template <class T, class TL, int BW, int Q, int NDF>
-__global__ void __launch_bounds__(128) k_cma_hmht_rows(T* __restrict__ bands, int ncol, int nrow,
+__global__ void __launch_bounds__(128, Q == 1 ? 12 : 1) k_cma_hmht_rows(T* __restrict__ bands, int ncol, int nrow,
                                                        int bw, const TL* __restrict__ dh,
                                                        const TL* __restrict__ m2h, int ndf2h,
                                                        int nl, const int* __restrict__ rowptr,
@@ -460,7 +481,8 @@ int lfg_cma_assemble(lfg_cma m, lfg_lma a, const int* cb_to, const int* cb_from)
         dispatch_kind(a->kind, [&](auto tl) {
           using TL = decltype(tl);
           auto go = [&](auto k) {
-            launch_pdl(c, k, dim3(grid, m->nrow), dim3(128), 0, (T*)m->bands, m->ncol, m->nrow,
+            const int gx = (m->ncol + 128 * kAsmColsPerThread - 1) / (128 * kAsmColsPerThread);
+            launch_pdl(c, k, dim3(gx, m->nrow), dim3(128), 0, (T*)m->bands, m->ncol, m->nrow,
                        m->bw, (const TL*)a->a, m->asm_rowptr, (const int2*)m->asm_list);
           };
           if (m->bw <= 2) go(k_cma_asm_rows<T, TL, 2>);
@@ -689,7 +711,8 @@ int lfg_cma_assemble_m2v_lumped_inv(lfg_cma m, lfg_lma mm, const int* cbm) {
         dispatch_kind(mm->kind, [&](auto tl) {
           using TL = decltype(tl);
           auto go = [&](auto k) {
-            launch_pdl(c, k, dim3(grid, m->nrow), dim3(128), 0, (T*)m->bands, m->ncol, m->nrow,
+            const int gx = (m->ncol + 128 * kAsmColsPerThread - 1) / (128 * kAsmColsPerThread);
+            launch_pdl(c, k, dim3(gx, m->nrow), dim3(128), 0, (T*)m->bands, m->ncol, m->nrow,
                        m->bw, (const TL*)mm->a, m->asm_rowptr, (const int2*)m->asm_list);
           };
           if (m->bw <= 2) go(k_cma_asm_rows<T, TL, 2, true>);
