@@ -381,6 +381,74 @@ struct Update2NormOp {
   }
 };
 
+// The CG update of one iteration in one pass (cg_solve,
+// sci_iterative_solver_mod.f90:560-575): x += a p, r -= a q, acc <r, r>, and
+// the new x also written to snap when given.  Each value is formed as the
+// separate axpy kernels form it.
+template <class T>
+struct CgUpdateOp {
+  T* x;
+  const T* p;
+  T* r;
+  const T* q;
+  T* snap;
+  Sc a;
+  struct B {
+    T* x;
+    const T* p;
+    T* r;
+    const T* q;
+    T* snap;
+    T ap, am;
+    template <int W> __device__ void run(size_t i, double& acc) const {
+      LFG_PACK(T, W, xv, x, i);
+      LFG_PACK(T, W, pv, p, i);
+      LFG_PACK(T, W, rv, r, i);
+      LFG_PACK(T, W, qv, q, i);
+      Pack<T, W> nx, nr;
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        nx.e[k] = xv.e[k] + ap * pv.e[k];
+        nr.e[k] = rv.e[k] + am * qv.e[k];
+        acc += (double)nr.e[k] * (double)nr.e[k];
+      }
+      nx.store(x + i);
+      if (snap) nx.store(snap + i);
+      nr.store(r + i);
+    }
+  };
+  __device__ B bind() const {
+    const double ad = sc_eval(a);
+    return B{x, p, r, q, snap, (T)ad, (T)(-ad)};
+  }
+};
+
+// z = x / d and acc <x, z> in one pass: the diagonal preconditioner's apply
+// (X_divideby_Y) with the inner product that follows it in cg_solve.
+template <class T>
+struct DivideDotOp {
+  T* z;
+  const T* x;
+  const T* d;
+  struct B {
+    T* z;
+    const T* x;
+    const T* d;
+    template <int W> __device__ void run(size_t i, double& acc) const {
+      LFG_PACK(T, W, xv, x, i);
+      LFG_PACK(T, W, dv, d, i);
+      Pack<T, W> o;
+#pragma unroll
+      for (int k = 0; k < W; ++k) {
+        o.e[k] = xv.e[k] / dv.e[k];
+        acc += (double)xv.e[k] * (double)o.e[k];
+      }
+      o.store(z + i);
+    }
+  };
+  __device__ B bind() const { return B{z, x, d}; }
+};
+
 // x += b y; acc <x, next> (next null: <x, x>)  (gmres/fgmres Arnoldi, and
 // the monitored residual update of bicgstab / jacobi)
 template <class T>
@@ -641,6 +709,30 @@ void vec_update2_norm(lfg_field dx, lfg_field pv, lfg_field res, lfg_field v, Sc
                                                   (const T*)v->d, alpha},
                               dx->n(), all_aligned(dx->d, pv->d, res->d, v->d), slot,
                               "update2_norm", 6));
+}
+
+void vec_cg_update(lfg_field x, lfg_field p, lfg_field r, lfg_field q, lfg_field snap, Sc alpha,
+                   int slot) {
+  same_kind(x, p, "cg_update");
+  same_kind(x, r, "cg_update");
+  same_kind(x, q, "cg_update");
+  if (snap) same_kind(x, snap, "cg_update");
+  lfg_ctx c = x->ctx;
+  void* sn = snap ? snap->d : nullptr;
+  DISPATCH_KIND(x->kind, T,
+                launch_ewr<T>(c, CgUpdateOp<T>{(T*)x->d, (const T*)p->d, (T*)r->d,
+                                               (const T*)q->d, (T*)sn, alpha},
+                              x->n(), all_aligned(x->d, p->d, r->d, q->d, sn), slot,
+                              "cg_update", sn ? 7 : 6));
+}
+
+void vec_divide_dot(lfg_field z, lfg_field x, lfg_field d, int slot) {
+  same_kind(z, x, "divide_dot");
+  same_kind(z, d, "divide_dot");
+  lfg_ctx c = z->ctx;
+  DISPATCH_KIND(z->kind, T,
+                launch_ewr<T>(c, DivideDotOp<T>{(T*)z->d, (const T*)x->d, (const T*)d->d},
+                              z->n(), all_aligned(z->d, x->d, d->d), slot, "divide_dot", 3));
 }
 
 void vec_axpy_norm(lfg_field x, Sc b, lfg_field y, int slot) {

@@ -524,6 +524,10 @@ void vec_mgs_step(lfg_field v, lfg_field pv, lfg_field vj, lfg_field pvj, Sc alp
 void vec_scale2_dot(lfg_field v, lfg_field pv, Sc beta, lfg_field res, int slot);
 void vec_update2_norm(lfg_field dx, lfg_field pv, lfg_field res, lfg_field v, Sc alpha,
                       int slot);             // dx += a pv; res -= a v; slot = <res,res>
+// x += a p; r -= a q; slot = <r, r>; snap = x (snap may be null)
+void vec_cg_update(lfg_field x, lfg_field p, lfg_field r, lfg_field q, lfg_field snap, Sc alpha,
+                   int slot);
+void vec_divide_dot(lfg_field z, lfg_field x, lfg_field d, int slot);  // z = x / d; slot = <x, z>
 void vec_axpy_norm(lfg_field x, Sc b, lfg_field y, int slot);   // x += b y; slot = <x,x>
 // x += b y; slot = <x, next> (next null: <x, x>)
 void vec_axpy_dot(lfg_field x, Sc b, lfg_field y, lfg_field next, int slot);

@@ -441,6 +441,16 @@ struct CgSolver : lfg_solver_s {
   bool batched() const {
     return cfg.monitor_convergence && (size_t)ncol * nlev <= kCgBatchDofs;
   }
+  // z = P^{-1} r and slot = <r, z>; the diagonal preconditioner's division
+  // and the inner product in one pass
+  void precondition_dot(lfg_field r, lfg_field z, int slot) {
+    if (auto* dp = dynamic_cast<DiagPrec*>(prec)) {
+      vec_divide_dot(z, r, dp->diag, slot);
+      return;
+    }
+    prec->apply(r, z);
+    vec_dot(r, z, slot);
+  }
   void prepare() {
     if (batched())
       for (int i = snaps.size(); i < kCgBatch; ++i)
@@ -468,8 +478,7 @@ struct CgSolver : lfg_solver_s {
       return LFG_OK;
     }
     vec_set(z, sc_const(0.0));
-    prec->apply(r, z);
-    vec_dot(r, z, s_rz0);
+    precondition_dot(r, z, s_rz0);
     int rz = s_rz0, rzn = s_rz1;
     vec_copy(p, z);
     const double* R = ctx->red_results;
@@ -477,11 +486,9 @@ struct CgSolver : lfg_solver_s {
       // iteration j of a batch: its norm to slot s_nb + j, x to snaps[j]
       auto step = [&](int j) {
         op->apply_dot(p, z, p, s_pz);                               // z = A p, <p, A p>
-        vec_axpy(x, sc_div(1.0, R + rz, R + s_pz), p);
-        vec_axpy_norm(r, sc_div(-1.0, R + rz, R + s_pz), z, s_nb + j);
-        vec_copy(snaps[j].get(), x);
-        prec->apply(r, z);
-        vec_dot(r, z, rzn);                                          // rz_new
+        // x += alpha p, r -= alpha z, <r, r> to the batch's slot, x to snaps[j]
+        vec_cg_update(x, p, r, z, snaps[j].get(), sc_div(1.0, R + rz, R + s_pz), s_nb + j);
+        precondition_dot(r, z, rzn);                                 // z = P^-1 r, rz_new
         vec_aypx(p, sc_div(1.0, R + rzn, R + rz), z);
         std::swap(rz, rzn);
       };
@@ -511,9 +518,8 @@ struct CgSolver : lfg_solver_s {
     } else {
       for (iter = 1; iter <= cfg.max_iter; ++iter) {
         op->apply_dot(p, z, p, s_pz);                               // z = A p, <p, A p>
-        vec_axpy(x, sc_div(1.0, R + rz, R + s_pz), p);
         if (cfg.monitor_convergence) {
-          vec_axpy_norm(r, sc_div(-1.0, R + rz, R + s_pz), z, s_r);
+          vec_cg_update(x, p, r, z, nullptr, sc_div(1.0, R + rz, R + s_pz), s_r);
           r_nrm = std::sqrt(host(s_r));
           done = iter;
           if (r_nrm / r_nrm_0 <= cfg.r_tol || r_nrm <= cfg.a_tol) {
@@ -521,11 +527,11 @@ struct CgSolver : lfg_solver_s {
             break;
           }
         } else {
+          vec_axpy(x, sc_div(1.0, R + rz, R + s_pz), p);
           vec_axpy(r, sc_div(-1.0, R + rz, R + s_pz), z);
           done = iter;
         }
-        prec->apply(r, z);
-        vec_dot(r, z, rzn);                                          // rz_new
+        precondition_dot(r, z, rzn);                                 // z = P^-1 r, rz_new
         vec_aypx(p, sc_div(1.0, R + rzn, R + rz), z);
         std::swap(rz, rzn);
       }
