@@ -122,6 +122,57 @@ def test_multiply_and_scaled_add_against_oracle(ctx, kind):
 
 
 @pytest.mark.parametrize("kind", [R_DOUBLE, R_SINGLE])
+def test_products_of_wider_bands_against_oracle(ctx, kind):
+    """C += A B for W3 tridiagonal factors (spans 3 and 5: the kernel with
+    template span bounds 4 and 8) and for their pentadiagonal products
+    (spans 5 and 9: the general kernel), against the oracle."""
+    rng = np.random.default_rng(24)
+    dt = DT[kind]
+    p3T = oh.cma_size(NL, 1, 2, 0, 1, 1, 0)
+    pT3 = oh.cma_size(NL, 2, 1, 1, 0, 0, 1)
+    p3 = oh.cma_prod_size(p3T, pT3)                   # W3 <- W3, bandwidth 3
+    p5 = oh.cma_prod_size(p3, p3)                     # bandwidth 5
+    p9 = oh.cma_prod_size(p5, p5)                     # bandwidth 9
+
+    def op(p, bands):
+        return ColumnwiseOperator(ctx, kind, NCELL, p["nrow"], p["ncol"], p["bw"], p["alpha"],
+                                  p["beta"], p["gm"], p["gp"], np.arange(1, p["nrow"] + 1),
+                                  np.arange(1, p["ncol"] + 1), bands.ravel(order="F"))
+    for pa, pc in ((p3, p5), (p5, p9)):
+        Ab = rng.standard_normal((pa["bw"], pa["nrow"], NCELL))
+        Bb = rng.standard_normal((pa["bw"], pa["nrow"], NCELL))
+        C0 = rng.standard_normal((pc["bw"], pc["nrow"], NCELL))
+        C = op(pc, C0)
+        C.multiply(op(pa, Ab), op(pa, Bb))
+        ref = oh.cma_mul(Ab.astype(dt), pa, Bb.astype(dt), pa, C0.astype(dt), pc, NCELL)
+        assert rel(C.get(), ref) < TOL[kind]
+        C.multiply(op(pa, Ab), op(pa, Bb))            # same shapes: the check is kept
+        ref = oh.cma_mul(Ab.astype(dt), pa, Bb.astype(dt), pa, ref, pc, NCELL)
+        assert rel(C.get(), ref) < TOL[kind]
+
+
+@pytest.mark.parametrize("kind", [R_DOUBLE, R_SINGLE])
+def test_hmht_with_two_w3_dofs_per_cell(ctx, kind):
+    """asm_diag_hmht on a W3 space of two interior dofs per cell: two
+    entries per row on a three-wide band (the unrolled kernel's bound of
+    four entries), against the oracle."""
+    rng = np.random.default_rng(25)
+    dt = DT[kind]
+    p = oh.cma_size(NL, 2, 2, 0, 2, 0, 2)
+    dh = rng.standard_normal((NCELL * NL, 2, 4))
+    m2h = rng.standard_normal((NCELL * NL, 4, 4))
+    for d in range(4):
+        m2h[:, d, d] = 1.0 + rng.random(NCELL * NL)
+    Dh = lma(ctx, kind, dh, (2, 0), (4, 0))
+    M2h = lma(ctx, kind, m2h, (4, 0), (4, 0))
+    H = cma(ctx, kind, p)
+    cb = oh.banded_dofmap(NL, 2, 2, 0)
+    H.assemble_diag_hmht(Dh, M2h, cb)
+    ref = oh.cma_hmht(dh.astype(dt), m2h.astype(dt), p, NCELL, NL, cb, dt)
+    assert rel(H.get(), ref) < TOL[kind] * 10
+
+
+@pytest.mark.parametrize("kind", [R_DOUBLE, R_SINGLE])
 def test_hmht_and_m2v_against_oracle(ctx, kind):
     rng = np.random.default_rng(23)
     dt = DT[kind]
