@@ -113,11 +113,12 @@ enum { M_APPLY = 0, M_RESID = 1, M_RHS = 2 };
 // all loads of the chunk are issued before any arithmetic (addresses are
 // clamped into the column, so no load sits behind a branch), the stores
 // after (the compiler cannot reorder loads across stores through these
-// pointers).  DOT accumulates <y, w> (HASW) or <y, y> into acc.
-template <class T, int MODE, bool DOT, bool HASW, bool CF>
+// pointers).  DOT accumulates <y, w> (HASW) or <y, y> into acc.  y is
+// stored in TO (the values and acc are formed in T).
+template <class T, int MODE, bool DOT, bool HASW, bool CF, class TO = T>
 __device__ __forceinline__ void col_levels(const HelmArgs<T>& A, unsigned c, int k0,
                                            const T* __restrict__ x, const T* __restrict__ b,
-                                           T* __restrict__ y, const T* __restrict__ w,
+                                           TO* __restrict__ y, const T* __restrict__ w,
                                            double& acc) {
   const unsigned N = A.ncol;
   const int nl = A.nl;
@@ -169,14 +170,16 @@ __device__ __forceinline__ void col_levels(const HelmArgs<T>& A, unsigned c, int
   }
 #pragma unroll
   for (int kk = 0; kk < KC; ++kk)
-    if (kk < kn) y[(size_t)(k0 + kk) * N + c] = vout[kk];
+    if (kk < kn) y[(size_t)(k0 + kk) * N + c] = (TO)vout[kk];
 }
 
 // y = A x (RESID: y = b - A x).  DOT: accumulate <y, w> (w null: <y, y>)
 // into a deterministic reduction.  Thread = (column, chunk of KC levels).
-template <class T, bool RESID, bool DOT, bool HASW, bool CF>
+// TO: y's kind (FP32 for the mixed refinement's FP64 residual, rounded once
+// as a separate conversion would round it).
+template <class T, bool RESID, bool DOT, bool HASW, bool CF, class TO = T>
 __global__ void __launch_bounds__(256) k_helm_apply(HelmArgs<T> A, const T* __restrict__ x,
-                                                    const T* __restrict__ b, T* __restrict__ y,
+                                                    const T* __restrict__ b, TO* __restrict__ y,
                                                     const T* __restrict__ w, Red r) {
   grid_dep_wait();
   const unsigned N = A.ncol;
@@ -185,7 +188,8 @@ __global__ void __launch_bounds__(256) k_helm_apply(HelmArgs<T> A, const T* __re
   double acc = 0.0;
   for (unsigned t = blockIdx.x * blockDim.x + threadIdx.x; t < total; t += gridDim.x * blockDim.x) {
     const unsigned kc = t / N, c = t - kc * N;
-    col_levels<T, RESID ? M_RESID : M_APPLY, DOT, HASW, CF>(A, c, (int)kc * KC, x, b, y, w, acc);
+    col_levels<T, RESID ? M_RESID : M_APPLY, DOT, HASW, CF, TO>(A, c, (int)kc * KC, x, b, y, w,
+                                                               acc);
   }
   if (DOT) red_finish(r, acc);
 }
@@ -1165,6 +1169,28 @@ void helm_residual(lfg_helm op, lfg_field r_out, lfg_field x, lfg_field b, int s
   // x, b, the three bands and the couplings read, r written
   after_launch(c, "helm_residual",
                (uint64_t)(op->kind * (6 + coupling_words(op)) * (double)op->ncol * op->nl));
+}
+
+void helm_residual_lower(lfg_helm op, lfg_field r_out, lfg_field x, lfg_field b, int slot) {
+  LFG_REQUIRE(op->kind == LFG_R_DOUBLE, "helm_residual_lower: the operator must be r_double");
+  LFG_REQUIRE(r_out && r_out->kind == LFG_R_SINGLE && r_out->ncol == op->ncol &&
+                  r_out->nlev == op->nl,
+              "helm_residual_lower: r must be an r_single field of the operator's shape");
+  check_field(op, x, "helm_residual_lower");
+  check_field(op, b, "helm_residual_lower");
+  LFG_REQUIRE(slot >= 0, "helm_residual_lower: a reduction slot is required");
+  lfg_ctx c = op->ctx;
+  const Red r = c->red(slot);
+  const int bs = 256;
+  const size_t work = (size_t)op->ncol * ((op->nl + KC - 1) / KC);
+  auto k = op->hsym ? k_helm_apply<double, true, true, false, true, float>
+                    : k_helm_apply<double, true, true, false, false, float>;
+  launch_pdl(c, k, occ_grid(c, (const void*)k, bs, work), bs, 0, args_of<double>(op),
+             (const double*)x->d, (const double*)b->d, (float*)r_out->d, (const double*)nullptr,
+             r);
+  // x, b, the three bands and the couplings read in FP64, r written in FP32
+  after_launch(c, "helm_residual_lower",
+               (uint64_t)((8 * (5 + coupling_words(op)) + 4) * (double)op->ncol * op->nl));
 }
 
 void helm_smooth(lfg_helm op, double omega, lfg_field x_in, lfg_field b, lfg_field x_out,

@@ -536,6 +536,9 @@ void vec_scale_copy(lfg_field dst, Sc a, lfg_field src);        // dst = a src
 // Helmholtz launchers (lfg_helm.cu)
 void helm_apply(lfg_helm op, lfg_field y, lfg_field x, lfg_field dot_with, int slot);
 void helm_residual(lfg_helm op, lfg_field r, lfg_field x, lfg_field b, int norm_slot);
+// r = b - A x formed in FP64 by an r_double operator and stored in the
+// r_single field r; norm_slot = <b - A x, b - A x> in FP64
+void helm_residual_lower(lfg_helm op, lfg_field r, lfg_field x, lfg_field b, int norm_slot);
 // x_out = sweep(x_in); x_in null: zero guess.  rbuf: workspace of ncol*nl
 // values of the operator's kind for the right-hand side (null: the
 // context's scratch).

@@ -1034,7 +1034,7 @@ struct lfg_mixed_s {
   double tol = 1e-8;
   int max_outer = 10;
   int slot = 0;
-  FieldPtr r64, r32, e32;
+  FieldPtr r32, e32;  // the inner solve's residual and correction (its kind)
 };
 
 // ================================================================ C ABI
@@ -1268,7 +1268,6 @@ int lfg_mixed_create(lfg_helm op64, lfg_solver inner, double tol, int max_outer,
     m->max_outer = max_outer;
     m->slot = take_slots(2);
     try {
-      m->r64 = make_field(c, LFG_R_DOUBLE, op64->ncol, op64->nl);
       m->r32 = make_field(c, inner->kind, op64->ncol, op64->nl);
       m->e32 = make_field(c, inner->kind, op64->ncol, op64->nl);
     } catch (...) {
@@ -1297,9 +1296,9 @@ int lfg_mixed_apply(lfg_mixed m, lfg_field x, lfg_field b, int* outer, int* inne
                     x->ncol == m->op64->ncol && x->nlev == m->op64->nl &&
                     b->ncol == x->ncol && b->nlev == x->nlev,
                 "mixed_apply: x and b must be r_double fields of the operator");
-    lfg_field r64 = m->r64.get(), r32 = m->r32.get(), e32 = m->e32.get();
+    lfg_field r32 = m->r32.get(), e32 = m->e32.get();
     vec_set(x, sc_const(0.0));
-    vec_copy(r64, b);
+    vec_copy(r32, b);  // the first residual is b (x = 0)
     vec_dot(b, b, m->slot);
     const double nb = std::sqrt(c->read_result(m->slot));
     int o = 0, inner_steps = 0;
@@ -1308,7 +1307,6 @@ int lfg_mixed_apply(lfg_mixed m, lfg_field x, lfg_field b, int* outer, int* inne
       status = LFG_OK;
     } else {
       for (o = 1; o <= m->max_outer; ++o) {
-        vec_copy(r32, r64);
         vec_set(e32, sc_const(0.0));
         int its = 0;
         double ierr = 0.0;
@@ -1319,7 +1317,11 @@ int lfg_mixed_apply(lfg_mixed m, lfg_field x, lfg_field b, int* outer, int* inne
           break;
         }
         vec_axpy(x, sc_const(1.0), e32);
-        helm_residual(m->op64, r64, x, b, m->slot);
+        // r = b - A x in FP64, its norm, and r stored in the inner solve's
+        // kind for the next refinement (one pass: no FP64 residual field
+        // written and converted)
+        if (r32->kind == LFG_R_SINGLE) helm_residual_lower(m->op64, r32, x, b, m->slot);
+        else helm_residual(m->op64, r32, x, b, m->slot);
         rr = std::sqrt(c->read_result(m->slot)) / nb;
         if (std::isnan(rr)) {
           status = LFG_NAN;
