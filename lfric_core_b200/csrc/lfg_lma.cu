@@ -141,6 +141,7 @@ constexpr int kLocDf = 16;  // largest ndf handled by the two-phase form
 // fewer loads per thread, more threads with loads in flight.
 template <class T, bool TR, int NT, int NF, int OS = 1>
 __global__ void k_lma_local(LmaArgs<T> L, const T* __restrict__ x, T* __restrict__ loc) {
+  grid_dep_wait();
   constexpr int CIN = TR ? NT : NF, COUT = TR ? NF : NT;
   static_assert(OS == 1 || (COUT > 0 && COUT % OS == 0), "output split needs fixed sizes");
   constexpr int MAXIN = CIN > 0 ? CIN : kLocDf;
@@ -206,6 +207,7 @@ __global__ void k_lma_local(LmaArgs<T> L, const T* __restrict__ x, T* __restrict
 template <class T>
 __global__ void __launch_bounds__(256) k_lma_local_tsplit(LmaArgs<T> L, const T* __restrict__ x,
                                                           T* __restrict__ loc) {
+  grid_dep_wait();
   const size_t plane = (size_t)L.ncell * L.nl;
   const size_t total = 2 * plane, trips = (total + 31) & ~(size_t)31;
   for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < trips;
@@ -257,6 +259,7 @@ __device__ __forceinline__ int slot_off(int2 s) { return s.y >> 8; }
 template <class T, bool INC, int W, int KC>
 __global__ void k_lma_gather_tab(const int2* __restrict__ tab, int nent, int nlev, int nl,
                                  int ncell, const T* __restrict__ loc, T* __restrict__ y) {
+  grid_dep_wait();
   const int e = blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= nent) return;
   int2 s[W];
@@ -407,7 +410,7 @@ template <class T, bool TR>
 void launch_local(lfg_ctx c, lfg_lma m, const T* x, T* loc) {
   const size_t ncl = (size_t)m->ncell * m->nl;
   auto go = [&](void (*k)(LmaArgs<T>, const T*, T*), int os) {
-    k<<<occ_grid(c, (const void*)k, 256, ncl * os), 256, 0, c->stream>>>(args_of<T>(m), x, loc);
+    launch_pdl(c, k, occ_grid(c, (const void*)k, 256, ncl * os), 256, 0, args_of<T>(m), x, loc);
   };
   // 8x8: forward outputs split over 2 threads (48.0 against 53.7 us on the
   // C48x30 W0 operator); the transposed products split their inputs over a
@@ -431,7 +434,7 @@ void launch_gather_tab(lfg_ctx c, const int2* tab, int w, int nent, int nlev, in
   constexpr int KC = 4;
   const dim3 grid((nent + 127) / 128, (nlev + KC - 1) / KC);
   auto go = [&](void (*k)(const int2*, int, int, int, int, const T*, T*)) {
-    k<<<grid, 128, 0, c->stream>>>(tab, nent, nlev, nl, ncell, loc, y);
+    launch_pdl(c, k, grid, dim3(128), 0, tab, nent, nlev, nl, ncell, loc, y);
   };
   switch (w) {
     case 1: go(k_lma_gather_tab<T, INC, 1, KC>); break;
