@@ -358,3 +358,25 @@ def test_partitioned_multigrid_gcr_matches_the_single_domain_oracle(world):
         x[owned] = xo.reshape(-1, p.nlayers)
     x = x.ravel()
     assert np.linalg.norm(x - x1) / np.linalg.norm(x1) < 1e-10
+
+
+def test_partition_helpers_reject_bad_input():
+    """partition needs 1 <= world <= columns; halo_plan needs a rank for
+    every column; mg_owners needs every fine column to have a parent."""
+    from lfric_core_b200.mesh import cubed_sphere
+    from lfric_core_b200.problems import coarsen_map
+    links = cubed_sphere(4).face_links
+    with pytest.raises(ValueError):
+        partition(10, 0)
+    with pytest.raises(ValueError):
+        partition(3, 4)
+    bad = np.zeros(links.shape[0], dtype=np.int64)
+    bad[5] = 2
+    with pytest.raises(ValueError):
+        halo_plan(links, 0, 2, owner=bad)
+    child = coarsen_map(4).copy()
+    child.reshape(-1)[0] = child.reshape(-1)[1]      # one fine column lost its parent
+    with pytest.raises(ValueError):
+        mg_owners([child], 24, 2)
+    with pytest.raises(ValueError):                  # more ranks than coarsest columns
+        mg_owners([coarsen_map(4)], 24, 25)
