@@ -40,6 +40,11 @@ struct lfg_linop_s {
     apply(x, y);
     vec_dot(y, w ? w : y, slot);
   }
+  // r = b - A x; tmp (a field of the operator's shape) may be overwritten
+  virtual void residual(lfg_field x, lfg_field b, lfg_field r, lfg_field tmp) {
+    apply(x, tmp);
+    vec_axpby(r, sc_const(1.0), b, sc_const(-1.0), tmp);
+  }
 };
 
 namespace {
@@ -55,6 +60,10 @@ struct HelmLinop : lfg_linop_s {
   void apply(lfg_field x, lfg_field y) override { helm_apply(h, y, x, nullptr, -1); }
   void apply_dot(lfg_field x, lfg_field y, lfg_field w, int slot) override {
     helm_apply(h, y, x, w, slot);
+  }
+  // one pass: each b - (A x) rounded once, as apply + axpby round it
+  void residual(lfg_field x, lfg_field b, lfg_field r, lfg_field) override {
+    helm_residual(h, r, x, b, -1);
   }
 };
 
@@ -561,8 +570,7 @@ struct GcrSolver : lfg_solver_s {
     int iter, steps = 0;
     vec_set(dx, sc_const(0.0));
     prec->apply(b, dx);
-    op->apply(dx, Ax);
-    vec_axpby(res, sc_const(1.0), b, sc_const(-1.0), Ax);
+    op->residual(dx, b, res, Ax);
     sc_err = std::sqrt(dot(b, b, s_b));
     if (iters) *iters = 0;
     if (err_out) *err_out = NAN;
@@ -632,8 +640,7 @@ struct BlockGcrSolver : lfg_solver_s {
     double err = NAN;
     vec_set(x, sc_const(0.0));
     prec->apply(b, x);
-    op->apply(x, Ax);
-    vec_axpby(res, sc_const(1.0), b, sc_const(-1.0), Ax);
+    op->residual(x, b, res, Ax);
     if (cfg.monitor_convergence)
       for (int n = 0; n < nf; ++n) ie[n] = std::max(field_norm(b, n, s_f), cfg.a_tol * cfg.r_tol);
     int iter, steps = 0;
